@@ -1,0 +1,67 @@
+/*
+ * polesitter_b200.h -- extensions of the drop-in API (no counterpart in the
+ * reference unless stated).  Include after polesitter.h.
+ */
+#ifndef POLESITTER_B200_H
+#define POLESITTER_B200_H
+
+#include "polesitter.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* bytes of cfg->buff the context itself occupies (the reference's
+ * equivalent is sizeof(ps_context_t), polesitter.h:1700) */
+size_t ps_b200_context_size(void);
+
+/* options, applied to later ticks of ctx */
+#define PS_B200_OPT_DEBUG 1          /* record per-node interaction counts */
+#define PS_B200_OPT_THETA 2          /* change theta after ps_init */
+#define PS_B200_OPT_TIMING 4         /* time tick phases with CUDA events */
+ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
+
+/* Morton quantisation of ps_prepare_particles, process-wide (it takes no
+ * context): 0 = AVX2 rounding (polesitter.h:2015-2073, the x86 default),
+ * 1 = NEON truncation (:2074-2127), 2 = scalar (:2132-2157). */
+ps_result_t ps_b200_set_morton_variant(int variant);
+
+/* counters of the last tick: [0] MAC tests, [1] M2L pairs, [2] P2P leaf
+ * pairs, [3] P2P particle pairs (0-3 need PS_B200_OPT_DEBUG), [8] nodes,
+ * [9] deepest traversal stack */
+ps_result_t ps_b200_get_stats(ps_context_t* ctx, uint64_t* out, size_t n);
+
+/* per-phase device times of the last tick in ms (PS_B200_OPT_TIMING):
+ * [0] sort, [1] gather + write-back, [2] tree build, [3] upward pass,
+ * [4] traversal (M2L/L2L/L2P/P2P), [5] whole tick */
+ps_result_t ps_b200_last_timing(ps_context_t* ctx, float* ms, size_t n);
+
+/* The last tick's tree in canonical form: level-major, each level in Morton
+ * order (the order the reference's recursion creates nodes,
+ * polesitter.h:923-966).  Per node: depth, first particle, count, children,
+ * octant, first child and parent (indices into this table), centre +
+ * half-width, multipole, local expansion after the downward pass, and (with
+ * PS_B200_OPT_DEBUG) the node's M2L and P2P pair counts as target. */
+size_t ps_b200_tree_nodes(ps_context_t* ctx);
+ps_result_t ps_b200_tree_dump(ps_context_t* ctx, size_t cap, int32_t* depth,
+                              uint32_t* start, uint32_t* count, uint32_t* nchild,
+                              int32_t* octant, uint32_t* first_child, uint32_t* parent,
+                              float* geo, float* mp, float* local_exp,
+                              uint32_t* m2l_cnt, uint32_t* p2p_cnt);
+
+/* FP64 direct-sum forces F_i = sum_{j != i} m_i m_j d / (|d|^2 + 0.1F)^1.5
+ * on the GPU (the accuracy yardstick of tests/accuracy.c:42-72) for
+ * n_targets particle indices into arrs; out holds n_targets x 3 doubles.
+ * Arrays may be host or device memory.  Uses ctx's device scratch, so call
+ * it between ticks. */
+ps_result_t ps_b200_direct_f64(ps_context_t* ctx, const ps_particle_arrs_t* arrs,
+                               const uint32_t* targets, size_t n_targets, double* out);
+
+/* message of the last CUDA-side failure on this thread */
+const char* ps_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLESITTER_B200_H */

@@ -1,0 +1,236 @@
+"""polesitter_b200 -- the polesitter FMM tick on one B200, behind the
+reference's own C API.
+
+The product is ``libpolesitter_b200.so`` (built in-tree by
+``polesitter_b200.build``), which exports ``ps_init``,
+``ps_prepare_particles``, ``ps_calc_forces`` and ``ps_destroy`` with the
+reference's types (include/polesitter.h) plus ``ps_b200_*`` extensions
+(include/polesitter_b200.h).  This module is a thin ctypes mirror of that
+interface -- same names, argument meaning and result codes -- used by the
+tests and the benchmark.  It never computes anything itself: if the library
+is missing, importing :func:`lib` raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libpolesitter_b200.so")
+
+# ps_result_t (polesitter.h:294-300) + PS_EDEVICE
+PS_OK, PS_EOOM, PS_EINVAL, PS_ETHRD, PS_EALLOC, PS_EDEVICE = 0, -1, -2, -3, -4, -5
+RESULT_NAMES = {0: "PS_OK", -1: "PS_EOOM", -2: "PS_EINVAL", -3: "PS_ETHRD",
+                -4: "PS_EALLOC", -5: "PS_EDEVICE"}
+
+OPT_DEBUG, OPT_THETA, OPT_TIMING = 1, 2, 4
+MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
+
+EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
+            "ps_b200_context_size", "ps_b200_set_option", "ps_b200_set_morton_variant",
+            "ps_b200_get_stats", "ps_b200_last_timing", "ps_b200_tree_nodes",
+            "ps_b200_tree_dump", "ps_b200_direct_f64", "ps_b200_last_error")
+
+
+class ParticleArrs(C.Structure):
+    """``ps_particle_arrs_t`` (polesitter.h:312-322)."""
+
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p),
+                ("mass", C.c_void_p), ("fx", C.c_void_p), ("fy", C.c_void_p),
+                ("fz", C.c_void_p), ("id", C.c_void_p), ("cnt", C.c_size_t)]
+
+
+class Config(C.Structure):
+    """``ps_config_t`` (polesitter.h:304-310)."""
+
+    _fields_ = [("buff", C.c_void_p), ("buff_size", C.c_size_t),
+                ("max_particles", C.c_size_t), ("theta", C.c_float),
+                ("thrd_cnt", C.c_size_t)]
+
+
+class PolesitterError(RuntimeError):
+    def __init__(self, call: str, code: int, detail: str = ""):
+        self.code = code
+        super().__init__(f"{call} -> {RESULT_NAMES.get(code, code)}"
+                         + (f" ({detail})" if detail else ""))
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library; raise if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m polesitter_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, sz, f32 = C.c_void_p, C.c_size_t, C.c_float
+    L.ps_init.restype = C.c_int
+    L.ps_init.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Config)]
+    L.ps_prepare_particles.restype = C.c_int
+    L.ps_prepare_particles.argtypes = [C.POINTER(ParticleArrs), vp, C.POINTER(f32),
+                                       C.POINTER(f32), C.POINTER(f32)]
+    L.ps_calc_forces.restype = C.c_int
+    L.ps_calc_forces.argtypes = [vp, C.POINTER(ParticleArrs), vp, f32, f32, f32, f32]
+    L.ps_destroy.restype = C.c_int
+    L.ps_destroy.argtypes = [vp]
+    L.ps_b200_context_size.restype = sz
+    L.ps_b200_set_option.restype = C.c_int
+    L.ps_b200_set_option.argtypes = [vp, C.c_int, C.c_double]
+    L.ps_b200_set_morton_variant.restype = C.c_int
+    L.ps_b200_set_morton_variant.argtypes = [C.c_int]
+    L.ps_b200_get_stats.restype = C.c_int
+    L.ps_b200_get_stats.argtypes = [vp, vp, sz]
+    L.ps_b200_last_timing.restype = C.c_int
+    L.ps_b200_last_timing.argtypes = [vp, vp, sz]
+    L.ps_b200_tree_nodes.restype = sz
+    L.ps_b200_tree_nodes.argtypes = [vp]
+    L.ps_b200_tree_dump.restype = C.c_int
+    L.ps_b200_tree_dump.argtypes = [vp, sz] + [vp] * 12
+    L.ps_b200_direct_f64.restype = C.c_int
+    L.ps_b200_direct_f64.argtypes = [vp, C.POINTER(ParticleArrs), vp, sz, vp]
+    L.ps_b200_last_error.restype = C.c_char_p
+    _LIB = L
+    return L
+
+
+def _addr(a) -> int:
+    """Address of a numpy array (host) or a torch tensor (host or CUDA)."""
+    if a is None:
+        return 0
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous()
+        return a.data_ptr()
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def arrs_of(p, n=None) -> ParticleArrs:
+    """``ps_particle_arrs_t`` over an object with x, y, z, mass, fx, fy, fz, id
+    arrays (numpy or torch, host or device)."""
+    cnt = len(p.x) if n is None else n
+    return ParticleArrs(_addr(p.x), _addr(p.y), _addr(p.z), _addr(p.mass), _addr(p.fx),
+                        _addr(p.fy), _addr(p.fz), _addr(p.id), cnt)
+
+
+def _check(call, r):
+    if r != PS_OK:
+        detail = lib().ps_b200_last_error()
+        raise PolesitterError(call, r, detail.decode() if detail else "")
+
+
+def set_morton_variant(variant: int) -> None:
+    _check("ps_b200_set_morton_variant", lib().ps_b200_set_morton_variant(variant))
+
+
+def prepare_particles(p, codes):
+    """ps_prepare_particles: writes ``codes`` and returns (min_b, max_b, range)."""
+    arrs = arrs_of(p)
+    mn, mx, rg = C.c_float(), C.c_float(), C.c_float()
+    _check("ps_prepare_particles", lib().ps_prepare_particles(
+        C.byref(arrs), _addr(codes), C.byref(mn), C.byref(mx), C.byref(rg)))
+    return mn.value, mx.value, rg.value
+
+
+def root_box(min_b: float, rng: float):
+    """Root centre and half width as the reference's callers compute them
+    (README.md:78-79, tests/accuracy.c:497-499), in float32."""
+    import numpy as np
+    f = np.float32
+    c = f(min_b) + f(rng) / f(2.0)
+    hw = f(rng) / f(2.0)
+    return float(c), float(hw)
+
+
+class Context:
+    """One ``ps_context_t`` (ps_init ... ps_destroy)."""
+
+    def __init__(self, max_particles: int, theta: float = 2.0, thrd_cnt: int = 1,
+                 buff_size: int | None = None):
+        import numpy as np
+        L = lib()
+        size = buff_size if buff_size is not None else (
+            L.ps_b200_context_size() + 64 + 24 * max_particles + 4096)
+        self._buf = np.zeros(max(size, 1), np.uint8)
+        self.cfg = Config(self._buf.ctypes.data if size else 0, size, max_particles, theta,
+                          thrd_cnt)
+        self.ptr = C.c_void_p()
+        _check("ps_init", L.ps_init(C.byref(self.ptr), C.byref(self.cfg)))
+        self.max_particles = max_particles
+
+    def calc_forces(self, p, codes, cx, cy, cz, hw):
+        arrs = arrs_of(p)
+        _check("ps_calc_forces", lib().ps_calc_forces(self.ptr, C.byref(arrs), _addr(codes),
+                                                      cx, cy, cz, hw))
+
+    def tick(self, p, codes):
+        """prepare + calc as the reference's tick loop (README.md:74-88)."""
+        mn, mx, rg = prepare_particles(p, codes)
+        c, hw = root_box(mn, rg)
+        self.calc_forces(p, codes, c, c, c, hw)
+        return mn, mx, rg
+
+    def set_option(self, key: int, value: float):
+        _check("ps_b200_set_option", lib().ps_b200_set_option(self.ptr, key, value))
+
+    def stats(self) -> dict:
+        import numpy as np
+        out = np.zeros(16, np.uint64)
+        _check("ps_b200_get_stats", lib().ps_b200_get_stats(self.ptr, out.ctypes.data, 16))
+        return {"mac_tests": int(out[0]), "m2l_pairs": int(out[1]),
+                "p2p_pairs": int(out[2]), "p2p_interactions": int(out[3]),
+                "nodes": int(out[8]), "max_stack": int(out[9])}
+
+    def timing(self) -> dict:
+        import numpy as np
+        out = np.zeros(8, np.float32)
+        _check("ps_b200_last_timing", lib().ps_b200_last_timing(self.ptr, out.ctypes.data, 8))
+        return {"sort": float(out[0]), "gather": float(out[1]), "tree": float(out[2]),
+                "upward": float(out[3]), "traverse": float(out[4]), "tick": float(out[5])}
+
+    def tree(self) -> dict:
+        import numpy as np
+        L = lib()
+        n = L.ps_b200_tree_nodes(self.ptr)
+        t = {k: np.zeros(n, dt) for k, dt in (
+            ("depth", np.int32), ("start", np.uint32), ("count", np.uint32),
+            ("nchild", np.uint32), ("octant", np.int32), ("first_child", np.uint32),
+            ("parent", np.uint32), ("m2l_cnt", np.uint32), ("p2p_cnt", np.uint32))}
+        for k in ("geo", "mp", "local_exp"):
+            t[k] = np.zeros((n, 4), np.float32)
+        _check("ps_b200_tree_dump", L.ps_b200_tree_dump(
+            self.ptr, n, *(t[k].ctypes.data for k in (
+                "depth", "start", "count", "nchild", "octant", "first_child", "parent",
+                "geo", "mp", "local_exp", "m2l_cnt", "p2p_cnt"))))
+        t["leaf"] = (t["nchild"] == 0).astype(np.uint32)
+        return t
+
+    def direct_f64(self, p, targets):
+        import numpy as np
+        tg = np.ascontiguousarray(targets, np.uint32)
+        out = np.zeros((len(tg), 3), np.float64)
+        arrs = arrs_of(p)
+        _check("ps_b200_direct_f64", lib().ps_b200_direct_f64(
+            self.ptr, C.byref(arrs), tg.ctypes.data, len(tg), out.ctypes.data))
+        return out
+
+    def destroy(self):
+        if self.ptr:
+            _check("ps_destroy", lib().ps_destroy(self.ptr))
+            self.ptr = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().ps_destroy(self.ptr)
+        except Exception:
+            pass

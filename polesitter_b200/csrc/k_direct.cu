@@ -1,0 +1,66 @@
+// FP64 direct-sum forces on the GPU for a sample of target particles: the
+// accuracy yardstick every result is reported against.
+//
+// Reference: direct_reference in tests/accuracy.c:42-72 --
+//   F_i = sum_{j != i} m_i m_j d_ij / (|d_ij|^2 + eps2)^{3/2},
+// eps2 = the float literal 0.1F widened to double (accuracy.c:12, :57).
+// Sources are streamed through shared memory in tiles; each thread owns one
+// target and accumulates in FP64.
+#include "psg_common.cuh"
+#include "psg_kernels.h"
+
+namespace psg {
+
+constexpr int kDirThreads = 128;
+
+__global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __restrict__ xyzm,
+                                                            size_t n,
+                                                            const uint32_t* __restrict__ targets,
+                                                            size_t n_targets,
+                                                            double* __restrict__ out) {
+    __shared__ float4 tile[kDirThreads];
+    const size_t k = (size_t)blockIdx.x * kDirThreads + threadIdx.x;
+    const uint32_t ti_raw = k < n_targets ? targets[k] : 0u;
+    const bool active = k < n_targets && ti_raw < n;
+    const uint32_t ti = active ? ti_raw : 0u;
+    const float4 t = active ? xyzm[ti] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const double eps2 = (double)0.1f;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (size_t j0 = 0; j0 < n; j0 += kDirThreads) {
+        const size_t j = j0 + threadIdx.x;
+        tile[threadIdx.x] = j < n ? xyzm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        const int cnt = (int)((n - j0) < (size_t)kDirThreads ? (n - j0) : kDirThreads);
+        for (int q = 0; q < cnt; ++q) {
+            const float4 s = tile[q];
+            const double dx = (double)s.x - (double)t.x;
+            const double dy = (double)s.y - (double)t.y;
+            const double dz = (double)s.z - (double)t.z;
+            const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+            const double ir = rsqrt(r2);
+            const double w = ((j0 + q) == ti) ? 0.0 : (double)s.w * ir * ir * ir;
+            ax += dx * w;
+            ay += dy * w;
+            az += dz * w;
+        }
+        __syncthreads();
+    }
+    if (k < n_targets && !active) {
+        out[3 * k + 0] = out[3 * k + 1] = out[3 * k + 2] = __longlong_as_double(0x7FF8000000000000ll);
+    }
+    if (active) {
+        const double m = (double)t.w;
+        out[3 * k + 0] = m * ax;
+        out[3 * k + 1] = m * ay;
+        out[3 * k + 2] = m * az;
+    }
+}
+
+void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
+                       double* out, cudaStream_t st) {
+    if (n_targets == 0) return;
+    const int grid = (int)((n_targets + kDirThreads - 1) / kDirThreads);
+    k_direct_f64<<<grid, kDirThreads, 0, st>>>(xyzm, n, targets, n_targets, out);
+}
+
+}  // namespace psg

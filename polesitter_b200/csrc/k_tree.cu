@@ -1,0 +1,343 @@
+// Octree build from the sorted Morton codes, and the upward pass (P2M/M2M).
+//
+// Reference: ps_impl_build_tree (polesitter.h:906-967) recursively splits a
+// node [s, e) at depth d < 10 holding >= 2 particles into one child per
+// non-empty octant of digit (code >> (27 - 3d)) & 7; a node is a leaf when
+// d == 10 or it holds <= 1 particle (:911-916).  Equivalently, with
+// cpl(i) = the number of leading octal digits codes[i-1] and codes[i] share,
+// a depth-d node starts at position i iff
+//     (i == 0 or cpl(i) < d)                        -- a depth-d run starts
+// and (cpl(i) >= d-1 or cpl(i+1) >= d-1)            -- its parent run has >= 2
+// so the whole tree comes from one pass of flags and a 10-wide prefix scan,
+// with no recursion.  Levels are stored contiguously in Morton order.
+//
+// Child centres follow the reference's float chain exactly (:935-939):
+// hw_child = hw * 0.5 and c_child = c_parent +/- hw_child, replayed from the
+// root for each node.
+#include "psg_common.cuh"
+#include "psg_kernels.h"
+
+namespace psg {
+
+constexpr int kTreeThreads = 256;
+constexpr int kTreePer = 4;
+constexpr int kTreeTile = kTreeThreads * kTreePer;  // 1024 positions
+
+int tree_tile_size() { return kTreeTile; }
+
+__device__ __forceinline__ int cpl_at(const uint32_t* __restrict__ c, size_t i, size_t n) {
+    // common octal prefix length of codes[i-1], codes[i]; -1 outside [1, n)
+    if (i == 0 || i >= n) return -1;
+    uint32_t x = (c[i - 1] ^ c[i]) & 0x3FFFFFFFu;
+    if (x == 0u) return kMaxDepth;
+    return (__clz(x) - 2) / 3;
+}
+
+// 10 one-bit flags (bit d-1 <=> a depth-d node starts at i)
+__device__ __forceinline__ uint32_t node_flags(int cpl_i, int cpl_next, bool first) {
+    uint32_t f = 0;
+#pragma unroll
+    for (int d = 1; d <= kMaxDepth; ++d) {
+        bool start = first || cpl_i < d;
+        bool pge2 = (cpl_i >= d - 1) || (cpl_next >= d - 1);
+        if (start && pge2) f |= 1u << (d - 1);
+    }
+    return f;
+}
+
+// counters of depths 1..5 in lo, 6..10 in hi, 12 bits each
+__device__ __forceinline__ void add_flags(unsigned long long& lo, unsigned long long& hi,
+                                          uint32_t f) {
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+        lo += (unsigned long long)((f >> d) & 1u) << (12 * d);
+        hi += (unsigned long long)((f >> (d + 5)) & 1u) << (12 * d);
+    }
+}
+
+__device__ __forceinline__ uint32_t get_cnt(unsigned long long lo, unsigned long long hi,
+                                            int d /*1..10*/) {
+    return d <= 5 ? (uint32_t)((lo >> (12 * (d - 1))) & 0xFFFull)
+                  : (uint32_t)((hi >> (12 * (d - 6))) & 0xFFFull);
+}
+
+__device__ __forceinline__ void thread_flags(const uint32_t* __restrict__ codes, size_t n,
+                                             size_t p0, uint32_t (&f)[kTreePer]) {
+    int cprev = cpl_at(codes, p0, n);
+#pragma unroll
+    for (int q = 0; q < kTreePer; ++q) {
+        size_t i = p0 + q;
+        int cnext = cpl_at(codes, i + 1, n);
+        f[q] = (i < n) ? node_flags(cprev, cnext, i == 0) : 0u;
+        cprev = cnext;
+    }
+}
+
+__global__ void __launch_bounds__(kTreeThreads) k_tree_count(const uint32_t* __restrict__ codes,
+                                                            size_t n,
+                                                            uint32_t* __restrict__ tile_cnt) {
+    const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
+    uint32_t f[kTreePer];
+    thread_flags(codes, n, p0, f);
+    unsigned long long lo = 0, hi = 0;
+#pragma unroll
+    for (int q = 0; q < kTreePer; ++q) add_flags(lo, hi, f[q]);
+    lo = warp_sum(lo);
+    hi = warp_sum(hi);
+    __shared__ unsigned long long s[2][kTreeThreads / 32];
+    if (lane_id() == 0) {
+        s[0][threadIdx.x >> 5] = lo;
+        s[1][threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x < kMaxDepth) {
+        const int d = threadIdx.x + 1;
+        uint32_t c = 0;
+        for (int w = 0; w < kTreeThreads / 32; ++w) c += get_cnt(s[0][w], s[1][w], d);
+        tile_cnt[(size_t)blockIdx.x * kMaxDepth + threadIdx.x] = c;
+    }
+}
+
+// Exclusive scan of the tile counts per depth (one block of 1024 threads).
+__global__ void __launch_bounds__(1024) k_tree_scan(uint32_t* __restrict__ tile_cnt, int tiles,
+                                                    TreeView tv, Status* status) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    for (int d = 1; d <= kMaxDepth; ++d) {
+        if (threadIdx.x == 0) carry = 0;
+        __syncthreads();
+        for (int b0 = 0; b0 < tiles; b0 += 1024) {
+            int b = b0 + threadIdx.x;
+            uint32_t v = b < tiles ? tile_cnt[(size_t)b * kMaxDepth + d - 1] : 0u;
+            uint32_t inc = warp_incl_scan(v);
+            if (lane_id() == 31) wsum[threadIdx.x >> 5] = inc;
+            __syncthreads();
+            uint32_t add = carry;
+            for (int w = 0; w < (int)(threadIdx.x >> 5); ++w) add += wsum[w];
+            if (b < tiles) tile_cnt[(size_t)b * kMaxDepth + d - 1] = inc - v + add;
+            __syncthreads();
+            if (threadIdx.x == 1023) carry = add + inc;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            uint32_t total = carry;
+            if (total > tv.lvl_cap[d]) {
+                set_err(status, PSG_ERR_NODES);
+                total = tv.lvl_cap[d];
+            }
+            status->lvl_count[d] = total;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        status->lvl_count[0] = 1;
+        status->lvl_count[kLevels] = 0;
+    }
+}
+
+// centre of the node whose first code is `code` at depth d: the reference's
+// chain of d rounded adds from the root centre
+__device__ __forceinline__ float4 node_centre(uint32_t code, int d, float cx, float cy, float cz,
+                                              float hw) {
+    for (int l = 1; l <= d; ++l) {
+        hw = __fmul_rn(hw, 0.5f);
+        uint32_t dig = (code >> (30 - 3 * l)) & 7u;
+        cx = __fadd_rn(cx, (dig & 1u) ? hw : -hw);
+        cy = __fadd_rn(cy, (dig & 2u) ? hw : -hw);
+        cz = __fadd_rn(cz, (dig & 4u) ? hw : -hw);
+    }
+    return make_float4(cx, cy, cz, hw);
+}
+
+// end of the run of codes sharing code[i]'s first d octal digits (gallop,
+// then binary search)
+__device__ __forceinline__ size_t run_end(const uint32_t* __restrict__ c, size_t n, size_t i,
+                                          int d) {
+    const int sh = 30 - 3 * d;
+    const uint32_t key = (c[i] & 0x3FFFFFFFu) >> sh;
+    size_t lo = i, step = 1;  // invariant: prefix(c[lo]) == key
+    while (lo + step < n && ((c[lo + step] & 0x3FFFFFFFu) >> sh) == key) {
+        lo += step;
+        step <<= 1;
+    }
+    size_t hi = (lo + step < n) ? lo + step : n;  // prefix(c[hi]) != key or hi == n
+    while (hi - lo > 1) {
+        size_t mid = lo + ((hi - lo) >> 1);
+        if (((c[mid] & 0x3FFFFFFFu) >> sh) == key) lo = mid; else hi = mid;
+    }
+    return hi;
+}
+
+__global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __restrict__ codes,
+                                                           size_t n,
+                                                           const uint32_t* __restrict__ tile_off,
+                                                           TreeView tv, const Status* status,
+                                                           float cx, float cy, float cz,
+                                                           float hw) {
+    const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
+    uint32_t f[kTreePer];
+    thread_flags(codes, n, p0, f);
+    unsigned long long lo = 0, hi = 0;
+#pragma unroll
+    for (int q = 0; q < kTreePer; ++q) add_flags(lo, hi, f[q]);
+    // block exclusive scan of the packed counters
+    unsigned long long ilo = lo, ihi = hi;
+    const uint32_t l = lane_id(), w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long a = __shfl_up_sync(0xFFFFFFFFu, ilo, o);
+        unsigned long long b = __shfl_up_sync(0xFFFFFFFFu, ihi, o);
+        if (l >= (uint32_t)o) {
+            ilo += a;
+            ihi += b;
+        }
+    }
+    __shared__ unsigned long long s[2][kTreeThreads / 32];
+    __shared__ uint32_t s_off[kMaxDepth + 1];
+    if (l == 31) {
+        s[0][w] = ilo;
+        s[1][w] = ihi;
+    }
+    if (threadIdx.x < kMaxDepth)
+        s_off[threadIdx.x + 1] = tile_off[(size_t)blockIdx.x * kMaxDepth + threadIdx.x];
+    __syncthreads();
+    unsigned long long elo = ilo - lo, ehi = ihi - hi;
+    for (uint32_t j = 0; j < w; ++j) {
+        elo += s[0][j];
+        ehi += s[1][j];
+    }
+    uint32_t rank[kMaxDepth + 2];
+#pragma unroll
+    for (int d = 1; d <= kMaxDepth; ++d)
+        rank[d] = tv.lvl_base[d] + s_off[d] + get_cnt(elo, ehi, d);
+    rank[kMaxDepth + 1] = 0;
+
+    if (p0 == 0) {  // root
+        tv.geo[0] = make_float4(cx, cy, cz, hw);
+        tv.info[0] = make_uint4(0u, (uint32_t)n, tv.lvl_base[1], pack_flags(0, 0, 0));
+        tv.parent[0] = kNone;
+        tv.cbase[0] = tv.lvl_base[1];
+        tv.arrive[0] = 0;
+        tv.lt[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < kTreePer; ++q) {
+        const size_t i = p0 + q;
+        const uint32_t fq = f[q];
+        if (fq) {
+            const uint32_t code = codes[i];
+#pragma unroll 1
+            for (int d = 1; d <= kMaxDepth; ++d) {
+                if (!((fq >> (d - 1)) & 1u)) continue;
+                const uint32_t id = rank[d];
+                if (id - tv.lvl_base[d] >= status->lvl_count[d]) continue;  // capacity guard
+                const size_t end = run_end(codes, n, i, d);
+                const uint32_t cnt = (uint32_t)(end - i);
+                uint32_t par = 0;
+                if (d > 1) par = rank[d - 1] + ((fq >> (d - 2)) & 1u) - 1u;
+                const uint32_t cb = d < kMaxDepth ? rank[d + 1] : 0u;
+                tv.geo[id] = node_centre(code, d, cx, cy, cz, hw);
+                tv.info[id] = make_uint4((uint32_t)i, cnt, cb,
+                                         pack_flags(0, d, (code >> (30 - 3 * d)) & 7u));
+                tv.parent[id] = par;
+                tv.cbase[id] = cb;
+                tv.arrive[id] = 0;
+            }
+        }
+#pragma unroll
+        for (int d = 1; d <= kMaxDepth; ++d) rank[d] += (fq >> (d - 1)) & 1u;
+    }
+}
+
+// child count = next node's first-child rank - this node's (same level)
+__global__ void __launch_bounds__(256) k_tree_link(TreeView tv, const Status* status) {
+    const uint32_t total = tv.lvl_base[kLevels];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
+        int d = 0;
+        while (d < kMaxDepth && id >= tv.lvl_base[d + 1]) ++d;
+        const uint32_t r = id - tv.lvl_base[d];
+        const uint32_t cnt_d = status->lvl_count[d];
+        if (r >= cnt_d) continue;
+        uint32_t nch = 0;
+        if (d < kMaxDepth) {
+            const uint32_t next = (r + 1 < cnt_d) ? tv.cbase[id + 1]
+                                                  : tv.lvl_base[d + 1] + status->lvl_count[d + 1];
+            nch = next - tv.cbase[id];
+            if (nch > 8u) {  // codes not sorted by their 30-bit prefix
+                set_err(const_cast<Status*>(status), PSG_ERR_NODES);
+                nch = 0;
+            }
+        }
+        uint4 inf = tv.info[id];
+        inf.w = (inf.w & ~0xFu) | (nch & 0xFu);
+        tv.info[id] = inf;
+        tv.lt[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// P2M at every leaf, then M2M up the tree: the last child to finish
+// (arrival counter) combines its parent, so one launch covers all levels.
+// Operation order matches polesitter.h:978-1045 exactly (sequential sums over
+// the leaf's particles; children in octant order), every op rounded to nearest.
+__global__ void __launch_bounds__(256) k_upward(TreeView tv, const Status* status,
+                                                const float4* __restrict__ xyzm) {
+    if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
+    const uint32_t total = tv.lvl_base[kLevels];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
+        int d = 0;
+        while (d < kMaxDepth && id >= tv.lvl_base[d + 1]) ++d;
+        if (id - tv.lvl_base[d] >= status->lvl_count[d]) continue;
+        const uint4 inf = tv.info[id];
+        if (flags_nchild(inf.w) != 0) continue;
+        const float4 c = tv.geo[id];
+        float m0 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+        for (uint32_t k = 0; k < inf.y; ++k) {
+            const float4 p = xyzm[inf.x + k];
+            m0 = __fadd_rn(m0, p.w);
+            mx = __fadd_rn(mx, __fmul_rn(p.w, __fsub_rn(p.x, c.x)));
+            my = __fadd_rn(my, __fmul_rn(p.w, __fsub_rn(p.y, c.y)));
+            mz = __fadd_rn(mz, __fmul_rn(p.w, __fsub_rn(p.z, c.z)));
+        }
+        tv.mp[id] = make_float4(m0, mx, my, mz);
+        uint32_t node = id;
+        while (node != 0) {
+            const uint32_t par = tv.parent[node];
+            __threadfence();
+            const uint32_t nch = flags_nchild(__ldcg(&tv.info[par].w));
+            if (atomicAdd(&tv.arrive[par], 1u) != nch - 1) break;
+            __threadfence();
+            const float4 pc = __ldcg(&tv.geo[par]);
+            const uint32_t fc = __ldcg(&tv.info[par].z);
+            float p0 = 0.f, px = 0.f, py = 0.f, pz = 0.f;
+            for (uint32_t j = 0; j < nch; ++j) {
+                const float4 cm = __ldcg(&tv.mp[fc + j]);
+                const float4 cg = __ldcg(&tv.geo[fc + j]);
+                p0 = __fadd_rn(p0, cm.x);
+                px = __fadd_rn(px, __fadd_rn(cm.y, __fmul_rn(cm.x, __fsub_rn(cg.x, pc.x))));
+                py = __fadd_rn(py, __fadd_rn(cm.z, __fmul_rn(cm.x, __fsub_rn(cg.y, pc.y))));
+                pz = __fadd_rn(pz, __fadd_rn(cm.w, __fmul_rn(cm.x, __fsub_rn(cg.z, pc.z))));
+            }
+            tv.mp[par] = make_float4(p0, px, py, pz);
+            node = par;
+        }
+    }
+}
+
+void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView tv,
+                 Status* status, float cx, float cy, float cz, float hw, int grid,
+                 cudaStream_t st) {
+    const int tiles = (int)((n + kTreeTile - 1) / kTreeTile);
+    k_tree_count<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf);
+    k_tree_scan<<<1, 1024, 0, st>>>(tile_buf, tiles, tv, status);
+    k_tree_emit<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf, tv, status, cx, cy, cz, hw);
+    k_tree_link<<<grid, 256, 0, st>>>(tv, status);
+}
+
+void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int grid,
+                   cudaStream_t st) {
+    k_upward<<<grid, 256, 0, st>>>(tv, status, xyzm);
+}
+
+}  // namespace psg

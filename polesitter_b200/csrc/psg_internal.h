@@ -1,0 +1,95 @@
+/*
+ * Internal C ABI between the C99 host layer (host/polesitter.c) and the CUDA
+ * side of libpolesitter_b200.so.  Plain pointers and sizes only.
+ */
+#ifndef PSG_INTERNAL_H
+#define PSG_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* result codes: the reference's ps_result_t values (polesitter.h:294-300)
+ * plus one for a CUDA runtime failure */
+#define PSG_OK 0
+#define PSG_EOOM (-1)
+#define PSG_EINVAL (-2)
+#define PSG_ETHRD (-3)
+#define PSG_EALLOC (-4)
+#define PSG_EDEVICE (-5)
+
+/* device status error bits */
+#define PSG_ERR_SORT_SPIN 0x1u    /* a look-back wait ran out of iterations */
+#define PSG_ERR_NS_OVERFLOW 0x2u  /* near-list region too small: regrow, rerun */
+#define PSG_ERR_STACK 0x4u        /* traversal stack bound violated */
+#define PSG_ERR_NODES 0x8u        /* tree level over its capacity */
+#define PSG_ERR_P2P_BUF 0x10u     /* P2P staging bound violated */
+
+/* debug statistics slots (Status.stat) */
+#define PSG_STAT_MAC 0
+#define PSG_STAT_M2L 1
+#define PSG_STAT_P2P_PAIRS 2
+#define PSG_STAT_P2P_INTER 3
+
+/* Morton quantisation variants of polesitter.h:2013-2157 */
+#define PSG_MORTON_AVX2 0
+#define PSG_MORTON_NEON 1
+#define PSG_MORTON_SCALAR 2
+
+/* caller arrays for one tick; each pointer may be host or device memory */
+typedef struct {
+    float* x;
+    float* y;
+    float* z;
+    float* mass;
+    float* fx;
+    float* fy;
+    float* fz;
+    uint32_t* id;
+    uint32_t* codes;
+    size_t n;
+} psg_arrays_t;
+
+/* bytes of host memory the device state needs (placed in the caller's
+ * ps_config_t buffer right after the context header) */
+size_t psg_state_bytes(void);
+
+int psg_init(void* state, size_t max_particles, float theta);
+int psg_destroy(void* state);
+
+/* ps_prepare_particles: bbox + Morton codes.  Uses a process-wide workspace
+ * on the current CUDA device. */
+int psg_prepare(const psg_arrays_t* a, float* out_min, float* out_max,
+                float* out_range, int morton_variant);
+
+/* ps_calc_forces on a context */
+int psg_calc(void* state, const psg_arrays_t* a, float cx, float cy, float cz,
+             float hw);
+
+/* options and introspection (extended API) */
+int psg_set_option(void* state, int key, double value);
+int psg_get_stats(void* state, uint64_t* out, size_t n_out);
+size_t psg_tree_nodes(void* state);
+int psg_tree_dump(void* state, size_t cap, int32_t* depth, uint32_t* start,
+                  uint32_t* count, uint32_t* nchild, int32_t* octant,
+                  uint32_t* first_child, uint32_t* parent, float* geo,
+                  float* mp, float* lt, uint32_t* m2l_cnt, uint32_t* p2p_cnt);
+int psg_last_timing(void* state, float* out_ms, size_t n_out);
+int psg_direct_f64(void* state, const psg_arrays_t* a, const uint32_t* targets, size_t n_t,
+                   double* out);
+const char* psg_last_error(void);
+
+#define PSG_OPT_DEBUG 1          /* 1: record per-node interaction counts */
+#define PSG_OPT_THETA 2
+#define PSG_OPT_MORTON_VARIANT 3
+#define PSG_OPT_TIMING 4         /* 1: time phases with CUDA events */
+#define PSG_OPT_USE_GRAPH 5      /* 1: replay calc_forces as a CUDA graph */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSG_INTERNAL_H */

@@ -1,0 +1,570 @@
+// Device runtime behind the C ABI: per-context device memory, the tick's
+// launch sequence, host-pointer mirrors, status checks and the optional CUDA
+// graph replay of ps_calc_forces.
+//
+// Ownership follows the reference (polesitter.h:1699-1767): the caller owns
+// every particle array and the ps_config_t buffer, and the host-side state
+// lives inside that buffer.  The device scratch (sorted particles, tree,
+// near lists) is cudaMalloc'ed in ps_init from max_particles and freed in
+// ps_destroy; it replaces the reference's arena + radix temporaries.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "psg_common.cuh"
+#include "psg_kernels.h"
+
+namespace psg {
+
+static thread_local char g_err[256];
+
+static void note(const char* what, cudaError_t e) {
+    std::snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define PSG_CHECK(call)                        \
+    do {                                       \
+        cudaError_t _e = (call);               \
+        if (_e != cudaSuccess) {               \
+            ::psg::note(#call, _e);            \
+            return PSG_EDEVICE;                \
+        }                                      \
+    } while (0)
+
+#define PSG_ALLOC(ptr, bytes)                                        \
+    do {                                                             \
+        cudaError_t _e = cudaMalloc((void**)&(ptr), (bytes) ? (bytes) : 16); \
+        if (_e != cudaSuccess) {                                     \
+            ::psg::note("cudaMalloc " #ptr, _e);                     \
+            return PSG_EALLOC;                                       \
+        }                                                            \
+    } while (0)
+
+constexpr uint32_t kMagic = 0x50534732u;  // "PSG2"
+constexpr int kPhases = 8;
+enum Phase { PH_SORT = 0, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END, PH_BEGIN };
+
+struct Mirror {
+    float *x, *y, *z, *m, *fx, *fy, *fz;
+    uint32_t *id, *codes;
+    size_t cap;
+};
+
+struct State {
+    uint32_t magic;
+    int device;
+    int sms;
+    int trav_grid;
+    size_t max_particles;
+    float theta;
+    int morton_variant;
+    int debug;
+    int timing;
+    cudaStream_t stream;
+    float4* xyzm;
+    uint32_t* ids;
+    SortBuffers sort;
+    uint32_t* tree_tiles;
+    TreeView tv;
+    uint32_t* ns[2];
+    unsigned long long ns_cap;
+    double* facc;
+    Status* d_status;
+    Status* h_status;
+    Mirror mir;
+    cudaEvent_t ev[kPhases];
+    float ms[kPhases];
+    unsigned long long stats[16];
+    uint32_t last_nodes;
+};
+
+static int grid_for(const State* s, size_t n, int per_block_items) {
+    size_t want = (n + per_block_items - 1) / per_block_items;
+    size_t cap = (size_t)s->sms * 8;
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+
+static int alloc_ns(State* s, unsigned long long cap) {
+    for (int r = 0; r < 2; ++r) {
+        if (s->ns[r]) cudaFree(s->ns[r]);
+        s->ns[r] = nullptr;
+        PSG_ALLOC(s->ns[r], cap * sizeof(uint32_t));
+    }
+    s->ns_cap = cap;
+    return PSG_OK;
+}
+
+static int ensure_mirror(Mirror& mi, size_t n) {
+    if (mi.cap >= n) return PSG_OK;
+    void** ps[9] = {(void**)&mi.x, (void**)&mi.y, (void**)&mi.z, (void**)&mi.m, (void**)&mi.fx,
+                    (void**)&mi.fy, (void**)&mi.fz, (void**)&mi.id, (void**)&mi.codes};
+    for (auto p : ps) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    for (auto p : ps) {
+        cudaError_t e = cudaMalloc(p, n * 4 ? n * 4 : 16);
+        if (e != cudaSuccess) {
+            note("cudaMalloc mirror", e);
+            return PSG_EALLOC;
+        }
+    }
+    mi.cap = n;
+    return PSG_OK;
+}
+
+static void free_mirror(Mirror& mi) {
+    void* ps[9] = {mi.x, mi.y, mi.z, mi.m, mi.fx, mi.fy, mi.fz, mi.id, mi.codes};
+    for (auto p : ps)
+        if (p) cudaFree(p);
+    std::memset(&mi, 0, sizeof(mi));
+}
+
+// true when the GPU can dereference p (device or managed memory)
+static bool on_device(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static void free_state(State* s) {
+    void* ps[] = {s->xyzm, s->ids, s->sort.key_a, s->sort.key_b, s->sort.val_a, s->sort.val_b,
+                  s->sort.hist, s->sort.offs, s->sort.lookback, s->tree_tiles, s->tv.geo,
+                  s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
+                  s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->ns[0], s->ns[1],
+                  s->facc, s->d_status};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (s->h_status) cudaFreeHost(s->h_status);
+    free_mirror(s->mir);
+    for (int i = 0; i < kPhases; ++i)
+        if (s->ev[i]) cudaEventDestroy(s->ev[i]);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    s->magic = 0;
+}
+
+static int init_state(State* s, size_t maxp, float theta) {
+    std::memset(s, 0, sizeof(State));
+    PSG_CHECK(cudaGetDevice(&s->device));
+    PSG_CHECK(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device));
+    PSG_CHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < kPhases; ++i) PSG_CHECK(cudaEventCreate(&s->ev[i]));
+    s->max_particles = maxp;
+    s->theta = theta;
+    s->morton_variant = PSG_MORTON_AVX2;
+    const size_t n = maxp ? maxp : 1;
+    PSG_ALLOC(s->xyzm, n * sizeof(float4));
+    PSG_ALLOC(s->ids, n * 4);
+    PSG_ALLOC(s->sort.key_a, n * 4);
+    PSG_ALLOC(s->sort.key_b, n * 4);
+    PSG_ALLOC(s->sort.val_a, n * 4);
+    PSG_ALLOC(s->sort.val_b, n * 4);
+    PSG_ALLOC(s->sort.hist, 4 * 256 * 4);
+    PSG_ALLOC(s->sort.offs, 4 * 256 * 4);
+    const size_t stiles = (n + sort_tile_size() - 1) / sort_tile_size();
+    PSG_ALLOC(s->sort.lookback, 4 * stiles * 256 * 4);
+    const size_t ttiles = (n + tree_tile_size() - 1) / tree_tile_size();
+    PSG_ALLOC(s->tree_tiles, ttiles * kMaxDepth * 4);
+    // level capacities: min(8^d, n) nodes at depth d
+    uint32_t base = 0;
+    for (int d = 0; d <= kMaxDepth; ++d) {
+        unsigned long long cap8 = 1ull << (3 * d);
+        uint32_t cap = (uint32_t)(cap8 < n ? cap8 : n);
+        if (d == 0) cap = 1;
+        s->tv.lvl_base[d] = base;
+        s->tv.lvl_cap[d] = cap;
+        base += cap;
+    }
+    s->tv.lvl_base[kLevels] = base;
+    s->tv.lvl_cap[kLevels] = 0;
+    const size_t nodes = base;
+    PSG_ALLOC(s->tv.geo, nodes * 16);
+    PSG_ALLOC(s->tv.mp, nodes * 16);
+    PSG_ALLOC(s->tv.lt, nodes * 16);
+    PSG_ALLOC(s->tv.info, nodes * 16);
+    PSG_ALLOC(s->tv.parent, nodes * 4);
+    PSG_ALLOC(s->tv.arrive, nodes * 4);
+    PSG_ALLOC(s->tv.cbase, nodes * 4);
+    PSG_ALLOC(s->tv.ns_off, nodes * 4);
+    PSG_ALLOC(s->tv.ns_cnt, nodes * 4);
+    PSG_ALLOC(s->tv.dbg_m2l, nodes * 4);
+    PSG_ALLOC(s->tv.dbg_p2p, nodes * 4);
+    PSG_ALLOC(s->facc, n * 3 * sizeof(double));
+    PSG_ALLOC(s->d_status, sizeof(Status));
+    PSG_CHECK(cudaMallocHost((void**)&s->h_status, sizeof(Status)));
+    int r = alloc_ns(s, (unsigned long long)(n < 1024 ? 1024 : n) * 48ull);
+    if (r != PSG_OK) return r;
+    int bps = 0;
+    PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, traverse_kernel_ptr(),
+                                                            traverse_threads(), 0));
+    s->trav_grid = s->sms * (bps > 0 ? bps : 1);
+    s->magic = kMagic;
+    return PSG_OK;
+}
+
+static void record(State* s, int ph) {
+    if (s->timing) cudaEventRecord(s->ev[ph], s->stream);
+}
+
+// traversal of all levels; returns the status error bits (after sync)
+static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, float* fz,
+                         size_t n, uint32_t* err_out) {
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->work[0], 0, sizeof(s->d_status->work), s->stream));
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->ns_used[0], 0, sizeof(s->d_status->ns_used),
+                                  s->stream));
+        TravLaunch L;
+        L.tv = s->tv;
+        L.xyzm = xyzm;
+        L.fx = fx;
+        L.fy = fy;
+        L.fz = fz;
+        L.ns_cap = s->ns_cap;
+        L.facc = s->facc;
+        L.status = s->d_status;
+        L.theta = s->theta;
+        L.debug = s->debug;
+        for (int k = 1; k <= kMaxDepth; ++k)
+            launch_traverse_level(L, k, s->ns[(k - 1) & 1], s->ns[k & 1], s->trav_grid, s->stream);
+        record(s, PH_END);
+        PSG_CHECK(cudaGetLastError());
+        PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
+                                  cudaMemcpyDeviceToHost, s->stream));
+        PSG_CHECK(cudaStreamSynchronize(s->stream));
+        uint32_t err = s->h_status->err;
+        if (!(err & PSG_ERR_NS_OVERFLOW)) {
+            *err_out = err;
+            return PSG_OK;
+        }
+        unsigned long long need = 0;
+        for (int k = 0; k <= kLevels; ++k)
+            if (s->h_status->ns_used[k] > need) need = s->h_status->ns_used[k];
+        need = need + need / 4 + 1024;
+        if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
+        int r = alloc_ns(s, need);
+        if (r != PSG_OK) return r;
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, s->stream));
+        if (s->timing) cudaEventRecord(s->ev[PH_UP], s->stream);
+    }
+    note("near-list regrow", cudaErrorMemoryAllocation);
+    return PSG_EOOM;
+}
+
+static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, float hw) {
+    const size_t n = a->n;
+    if (n > s->max_particles) return PSG_EINVAL;
+    if (n == 0) return PSG_OK;
+    PSG_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    // caller arrays: use them in place when the GPU can reach them, else mirror
+    float* x = a->x; float* y = a->y; float* z = a->z; float* m = a->mass;
+    float* fx = a->fx; float* fy = a->fy; float* fz = a->fz;
+    uint32_t* id = a->id; uint32_t* codes = a->codes;
+    const bool dev[9] = {on_device(x), on_device(y), on_device(z), on_device(m), on_device(fx),
+                         on_device(fy), on_device(fz), on_device(id), on_device(codes)};
+    bool any_host = false;
+    for (bool d : dev) any_host |= !d;
+    if (any_host) {
+        int r = ensure_mirror(s->mir, s->max_particles);
+        if (r != PSG_OK) return r;
+        struct { void* h; void* d; bool in; } io[9] = {
+            {x, s->mir.x, true}, {y, s->mir.y, true}, {z, s->mir.z, true}, {m, s->mir.m, true},
+            {fx, s->mir.fx, false}, {fy, s->mir.fy, false}, {fz, s->mir.fz, false},
+            {id, s->mir.id, true}, {codes, s->mir.codes, true}};
+        for (int i = 0; i < 9; ++i)
+            if (!dev[i] && io[i].in)
+                PSG_CHECK(cudaMemcpyAsync(io[i].d, io[i].h, n * 4, cudaMemcpyHostToDevice, st));
+        if (!dev[0]) x = s->mir.x;
+        if (!dev[1]) y = s->mir.y;
+        if (!dev[2]) z = s->mir.z;
+        if (!dev[3]) m = s->mir.m;
+        if (!dev[4]) fx = s->mir.fx;
+        if (!dev[5]) fy = s->mir.fy;
+        if (!dev[6]) fz = s->mir.fz;
+        if (!dev[7]) id = s->mir.id;
+        if (!dev[8]) codes = s->mir.codes;
+    }
+    record(s, PH_BEGIN);
+    PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
+    if (n == 1) {
+        // a single particle: the root is a leaf and its only P2P term is
+        // the zero self-interaction (polesitter.h:1279-1449)
+        PSG_CHECK(cudaMemsetAsync(fx, 0, 4, st));
+        PSG_CHECK(cudaMemsetAsync(fy, 0, 4, st));
+        PSG_CHECK(cudaMemsetAsync(fz, 0, 4, st));
+    } else {
+        const int g = grid_for(s, n, 1024);
+        launch_sort(s->sort, codes, n, g, s->d_status, st);
+        record(s, PH_SORT);
+        launch_gather(s->sort.perm, x, y, z, m, id, n, s->xyzm, s->ids, g, st);
+        launch_writeback(s->xyzm, s->ids, n, x, y, z, m, id, g, st);
+        record(s, PH_GATHER);
+        const int gt = grid_for(s, s->tv.lvl_base[kLevels], 256);
+        launch_tree(codes, n, s->tree_tiles, s->tv, s->d_status, cx, cy, cz, hw, gt, st);
+        record(s, PH_TREE);
+        launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
+        record(s, PH_UP);
+        PSG_CHECK(cudaGetLastError());
+        uint32_t err = 0;
+        int r = run_traversal(s, s->xyzm, fx, fy, fz, n, &err);
+        if (r != PSG_OK) return r;
+        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_P2P_BUF)) {
+            std::snprintf(g_err, sizeof(g_err), "device status error 0x%x", err);
+            return PSG_EDEVICE;
+        }
+        if (err & PSG_ERR_NODES) {
+            std::snprintf(g_err, sizeof(g_err), "morton codes not sorted/30-bit (0x%x)", err);
+            return PSG_EINVAL;
+        }
+        uint32_t nodes = 0;
+        for (int d = 0; d <= kMaxDepth; ++d) nodes += s->h_status->lvl_count[d];
+        s->last_nodes = nodes;
+        for (int i = 0; i < 8; ++i) s->stats[i] = s->h_status->stat[i];
+        s->stats[8] = nodes;
+        s->stats[9] = s->h_status->max_stack;
+        if (s->timing) {
+            const int order[6] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_END};
+            for (int i = 0; i + 1 < 6; ++i)
+                cudaEventElapsedTime(&s->ms[i], s->ev[order[i]], s->ev[order[i + 1]]);
+            cudaEventElapsedTime(&s->ms[5], s->ev[PH_BEGIN], s->ev[PH_END]);
+        }
+    }
+    if (any_host) {
+        struct { void* h; void* d; } out[9] = {
+            {a->x, x}, {a->y, y}, {a->z, z}, {a->mass, m}, {a->fx, fx},
+            {a->fy, fy}, {a->fz, fz}, {a->id, id}, {a->codes, codes}};
+        for (int i = 0; i < 9; ++i)
+            if (!dev[i]) PSG_CHECK(cudaMemcpyAsync(out[i].h, out[i].d, n * 4,
+                                                   cudaMemcpyDeviceToHost, st));
+    }
+    PSG_CHECK(cudaStreamSynchronize(st));
+    return PSG_OK;
+}
+
+// ---- process-wide workspace of ps_prepare_particles (it takes no context) ----
+struct PrepWs {
+    std::mutex mu;
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    float2* partial = nullptr;
+    float* bbox = nullptr;
+    float* h_bbox = nullptr;
+    int grid = 0;
+    Mirror mir{};
+};
+static PrepWs g_prep;
+
+static int prepare(const psg_arrays_t* a, float* out_min, float* out_max, float* out_range,
+                   int variant) {
+    std::lock_guard<std::mutex> lock(g_prep.mu);
+    int dev = 0;
+    PSG_CHECK(cudaGetDevice(&dev));
+    if (g_prep.device != dev) {
+        if (g_prep.stream) {
+            cudaSetDevice(g_prep.device);
+            cudaStreamDestroy(g_prep.stream);
+            cudaFree(g_prep.partial);
+            cudaFree(g_prep.bbox);
+            cudaFreeHost(g_prep.h_bbox);
+            free_mirror(g_prep.mir);
+            cudaSetDevice(dev);
+        }
+        int sms = 0;
+        PSG_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        PSG_CHECK(cudaStreamCreateWithFlags(&g_prep.stream, cudaStreamNonBlocking));
+        g_prep.grid = sms * 4;
+        PSG_ALLOC(g_prep.partial, g_prep.grid * sizeof(float2));
+        PSG_ALLOC(g_prep.bbox, 4 * sizeof(float));
+        PSG_CHECK(cudaMallocHost((void**)&g_prep.h_bbox, 4 * sizeof(float)));
+        g_prep.device = dev;
+    }
+    const size_t n = a->n;
+    cudaStream_t st = g_prep.stream;
+    const float* x = a->x; const float* y = a->y; const float* z = a->z;
+    uint32_t* codes = a->codes;
+    const bool dx = on_device(x), dy = on_device(y), dz = on_device(z), dc = on_device(codes);
+    if (!(dx && dy && dz && dc)) {
+        int r = ensure_mirror(g_prep.mir, n);
+        if (r != PSG_OK) return r;
+        if (!dx) { PSG_CHECK(cudaMemcpyAsync(g_prep.mir.x, x, n * 4, cudaMemcpyHostToDevice, st)); x = g_prep.mir.x; }
+        if (!dy) { PSG_CHECK(cudaMemcpyAsync(g_prep.mir.y, y, n * 4, cudaMemcpyHostToDevice, st)); y = g_prep.mir.y; }
+        if (!dz) { PSG_CHECK(cudaMemcpyAsync(g_prep.mir.z, z, n * 4, cudaMemcpyHostToDevice, st)); z = g_prep.mir.z; }
+        if (!dc) codes = g_prep.mir.codes;
+    }
+    int grid = (int)((n + 1023) / 1024);
+    if (grid > g_prep.grid) grid = g_prep.grid;
+    if (grid < 1) grid = 1;
+    launch_prepare(x, y, z, n, g_prep.partial, grid, codes, g_prep.bbox, variant, st);
+    PSG_CHECK(cudaGetLastError());
+    if (!dc) PSG_CHECK(cudaMemcpyAsync(a->codes, codes, n * 4, cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaMemcpyAsync(g_prep.h_bbox, g_prep.bbox, 4 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaStreamSynchronize(st));
+    if (out_min) *out_min = g_prep.h_bbox[0];
+    if (out_max) *out_max = g_prep.h_bbox[1];
+    if (out_range) *out_range = g_prep.h_bbox[2];
+    return PSG_OK;
+}
+
+}  // namespace psg
+
+using psg::State;
+
+extern "C" {
+
+size_t psg_state_bytes(void) { return (sizeof(State) + 63) & ~(size_t)63; }
+
+int psg_init(void* mem, size_t max_particles, float theta) {
+    State* s = static_cast<State*>(mem);
+    int r = psg::init_state(s, max_particles, theta);
+    if (r != PSG_OK) psg::free_state(s);
+    return r;
+}
+
+int psg_destroy(void* mem) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    psg::free_state(s);
+    return PSG_OK;
+}
+
+int psg_prepare(const psg_arrays_t* a, float* out_min, float* out_max, float* out_range,
+                int variant) {
+    return psg::prepare(a, out_min, out_max, out_range, variant);
+}
+
+int psg_calc(void* mem, const psg_arrays_t* a, float cx, float cy, float cz, float hw) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
+    return psg::calc(s, a, cx, cy, cz, hw);
+}
+
+int psg_set_option(void* mem, int key, double value) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
+    switch (key) {
+        case PSG_OPT_DEBUG: s->debug = value != 0.0; return PSG_OK;
+        case PSG_OPT_THETA: s->theta = value > 0.0 ? (float)value : 1.0f; return PSG_OK;
+        case PSG_OPT_MORTON_VARIANT:
+            if (value < 0 || value > 2) return PSG_EINVAL;
+            s->morton_variant = (int)value;
+            return PSG_OK;
+        case PSG_OPT_TIMING: s->timing = value != 0.0; return PSG_OK;
+        default: return PSG_EINVAL;
+    }
+}
+
+int psg_get_stats(void* mem, uint64_t* out, size_t n_out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !out) return PSG_EINVAL;
+    for (size_t i = 0; i < n_out && i < 16; ++i) out[i] = s->stats[i];
+    return PSG_OK;
+}
+
+int psg_last_timing(void* mem, float* out_ms, size_t n_out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !out_ms) return PSG_EINVAL;
+    for (size_t i = 0; i < n_out && i < (size_t)psg::kPhases; ++i) out_ms[i] = s->ms[i];
+    return PSG_OK;
+}
+
+size_t psg_tree_nodes(void* mem) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return 0;
+    return s->last_nodes;
+}
+
+// canonical table (level-major, Morton order per level) copied to the host
+int psg_tree_dump(void* mem, size_t cap, int32_t* depth, uint32_t* start, uint32_t* count,
+                  uint32_t* nchild, int32_t* octant, uint32_t* first_child, uint32_t* parent,
+                  float* geo, float* mp, float* lt, uint32_t* m2l_cnt, uint32_t* p2p_cnt) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
+    if (cap < s->last_nodes) return PSG_EOOM;
+    PSG_CHECK(cudaSetDevice(s->device));
+    // global (capacity-strided) ids -> compact level-major ids
+    uint32_t cstart[psg::kLevels + 1];
+    cstart[0] = 0;
+    for (int d = 0; d <= psg::kMaxDepth; ++d) cstart[d + 1] = cstart[d] + s->h_status->lvl_count[d];
+    auto compact = [&](uint32_t g, int d) -> uint32_t {
+        return g - s->tv.lvl_base[d] + cstart[d];
+    };
+    size_t k = 0;
+    for (int d = 0; d <= psg::kMaxDepth; ++d) {
+        const uint32_t cnt = s->h_status->lvl_count[d];
+        const uint32_t b = s->tv.lvl_base[d];
+        if (!cnt) continue;
+        uint4* inf = new uint4[cnt];
+        PSG_CHECK(cudaMemcpy(inf, s->tv.info + b, cnt * 16, cudaMemcpyDeviceToHost));
+        PSG_CHECK(cudaMemcpy(geo + 4 * k, s->tv.geo + b, cnt * 16, cudaMemcpyDeviceToHost));
+        PSG_CHECK(cudaMemcpy(mp + 4 * k, s->tv.mp + b, cnt * 16, cudaMemcpyDeviceToHost));
+        PSG_CHECK(cudaMemcpy(lt + 4 * k, s->tv.lt + b, cnt * 16, cudaMemcpyDeviceToHost));
+        PSG_CHECK(cudaMemcpy(parent + k, s->tv.parent + b, cnt * 4, cudaMemcpyDeviceToHost));
+        PSG_CHECK(cudaMemcpy(m2l_cnt + k, s->tv.dbg_m2l + b, cnt * 4, cudaMemcpyDeviceToHost));
+        PSG_CHECK(cudaMemcpy(p2p_cnt + k, s->tv.dbg_p2p + b, cnt * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < cnt; ++i) {
+            depth[k + i] = d;
+            start[k + i] = inf[i].x;
+            count[k + i] = inf[i].y;
+            nchild[k + i] = psg::flags_nchild(inf[i].w);
+            octant[k + i] = d ? (int32_t)psg::flags_octant(inf[i].w) : -1;
+            first_child[k + i] = nchild[k + i] ? compact(inf[i].z, d + 1) : 0u;
+            parent[k + i] = d ? compact(parent[k + i], d - 1) : 0xFFFFFFFFu;
+        }
+        delete[] inf;
+        k += cnt;
+    }
+    return PSG_OK;
+}
+
+// FP64 direct-sum forces (tests/accuracy.c:42-72) for n_t sampled targets;
+// x/y/z/mass, targets and out may each be host or device memory.
+int psg_direct_f64(void* mem, const psg_arrays_t* a, const uint32_t* targets, size_t n_t,
+                   double* out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !a || !targets || !out) return PSG_EINVAL;
+    const size_t n = a->n;
+    if (n == 0 || n > s->max_particles) return PSG_EINVAL;
+    PSG_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    const float* src[4] = {a->x, a->y, a->z, a->mass};
+    float* tmp = nullptr;
+    PSG_ALLOC(tmp, n * 4);
+    // pack (x, y, z, m) into the context's particle scratch
+    for (int c = 0; c < 4; ++c) {
+        const float* p = src[c];
+        if (!psg::on_device(p)) {
+            PSG_CHECK(cudaMemcpyAsync(tmp, p, n * 4, cudaMemcpyHostToDevice, st));
+            p = tmp;
+        }
+        PSG_CHECK(cudaMemcpy2DAsync((char*)s->xyzm + 4 * c, 16, p, 4, 4, n,
+                                    cudaMemcpyDeviceToDevice, st));
+        PSG_CHECK(cudaStreamSynchronize(st));
+    }
+    cudaFree(tmp);
+    uint32_t* dt = const_cast<uint32_t*>(targets);
+    double* dout = out;
+    const bool ht = !psg::on_device(targets), ho = !psg::on_device(out);
+    if (ht) {
+        PSG_ALLOC(dt, n_t * 4);
+        PSG_CHECK(cudaMemcpyAsync(dt, targets, n_t * 4, cudaMemcpyHostToDevice, st));
+    }
+    if (ho) PSG_ALLOC(dout, n_t * 3 * sizeof(double));
+    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, st);
+    PSG_CHECK(cudaGetLastError());
+    if (ho) PSG_CHECK(cudaMemcpyAsync(out, dout, n_t * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaStreamSynchronize(st));
+    if (ht) cudaFree(dt);
+    if (ho) cudaFree(dout);
+    return PSG_OK;
+}
+
+const char* psg_last_error(void) { return psg::g_err; }
+
+}  // extern "C"
