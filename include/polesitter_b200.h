@@ -19,6 +19,7 @@ size_t ps_b200_context_size(void);
 #define PS_B200_OPT_DEBUG 1          /* record per-node interaction counts */
 #define PS_B200_OPT_THETA 2          /* change theta after ps_init */
 #define PS_B200_OPT_TIMING 4         /* time tick phases with CUDA events */
+#define PS_B200_OPT_KAHAN 6          /* compensated (Kahan) FP32 sums in P2P */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
 
 /* Morton quantisation of ps_prepare_particles, process-wide (it takes no
@@ -26,14 +27,15 @@ ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
  * 1 = NEON truncation (:2074-2127), 2 = scalar (:2132-2157). */
 ps_result_t ps_b200_set_morton_variant(int variant);
 
-/* counters of the last tick: [0] MAC tests, [1] M2L pairs, [2] P2P leaf
- * pairs, [3] P2P particle pairs (0-3 need PS_B200_OPT_DEBUG), [8] nodes,
- * [9] deepest traversal stack */
+/* counters of the last tick: [1] M2L pairs, [2] P2P leaf pairs, [3] P2P
+ * particle pairs, [9] deepest traversal stack (these need
+ * PS_B200_OPT_DEBUG), [8] nodes, [10] P2P list chunks */
 ps_result_t ps_b200_get_stats(ps_context_t* ctx, uint64_t* out, size_t n);
 
 /* per-phase device times of the last tick in ms (PS_B200_OPT_TIMING):
  * [0] sort, [1] gather + write-back, [2] tree build, [3] upward pass,
- * [4] traversal (M2L/L2L/L2P/P2P), [5] whole tick */
+ * [4] interaction pass of internal nodes (MAC/M2L/L2L, all levels),
+ * [5] leaf pass (MAC/M2L/L2L + P2P + L2P), [6] whole tick */
 ps_result_t ps_b200_last_timing(ps_context_t* ctx, float* ms, size_t n);
 
 /* The last tick's tree in canonical form: level-major, each level in Morton

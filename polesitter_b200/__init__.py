@@ -24,7 +24,7 @@ PS_OK, PS_EOOM, PS_EINVAL, PS_ETHRD, PS_EALLOC, PS_EDEVICE = 0, -1, -2, -3, -4, 
 RESULT_NAMES = {0: "PS_OK", -1: "PS_EOOM", -2: "PS_EINVAL", -3: "PS_ETHRD",
                 -4: "PS_EALLOC", -5: "PS_EDEVICE"}
 
-OPT_DEBUG, OPT_THETA, OPT_TIMING = 1, 2, 4
+OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN = 1, 2, 4, 6
 MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 
 EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
@@ -178,18 +178,21 @@ class Context:
 
     def stats(self) -> dict:
         import numpy as np
-        out = np.zeros(16, np.uint64)
-        _check("ps_b200_get_stats", lib().ps_b200_get_stats(self.ptr, out.ctypes.data, 16))
-        return {"mac_tests": int(out[0]), "m2l_pairs": int(out[1]),
-                "p2p_pairs": int(out[2]), "p2p_interactions": int(out[3]),
-                "nodes": int(out[8]), "max_stack": int(out[9])}
+        out = np.zeros(24, np.uint64)
+        _check("ps_b200_get_stats", lib().ps_b200_get_stats(self.ptr, out.ctypes.data, 24))
+        return {"m2l_pairs": int(out[1]), "p2p_pairs": int(out[2]),
+                "p2p_interactions": int(out[3]), "chunks_first": int(out[4]),
+                "chunks_dfs": int(out[5]), "tests_first": int(out[6]), "tests_dfs": int(out[7]),
+                "nodes": int(out[8]), "max_stack": int(out[9]), "p2p_chunks": int(out[10]),
+                "lanes": int(out[16]), "leaf_groups": int(out[17]), "dfs_steps": int(out[18])}
 
     def timing(self) -> dict:
         import numpy as np
         out = np.zeros(8, np.float32)
         _check("ps_b200_last_timing", lib().ps_b200_last_timing(self.ptr, out.ctypes.data, 8))
         return {"sort": float(out[0]), "gather": float(out[1]), "tree": float(out[2]),
-                "upward": float(out[3]), "traverse": float(out[4]), "tick": float(out[5])}
+                "upward": float(out[3]), "internal": float(out[4]), "leaves": float(out[5]),
+                "tick": float(out[6])}
 
     def tree(self) -> dict:
         import numpy as np

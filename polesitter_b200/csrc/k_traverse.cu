@@ -1,40 +1,50 @@
-// The interaction pass of the FMM tick, fused: MAC + M2L + L2L + L2P + P2P.
+// The interaction pass of the FMM tick: MAC + M2L + L2L, and for leaves also
+// P2P + L2P, producing the final forces.
 //
 // Reference (PS_MULTITHREADING build): every node at depth 2, and every leaf
 // above it, is paired with the root (ps_impl_dispatch_fmm, polesitter.h:
 // 1772-1801, :1883-1885), and each pair (t, s) is walked by the dual
 // recursion of ps_impl_fmm_interaction_pass (:1050-1146):
 //   separated (MAC)        -> M2L: t.local += field of s's monopole+dipole
-//   both leaves            -> left to P2P (the P2P pass :1258-1494 walks the
-//                             same pairs with the same MAC)
+//   both leaves            -> P2P (the P2P pass :1258-1494 walks the same
+//                             pairs with the same MAC)
 //   t leaf                 -> (t, each child of s)
 //   s leaf                 -> (each child of t, s)
 //   otherwise              -> (each child of t) x (each child of s)
-// then L2L adds every parent's field to its children (:1238-1251) and L2P
-// gives F = m * field at the leaves (:1224-1233), then P2P adds the direct
-// leaf x leaf sums.
+// then L2L adds every parent's field to its children (:1238-1251), L2P sets
+// F = m * field at the leaves (:1224-1233) and P2P adds the direct sums
+// f_t += m_t * sum_{j in s} m_j d / (|d|^2 + 0.1)^{3/2} (:1279-1449).
 //
-// B200 formulation (target-major, level-synchronous, no pair lists in HBM):
-// every pair (t, s) the recursion visits with an internal t at depth k and
-// internal s has its children pairs generated from t's "near list" NS(t) =
-// the sources s that t was not separated from.  So for each internal node p
-// at depth k-1 ("group"), the candidates of ALL its children are
-//   cand(p) = {root}                                  if k <= 2
-//   cand(p) = U_{s in NS(p)} (s leaf ? {s} : children(s))   otherwise
-// and one warp processes a group: lane j holds candidate j's centre,
-// multipole and links in registers and tests it against every child u of p
-// (<= 8), accumulating M2L in registers.  Non-separated candidates go to
-// NS(u) when u is internal (written to HBM for level k+1), to u's P2P buffer
-// when both are leaves, and onto a bounded DFS stack in shared memory when u
-// is a leaf and s is internal (the "t leaf" recursion).  A leaf's visits all
-// happen inside this warp, so the warp also finishes it: L(u) = M2L(u) +
-// L(p) (L2L), and F_i = m_i * (L(u) + sum of P2P) for its particles, written
-// once, with no atomics.  Internal children get L(u) = M2L(u) + L(p) stored
-// for their own groups at level k+1.
+// B200 formulation (target-major, no interaction lists in HBM).  The pairs
+// an internal target t hands to its children are its "near list" NS(t) =
+// the sources it was not separated from, so all children of an internal node
+// p (a "group") see the same candidates
+//   cand(p) = {root}                                         if depth(p) <= 1
+//   cand(p) = U_{s in NS(p)} (s leaf ? {s} : children(s))    otherwise.
+// One warp processes a group.  Candidates are staged 32 at a time in shared
+// memory together with the set of children each must be tested against; the
+// (candidate, child) pairs are flattened so every lane runs one MAC test per
+// step, and M2L results accumulate in lane-private shared-memory slots (one
+// per child), reduced once at the end.  Two kinds of launch:
+//
+//  * MODE_INTERNAL, one per level k = 2..10: the internal children of the
+//    depth-(k-1) groups.  Non-separated candidates go to NS(u) in HBM for
+//    level k+1; L(u) = M2L(u) + L(p) is stored.
+//  * MODE_LEAF, one launch after all levels: the leaf children of every
+//    group.  A non-separated leaf candidate is a P2P source, staged in shared
+//    memory (chunks spill to HBM only past 32 sources); a non-separated
+//    internal candidate is the "t leaf" recursion -- it goes onto a DFS stack
+//    in shared memory whose entries carry the set of sibling leaves that
+//    still need it opened, so siblings share one descent.  At the end the
+//    warp finishes each leaf: L(u) = M2L(u) + L(p) and, per particle,
+//    F = m * (L(u) + sum of its P2P terms) -- written once, no atomics.
+//    Running all levels' leaves in one launch lets the long descents of
+//    shallow leaves overlap with everything else.
 //
 // The MAC replays the reference's rounded float sequence exactly
 // (mac_separated), so the interaction set is identical, ties included.
-// Bound: FP32 pipe (M2L ~35 flop + 1 MUFU per pair, P2P ~20 flop + 1 MUFU).
+// Bound: FP32 pipe (M2L ~35 flop + 1 MUFU per pair; P2P ~20 flop + 1 MUFU
+// per particle pair) and the latency of the candidate loads.
 #include "psg_common.cuh"
 #include "psg_kernels.h"
 
@@ -42,40 +52,48 @@ namespace psg {
 
 constexpr int kTravWarps = 4;
 constexpr int kTravThreads = kTravWarps * 32;
-constexpr int kCandBuf = 256;     // one expanded chunk of 32 near-list entries
-constexpr int kStackCap = 512;    // DFS stack (entries: slot << 28 | node)
-constexpr int kStackSlack = 72;   // 9 levels x 7 growth of a single-entry descent
-constexpr int kP2PBuf = 128;      // buffered P2P source leaves (slot << 28 | node)
-constexpr uint32_t kNodeMask = (1u << 28) - 1;
-constexpr int kGroupBatch = 4;
+constexpr int kExpand = 16;               // near-list / stack entries opened per batch
+constexpr int kCandBuf = kExpand * 8;     // their children
+constexpr int kStackCap = 256;            // DFS stack entries (node, child mask)
+constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-entry descent
+constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
+constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
 
-struct TravArgs {
-    TreeView tv;
-    const float4* xyzm;
-    float* fx;
-    float* fy;
-    float* fz;
-    const uint32_t* ns_in;
-    uint32_t* ns_out;
-    unsigned long long ns_cap;
-    double* facc;          // [N][3] partial P2P sums for multi-flush leaves
-    Status* status;
-    float theta;
-    int level;
-    int debug;
+enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
+
+struct SmemCommon {
+    float4 cgeo[8];        // the group's children: centre + half width
+    float4 sgeo[32];       // staged candidates
+    float4 smp[32];
+    uint32_t slink[32];
+    uint32_t snode[32];
+    uint32_t near[32];     // per candidate: children it is NOT separated from
+    uint32_t dbg_m2l[8];
+    float acc[8][3][32];   // per child, per component, per lane M2L partial sums
+    uint32_t cand_node[kCandBuf];
+    uint8_t cand_mask[kCandBuf];
+    uint8_t pair[32 * 8];  // (candidate << 3 | child) tests of the staged chunk
 };
 
-struct WarpSmem {
-    float4 cgeo[8];
-    uint4 cinfo[8];
-    uint32_t cand[kCandBuf];
-    uint32_t stk[kStackCap];
-    uint32_t p2p[kP2PBuf];
+struct SmemInternal : SmemCommon {
+    uint32_t ns_cnt[8];
+    unsigned long long ns_next, ns_end;
 };
 
-struct M2LAcc {
-    float v[8][3];
+struct SmemLeaf : SmemCommon {
+    uint32_t dbg_p2p[8];
+    uint32_t p2p_fill[8];
+    uint32_t p2p_head[8];
+    uint32_t chunk_next, chunk_end;
+    uint32_t p2p[8][kP2PChunk];
+    uint32_t stk_node[kStackCap];
+    uint8_t stk_mask[kStackCap];
 };
+
+template <int MODE>
+struct SmemOf { using T = SmemInternal; };
+template <>
+struct SmemOf<MODE_LEAF> { using T = SmemLeaf; };
 
 __device__ __forceinline__ void m2l_field(float dx, float dy, float dz, float d2, float4 mp,
                                           float& fx, float& fy, float& fz) {
@@ -87,391 +105,481 @@ __device__ __forceinline__ void m2l_field(float dx, float dy, float dz, float d2
     const float ir5 = ir3 * inv2;
     const float mdr = fmaf(mp.y, dx, fmaf(mp.z, dy, mp.w * dz));
     const float a = fmaf(mp.x, ir3, -3.0f * mdr * ir5);
-    const float b = ir3;
-    fx = fmaf(dx, a, mp.y * b);
-    fy = fmaf(dy, a, mp.z * b);
-    fz = fmaf(dz, a, mp.w * b);
+    fx = fmaf(dx, a, mp.y * ir3);
+    fy = fmaf(dy, a, mp.z * ir3);
+    fz = fmaf(dz, a, mp.w * ir3);
 }
 
-__device__ __forceinline__ void acc_add_dyn(M2LAcc& acc, uint32_t slot, float fx, float fy,
-                                            float fz) {
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        if ((uint32_t)q == slot) {
-            acc.v[q][0] += fx;
-            acc.v[q][1] += fy;
-            acc.v[q][2] += fz;
-        }
-    }
-}
-
-// Direct sums of the buffered P2P pairs (polesitter.h:1279-1449 with rsqrt):
-// for every leaf target slot and each of its particles, lanes walk the
-// buffered source leaves of that slot; the warp total goes to facc (or, on
-// the last flush, into the returned per-particle value via `fin`).
-__device__ void p2p_flush(const TravArgs& A, WarpSmem& sm, uint32_t np, uint32_t leaf_slots,
-                          bool last, bool& flushed_before, const float4* Lslot) {
+// Spill slot q's staged P2P sources as one chunk, chained to the leaf's
+// previous chunk.  Warp-collective; chunk ids come from a per-warp pool.
+__device__ __noinline__ void flush_p2p(SmemLeaf& sm, uint32_t q, P2PStore st, Status* status) {
     const uint32_t lane = lane_id();
-    const TreeView& tv = A.tv;
-#pragma unroll 1
-    for (uint32_t sl = 0; sl < 8; ++sl) {
-        if (!((leaf_slots >> sl) & 1u)) continue;
-        const uint4 ui = sm.cinfo[sl];
-        const uint32_t ustart = ui.x, ucnt = ui.y;
-#pragma unroll 1
-        for (uint32_t ti = 0; ti < ucnt; ++ti) {
-            const float4 t = A.xyzm[ustart + ti];
-            float ax = 0.f, ay = 0.f, az = 0.f;
-            for (uint32_t e = lane; e < np; e += 32) {
-                const uint32_t ent = sm.p2p[e];
-                if ((ent >> 28) != sl) continue;
-                const uint4 si = tv.info[ent & kNodeMask];
-                for (uint32_t j = 0; j < si.y; ++j) {
-                    const float4 p = A.xyzm[si.x + j];
-                    const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
-                    const float inv = rsqrtf(r2);
-                    const float f = p.w * (inv * inv * inv);
-                    ax = fmaf(dx, f, ax);
-                    ay = fmaf(dy, f, ay);
-                    az = fmaf(dz, f, az);
-                }
-            }
-            double sx = warp_sum((double)ax);
-            double sy = warp_sum((double)ay);
-            double sz = warp_sum((double)az);
-            const size_t gi = (size_t)ustart + ti;
-            if (lane == 0) {
-                if (flushed_before) {
-                    sx += A.facc[3 * gi + 0];
-                    sy += A.facc[3 * gi + 1];
-                    sz += A.facc[3 * gi + 2];
-                }
-                if (last) {
-                    const float4 L = Lslot[sl];
-                    const double m = (double)t.w;
-                    A.fx[gi] = (float)(m * ((double)L.y + sx));
-                    A.fy[gi] = (float)(m * ((double)L.z + sy));
-                    A.fz[gi] = (float)(m * ((double)L.w + sz));
-                } else {
-                    A.facc[3 * gi + 0] = sx;
-                    A.facc[3 * gi + 1] = sy;
-                    A.facc[3 * gi + 2] = sz;
-                }
-            }
+    const uint32_t fill = sm.p2p_fill[q];
+    if (fill == 0) return;
+    if (sm.chunk_next >= sm.chunk_end) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(&status->p2p_chunks, kChunkPool);
+        c = __shfl_sync(0xFFFFFFFFu, c, 0);
+        __syncwarp();
+        if (lane == 0) {
+            sm.chunk_next = c;
+            sm.chunk_end = c + kChunkPool;
         }
+        __syncwarp();
     }
-    if (!last) flushed_before = true;
+    const uint32_t c = sm.chunk_next;
+    const bool ok = c < st.cap_chunks;
+    if (ok) {
+        if (lane < fill) st.src[(size_t)c * kP2PChunk + lane] = sm.p2p[q][lane];
+        if (lane == 0) {
+            st.next[c] = sm.p2p_head[q];
+            st.cnt[c] = fill;
+        }
+    } else if (lane == 0) {
+        set_err(status, PSG_ERR_P2P_OVERFLOW);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        sm.chunk_next = c + 1;
+        if (ok) sm.p2p_head[q] = c;
+        sm.p2p_fill[q] = 0;
+    }
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_traverse(TravArgs A) {
-    __shared__ WarpSmem smem[kTravWarps];
+// Direct sum of source leaf `s` on target particle t (polesitter.h:1424-1444
+// with rsqrt), optionally Kahan-compensated.
+__device__ __forceinline__ void p2p_leaf(const float4* __restrict__ xyzm, uint4 si, float4 t,
+                                         bool kahan, float& ax, float& ay, float& az, float& cx,
+                                         float& cy, float& cz) {
+    for (uint32_t j = 0; j < si.y; ++j) {
+        const float4 p = xyzm[si.x + j];
+        const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
+        const float inv = rsqrtf(r2);
+        const float f = p.w * (inv * inv * inv);
+        if (kahan) {
+            const float yx = __fsub_rn(__fmul_rn(dx, f), cx);
+            const float yy = __fsub_rn(__fmul_rn(dy, f), cy);
+            const float yz = __fsub_rn(__fmul_rn(dz, f), cz);
+            const float tx = __fadd_rn(ax, yx);
+            const float ty = __fadd_rn(ay, yy);
+            const float tz = __fadd_rn(az, yz);
+            cx = __fsub_rn(__fsub_rn(tx, ax), yx);
+            cy = __fsub_rn(__fsub_rn(ty, ay), yy);
+            cz = __fsub_rn(__fsub_rn(tz, az), yz);
+            ax = tx;
+            ay = ty;
+            az = tz;
+        } else {
+            ax = fmaf(dx, f, ax);
+            ay = fmaf(dy, f, ay);
+            az = fmaf(dz, f, az);
+        }
+    }
+}
+
+template <int MODE, bool DEBUG>
+__global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
+    using Smem = typename SmemOf<MODE>::T;
+    __shared__ Smem smem[kTravWarps];
     const uint32_t lane = lane_id();
     const uint32_t lt_mask = lanemask_lt();
-    WarpSmem& sm = smem[threadIdx.x >> 5];
+    Smem& sm = smem[threadIdx.x >> 5];
     const TreeView& tv = A.tv;
-    const int k = A.level;
+    Status* status = A.status;
+    if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
     const float theta2 = __fmul_rn(A.theta, A.theta);
-    const uint32_t gbase = tv.lvl_base[k - 1];
-    const uint32_t ngroups = A.status->lvl_count[k - 1];
-    if (A.status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
+
+    // group index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
+    // the nodes at depths 0..9, level after level
+    uint32_t cum[kMaxDepth + 1];
+    uint32_t total = 0;
+    uint32_t* work;
+    if (MODE == MODE_INTERNAL) {
+        total = status->lvl_count[A.level - 1];
+        work = &status->work[A.level];
+    } else {
+#pragma unroll
+        for (int d = 0; d < kMaxDepth; ++d) {
+            cum[d] = total;
+            total += status->lvl_count[d];
+        }
+        cum[kMaxDepth] = total;
+        work = &status->work[0];
+    }
+    if (lane == 0) {
+        if constexpr (MODE == MODE_INTERNAL) {
+            sm.ns_next = 0;
+            sm.ns_end = 0;
+        } else {
+            sm.chunk_next = 0;
+            sm.chunk_end = 0;
+        }
+    }
+    __syncwarp();
+    const uint32_t batch = MODE == MODE_INTERNAL ? 4u : 8u;
 
     for (;;) {
         uint32_t g0 = 0;
-        if (lane == 0) g0 = atomicAdd(&A.status->work[k], (uint32_t)kGroupBatch);
+        if (lane == 0) g0 = atomicAdd(work, batch);
         g0 = __shfl_sync(0xFFFFFFFFu, g0, 0);
-        if (g0 >= ngroups) break;
+        if (g0 >= total) break;
 #pragma unroll 1
-        for (uint32_t g = g0; g < g0 + kGroupBatch && g < ngroups; ++g) {
-            const uint32_t pid = gbase + g;
-            const uint4 pinf = tv.info[pid];
-            const uint32_t nc = flags_nchild(pinf.w);
+        for (uint32_t g = g0; g < g0 + batch && g < total; ++g) {
+            uint32_t pid, dp;
+            if (MODE == MODE_INTERNAL) {
+                dp = A.level - 1;
+                pid = tv.lvl_base[dp] + g;
+            } else {
+                dp = 0;
+                uint32_t off = 0;
+#pragma unroll
+                for (int d = 1; d < kMaxDepth; ++d) {
+                    if (g >= cum[d]) {
+                        dp = d;
+                        off = cum[d];
+                    }
+                }
+                pid = tv.lvl_base[dp] + (g - off);
+            }
+            const uint32_t plink = tv.link[pid];
+            const uint32_t nc = plink >> 28;
             if (nc == 0) continue;
-            const uint32_t fc = pinf.z;
+            const uint32_t fc = plink & kLinkMask;
+            uint32_t cl = 0;
             if (lane < nc) {
                 sm.cgeo[lane] = tv.geo[fc + lane];
-                sm.cinfo[lane] = tv.info[fc + lane];
+                cl = tv.link[fc + lane];
             }
-            __syncwarp();
-            // slot masks: which children are targets, which are leaves
-            uint32_t leaf_mask = 0, tgt_mask = 0;
-            for (uint32_t q = 0; q < nc; ++q) {
-                const bool lf = flags_nchild(sm.cinfo[q].w) == 0;
-                leaf_mask |= (uint32_t)lf << q;
-            }
-            tgt_mask = (k == 1) ? leaf_mask : ((1u << nc) - 1u);
-            const uint32_t int_mask = tgt_mask & ~leaf_mask;
+            const uint32_t leaf_mask =
+                __ballot_sync(0xFFFFFFFFu, lane < nc && (cl >> 28) == 0) & 0xFFu;
+            const uint32_t tgt_mask =
+                MODE == MODE_INTERNAL ? (((1u << nc) - 1u) & ~leaf_mask) : leaf_mask;
             if (tgt_mask == 0) continue;
-            const float4 Lp = tv.lt[pid];
-
-            // candidate count and near-list reservation for internal children
-            const uint32_t* nsl = nullptr;
-            uint32_t nsn = 0, cand_total = 1;
-            if (k >= 3) {
-                nsl = A.ns_in + tv.ns_off[pid];
-                nsn = tv.ns_cnt[pid];
-                uint32_t c = 0;
-                for (uint32_t e = lane; e < nsn; e += 32) {
-                    const uint32_t nch = flags_nchild(tv.info[nsl[e]].w);
-                    c += nch ? nch : 1u;
+            if (lane < 8) {
+                if (DEBUG) sm.dbg_m2l[lane] = 0;
+                if constexpr (MODE == MODE_INTERNAL) {
+                    sm.ns_cnt[lane] = 0;
+                } else {
+                    sm.p2p_fill[lane] = 0;
+                    sm.p2p_head[lane] = kNone;
+                    if (DEBUG) sm.dbg_p2p[lane] = 0;
                 }
-                cand_total = warp_sum(c);
             }
-            const uint32_t n_int = __popc(int_mask);
+            for (uint32_t m = tgt_mask; m; m &= m - 1) {
+                const uint32_t q = __ffs(m) - 1;
+                sm.acc[q][0][lane] = 0.f;
+                sm.acc[q][1][lane] = 0.f;
+                sm.acc[q][2][lane] = 0.f;
+            }
+            const float4 Lp = tv.lt[pid];
+            const bool root_only = dp <= 1;
+            const uint32_t* nsl = nullptr;
+            uint32_t nsn = 0;
+            if (!root_only) {
+                nsl = A.ns + tv.ns_off[pid];
+                nsn = tv.ns_cnt[pid];
+            }
+            // MODE_INTERNAL: reserve n_int x |cand| near-list entries
+            uint32_t cand_total = 1;
             unsigned long long ns_base = 0;
             bool ns_ok = true;
-            if (n_int && cand_total) {
-                unsigned long long need = (unsigned long long)n_int * cand_total;
-                if (lane == 0) ns_base = atomicAdd(&A.status->ns_used[k], need);
-                ns_base = __shfl_sync(0xFFFFFFFFu, ns_base, 0);
-                if (ns_base + need > A.ns_cap) {
-                    ns_ok = false;
-                    if (lane == 0) set_err(A.status, PSG_ERR_NS_OVERFLOW);
+            if constexpr (MODE == MODE_INTERNAL) {
+                if (!root_only) {
+                    uint32_t c = 0;
+                    for (uint32_t e = lane; e < nsn; e += 32) {
+                        const uint32_t nch = tv.link[nsl[e]] >> 28;
+                        c += nch ? nch : 1u;
+                    }
+                    cand_total = warp_sum(c);
                 }
-            }
-            uint32_t ns_cnt[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) ns_cnt[q] = 0;
-            M2LAcc acc;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) acc.v[q][0] = acc.v[q][1] = acc.v[q][2] = 0.f;
-            uint32_t dbg_m2l[8], dbg_p2p[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) dbg_m2l[q] = dbg_p2p[q] = 0;
-            uint32_t ssize = 0, np = 0;
-            bool flushed = false;
-
-            // ---------- DFS step over the stack (leaf targets vs internal s) ----------
-            auto dfs_step = [&]() {
-                int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
-                uint32_t kp = (uint32_t)min(32, min((int)ssize, max(1, room)));
-                uint32_t ent = 0;
-                const bool act = lane < kp;
-                if (act) ent = sm.stk[ssize - kp + lane];
-                ssize -= kp;
+                const unsigned long long need =
+                    (unsigned long long)__popc(tgt_mask) * cand_total;
                 __syncwarp();
-                const uint32_t slot = ent >> 28;
-                uint4 sinf = make_uint4(0, 0, 0, 0);
-                if (act) sinf = tv.info[ent & kNodeMask];
-                const uint32_t snch = act ? flags_nchild(sinf.w) : 0u;
-                const float4 ug = sm.cgeo[slot];
-#pragma unroll 1
-                for (uint32_t c = 0; c < 8; ++c) {
-                    const bool v = c < snch;
-                    if (!__any_sync(0xFFFFFFFFu, v)) break;
-                    bool sep = false, p2p = false, push = false;
-                    uint32_t sc = 0;
-                    if (v) {
-                        sc = sinf.z + c;
-                        const float4 sg = tv.geo[sc];
-                        float dx, dy, dz, d2;
-                        sep = mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w,
-                                            theta2, dx, dy, dz, d2);
-                        if (sep) {
-                            float fx, fy, fz;
-                            m2l_field(dx, dy, dz, d2, tv.mp[sc], fx, fy, fz);
-                            acc_add_dyn(acc, slot, fx, fy, fz);
-                        } else if (flags_nchild(tv.info[sc].w) == 0) {
-                            p2p = true;
-                        } else {
-                            push = true;
-                        }
-                    }
-                    if (A.debug) {
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            dbg_m2l[q] += __popc(__ballot_sync(0xFFFFFFFFu, sep && slot == (uint32_t)q));
-                            dbg_p2p[q] += __popc(__ballot_sync(0xFFFFFFFFu, p2p && slot == (uint32_t)q));
-                        }
-                    }
-                    const uint32_t pm = __ballot_sync(0xFFFFFFFFu, p2p);
-                    if (pm) {
-                        if (np + __popc(pm) > (uint32_t)kP2PBuf) {
-                            p2p_flush(A, sm, np, tgt_mask & leaf_mask, false, flushed, nullptr);
-                            np = 0;
-                        }
-                        if (p2p) sm.p2p[np + __popc(pm & lt_mask)] = (slot << 28) | sc;
-                        np += __popc(pm);
-                    }
-                    const uint32_t qm = __ballot_sync(0xFFFFFFFFu, push);
-                    if (qm) {
-                        if (ssize + __popc(qm) > (uint32_t)kStackCap) {
-                            if (lane == 0) set_err(A.status, PSG_ERR_STACK);
-                        } else {
-                            if (push) sm.stk[ssize + __popc(qm & lt_mask)] = (slot << 28) | sc;
-                            ssize += __popc(qm);
-                        }
+                if (need && sm.ns_next + need > sm.ns_end) {
+                    const unsigned long long take = need > kNsPool ? need : kNsPool;
+                    unsigned long long b = 0;
+                    if (lane == 0) b = atomicAdd(&status->ns_used[0], take);
+                    b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                    __syncwarp();
+                    if (lane == 0) {
+                        sm.ns_next = b;
+                        sm.ns_end = b + take;
                     }
                     __syncwarp();
                 }
-                if (A.debug && lane == 0) atomicMax(&A.status->max_stack, ssize);
-            };
+                ns_base = sm.ns_next;
+                ns_ok = ns_base + need <= A.ns_cap;
+                if (!ns_ok && lane == 0) set_err(status, PSG_ERR_NS_OVERFLOW);
+                __syncwarp();
+                if (lane == 0) sm.ns_next = ns_base + need;
+            }
+            __syncwarp();
 
-            // ---------- phase A: candidates x children ----------
-            const uint32_t n_chunks = (k >= 3) ? (nsn + 31) / 32 : 1u;
-#pragma unroll 1
-            for (uint32_t ch = 0; ch < n_chunks; ++ch) {
-                uint32_t tot;
-                if (k >= 3) {
-                    const uint32_t e = ch * 32 + lane;
-                    uint32_t s0 = 0, c = 0, fcs = 0;
-                    bool lf = false;
-                    if (e < nsn) {
+            uint32_t ssize = 0, e0 = 0;
+            bool root_pending = root_only;
+            for (;;) {
+                // ---- next batch of candidates into cand[0, tot) ----
+                uint32_t tot = 0;
+                bool from_dfs = false;
+                if (root_pending) {
+                    if (lane == 0) {
+                        sm.cand_node[0] = 0;  // the root
+                        sm.cand_mask[0] = (uint8_t)tgt_mask;
+                    }
+                    tot = 1;
+                    root_pending = false;
+                } else if (e0 < nsn && (MODE == MODE_INTERNAL ||
+                                        ssize <= (uint32_t)(kStackCap - kStackSlack - kCandBuf))) {
+                    const uint32_t e = e0 + lane;
+                    uint32_t s0 = 0, c = 0, link = 0;
+                    if (lane < (uint32_t)kExpand && e < nsn) {
                         s0 = nsl[e];
-                        const uint4 si = tv.info[s0];
-                        const uint32_t nch = flags_nchild(si.w);
-                        lf = nch == 0;
-                        c = lf ? 1u : nch;
-                        fcs = si.z;
+                        link = tv.link[s0];
+                        const uint32_t nch = link >> 28;
+                        c = nch ? nch : 1u;
                     }
                     const uint32_t inc = warp_incl_scan(c);
                     tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
                     const uint32_t ex = inc - c;
-                    if (lf) sm.cand[ex] = s0;
-                    else for (uint32_t q = 0; q < c; ++q) sm.cand[ex + q] = fcs + q;
+                    const bool lf = (link >> 28) == 0;
+                    for (uint32_t i = 0; i < c; ++i) {
+                        sm.cand_node[ex + i] = lf ? s0 : (link & kLinkMask) + i;
+                        sm.cand_mask[ex + i] = (uint8_t)tgt_mask;
+                    }
+                    e0 += kExpand;
+                } else if (MODE == MODE_LEAF && ssize > 0) {
+                    // pop entries (bounded so the stack cannot overflow), open them
+                    const int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
+                    const uint32_t kp =
+                        (uint32_t)min(kExpand, min((int)ssize, max(1, room)));
+                    const bool act = lane < kp;
+                    uint32_t node = 0, mask = 0;
+                    if constexpr (MODE == MODE_LEAF) {
+                        if (act) {
+                            node = sm.stk_node[ssize - kp + lane];
+                            mask = sm.stk_mask[ssize - kp + lane];
+                        }
+                    }
+                    __syncwarp();
+                    ssize -= kp;
+                    from_dfs = true;
+                    if (DEBUG && lane == 0) atomicAdd(&status->stat[PSG_STAT_DFS_STEPS], 1ull);
+                    const uint32_t link = act ? tv.link[node] : 0u;
+                    const uint32_t nch = link >> 28;
+                    const uint32_t inc = warp_incl_scan(nch);
+                    tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+                    const uint32_t ex = inc - nch;
+                    for (uint32_t i = 0; i < nch; ++i) {
+                        sm.cand_node[ex + i] = (link & kLinkMask) + i;
+                        sm.cand_mask[ex + i] = (uint8_t)mask;
+                    }
                 } else {
-                    tot = 1;
-                    if (lane == 0) sm.cand[0] = 0;  // the root
+                    break;
                 }
                 __syncwarp();
+
+                // ---- test the candidates, 32 at a time ----
 #pragma unroll 1
                 for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
-                    const uint32_t j = j0 + lane;
-                    const bool valid = j < tot;
-                    uint32_t s = 0;
-                    float4 sg = make_float4(0.f, 0.f, 0.f, 0.f), smp = sg;
-                    bool sleaf = false;
-                    if (valid) {
-                        s = sm.cand[j];
-                        sg = tv.geo[s];
-                        smp = tv.mp[s];
-                        sleaf = flags_nchild(tv.info[s].w) == 0;
+                    const uint32_t cnt = min(32u, tot - j0);
+                    uint32_t node = 0, mask = 0;
+                    if (lane < cnt) {
+                        node = sm.cand_node[j0 + lane];
+                        mask = sm.cand_mask[j0 + lane] & tgt_mask;
+                        sm.sgeo[lane] = tv.geo[node];
+                        sm.smp[lane] = tv.mp[node];
+                        sm.slink[lane] = tv.link[node];
+                        sm.near[lane] = 0;
                     }
-#pragma unroll
-                    for (uint32_t q = 0; q < 8; ++q) {
-                        if (!((tgt_mask >> q) & 1u)) continue;
-                        const float4 ug = sm.cgeo[q];
-                        float dx, dy, dz, d2;
-                        const bool sep = valid && mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y,
-                                                                sg.z, sg.w, theta2, dx, dy, dz, d2);
-                        if (sep) {
-                            float fx, fy, fz;
-                            m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
-                            acc.v[q][0] += fx;
-                            acc.v[q][1] += fy;
-                            acc.v[q][2] += fz;
-                        }
-                        const bool near = valid && !sep;
-                        if (A.debug) dbg_m2l[q] += __popc(__ballot_sync(0xFFFFFFFFu, sep));
-                        if ((int_mask >> q) & 1u) {
-                            const uint32_t nm = __ballot_sync(0xFFFFFFFFu, near);
-                            if (nm && ns_ok) {
-                                const uint32_t sub = __popc(int_mask & ((1u << q) - 1u));
-                                const unsigned long long off =
-                                    ns_base + (unsigned long long)sub * cand_total + ns_cnt[q];
-                                if (near) A.ns_out[off + __popc(nm & lt_mask)] = s;
-                            }
-                            ns_cnt[q] += __popc(nm);
-                        } else {
-                            const bool p2p = near && sleaf;
-                            const bool push = near && !sleaf;
-                            const uint32_t pm = __ballot_sync(0xFFFFFFFFu, p2p);
-                            if (A.debug) dbg_p2p[q] += __popc(pm);
-                            if (pm) {
-                                if (np + __popc(pm) > (uint32_t)kP2PBuf) {
-                                    p2p_flush(A, sm, np, tgt_mask & leaf_mask, false, flushed,
-                                              nullptr);
-                                    np = 0;
-                                }
-                                if (p2p) sm.p2p[np + __popc(pm & lt_mask)] = (q << 28) | s;
-                                np += __popc(pm);
-                            }
-                            const uint32_t qm = __ballot_sync(0xFFFFFFFFu, push);
-                            if (qm) {
-                                if (ssize + __popc(qm) > (uint32_t)kStackCap) {
-                                    if (lane == 0) set_err(A.status, PSG_ERR_STACK);
-                                } else {
-                                    if (push) sm.stk[ssize + __popc(qm & lt_mask)] = (q << 28) | s;
-                                    ssize += __popc(qm);
-                                }
+                    const uint32_t npair = __popc(mask);
+                    const uint32_t pinc = warp_incl_scan(npair);
+                    const uint32_t T = __shfl_sync(0xFFFFFFFFu, pinc, 31);
+                    uint32_t pe = pinc - npair;
+                    for (uint32_t m = mask; m; m &= m - 1) sm.pair[pe++] = (uint8_t)((lane << 3) | (__ffs(m) - 1));
+                    if (MODE == MODE_LEAF && DEBUG && lane == 0) {
+                        atomicAdd(&status->stat[from_dfs ? PSG_STAT_CHUNKS_DFS : PSG_STAT_CHUNKS_A], 1ull);
+                        atomicAdd(&status->stat[from_dfs ? PSG_STAT_TESTS_DFS : PSG_STAT_TESTS_A],
+                                  (unsigned long long)T);
+                        atomicAdd(&status->stat[PSG_STAT_LANES], (unsigned long long)cnt);
+                    }
+                    __syncwarp();
+#pragma unroll 1
+                    for (uint32_t p0 = 0; p0 < T; p0 += 32) {
+                        const uint32_t i = p0 + lane;
+                        if (i < T) {
+                            const uint32_t pr = sm.pair[i];
+                            const uint32_t j = pr >> 3, q = pr & 7u;
+                            const float4 ug = sm.cgeo[q];
+                            const float4 sg = sm.sgeo[j];
+                            float dx, dy, dz, d2;
+                            if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w,
+                                              theta2, dx, dy, dz, d2)) {
+                                float fx, fy, fz;
+                                m2l_field(dx, dy, dz, d2, sm.smp[j], fx, fy, fz);
+                                sm.acc[q][0][lane] += fx;
+                                sm.acc[q][1][lane] += fy;
+                                sm.acc[q][2][lane] += fz;
+                                if (DEBUG) atomicAdd(&sm.dbg_m2l[q], 1u);
+                            } else {
+                                atomicOr(&sm.near[j], 1u << q);
                             }
                         }
-                        __syncwarp();
                     }
-                    // leave room for the next sub-chunk's pushes (<= 8 slots x 32)
-                    while (ssize > (uint32_t)(kStackCap - kStackSlack - 8 * 32)) dfs_step();
+                    __syncwarp();
+                    // near candidates: near lists (internal targets), P2P
+                    // sources and descents (leaf targets)
+                    const uint32_t nb = lane < cnt ? sm.near[lane] : 0u;
+                    const bool sleaf = (sm.slink[lane] >> 28) == 0;
+                    const uint32_t s = node;
+                    if constexpr (MODE == MODE_INTERNAL) {
+                        const uint32_t near_any = __reduce_or_sync(0xFFFFFFFFu, nb);
+#pragma unroll 1
+                        for (uint32_t m = near_any; m; m &= m - 1) {
+                            const uint32_t q = __ffs(m) - 1;
+                            const bool nr = (nb >> q) & 1u;
+                            const uint32_t nm = __ballot_sync(0xFFFFFFFFu, nr);
+                            const uint32_t base = sm.ns_cnt[q];
+                            if (ns_ok && nr) {
+                                const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
+                                A.ns[ns_base + (unsigned long long)sub * cand_total + base +
+                                     __popc(nm & lt_mask)] = s;
+                            }
+                            __syncwarp();
+                            if (lane == 0) sm.ns_cnt[q] = base + __popc(nm);
+                            __syncwarp();
+                        }
+                    } else {
+                        const uint32_t pp_bits = sleaf ? nb : 0u;
+                        const uint32_t pp_any = __reduce_or_sync(0xFFFFFFFFu, pp_bits);
+#pragma unroll 1
+                        for (uint32_t m = pp_any; m; m &= m - 1) {
+                            const uint32_t q = __ffs(m) - 1;
+                            uint32_t rem = __ballot_sync(0xFFFFFFFFu, (pp_bits >> q) & 1u);
+                            if (DEBUG && lane == 0) sm.dbg_p2p[q] += __popc(rem);
+                            while (rem) {
+                                const uint32_t fill = sm.p2p_fill[q];
+                                const uint32_t space = kP2PChunk - fill;
+                                if (space == 0) {
+                                    flush_p2p(sm, q, A.p2p, status);
+                                    continue;
+                                }
+                                const uint32_t rank = __popc(rem & lt_mask);
+                                const bool take = ((rem >> lane) & 1u) && rank < space;
+                                if (take) sm.p2p[q][fill + rank] = s;
+                                const uint32_t taken = __ballot_sync(0xFFFFFFFFu, take);
+                                rem &= ~taken;
+                                __syncwarp();
+                                if (lane == 0) sm.p2p_fill[q] = fill + __popc(taken);
+                                __syncwarp();
+                            }
+                        }
+                        // internal near sources: open them later for these leaves
+                        const uint32_t push = sleaf ? 0u : nb;
+                        const uint32_t pm = __ballot_sync(0xFFFFFFFFu, push != 0);
+                        if (pm) {
+                            const uint32_t pos = ssize + __popc(pm & lt_mask);
+                            if (push && pos < (uint32_t)kStackCap) {
+                                sm.stk_node[pos] = s;
+                                sm.stk_mask[pos] = (uint8_t)push;
+                            }
+                            ssize += __popc(pm);
+                            if (ssize > (uint32_t)kStackCap) {
+                                if (lane == 0) set_err(status, PSG_ERR_STACK);
+                                ssize = kStackCap;
+                            }
+                        }
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
+                if (MODE == MODE_LEAF && DEBUG && lane == 0) atomicMax(&status->max_stack, ssize);
             }
-            // ---------- phase B: finish the leaf-target recursions ----------
-            while (ssize > 0) dfs_step();
 
-            // ---------- L2L / outputs ----------
-            __shared__ float4 s_L[kTravWarps][8];
-#pragma unroll
-            for (uint32_t q = 0; q < 8; ++q) {
-                if (!((tgt_mask >> q) & 1u)) continue;
-                const float ax = warp_sum(acc.v[q][0]);
-                const float ay = warp_sum(acc.v[q][1]);
-                const float az = warp_sum(acc.v[q][2]);
+            // ---- L2L, and for leaves L2P + P2P: per-child outputs ----
+#pragma unroll 1
+            for (uint32_t m = tgt_mask; m; m &= m - 1) {
+                const uint32_t q = __ffs(m) - 1;
+                const uint32_t u = fc + q;
+                const float ax = warp_sum(sm.acc[q][0][lane]);
+                const float ay = warp_sum(sm.acc[q][1][lane]);
+                const float az = warp_sum(sm.acc[q][2][lane]);
                 // L(u) = M2L(u) + L(parent)  (polesitter.h:1248-1250)
                 const float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
                                              __fadd_rn(az, Lp.w));
-                if (lane == 0) {
-                    const uint32_t u = fc + q;
-                    tv.lt[u] = L;
-                    s_L[threadIdx.x >> 5][q] = L;
-                    if ((int_mask >> q) & 1u) {
-                        const uint32_t sub = __popc(int_mask & ((1u << q) - 1u));
+                if (lane == 0) tv.lt[u] = L;
+                if constexpr (MODE == MODE_INTERNAL) {
+                    if (lane == 0) {
+                        const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
                         tv.ns_off[u] = (uint32_t)(ns_base + (unsigned long long)sub * cand_total);
-                        tv.ns_cnt[u] = ns_ok ? ns_cnt[q] : 0u;
+                        tv.ns_cnt[u] = ns_ok ? sm.ns_cnt[q] : 0u;
                     }
-                    if (A.debug) {
-                        tv.dbg_m2l[u] = dbg_m2l[q];
-                        tv.dbg_p2p[u] = dbg_p2p[q];
+                } else {
+                    // sources: the staged ones (lane < fill) and spilled chunks
+                    const uint4 ui = tv.info[u];
+                    const uint32_t fill = sm.p2p_fill[q];
+                    const uint32_t head = sm.p2p_head[q];
+                    uint4 si0 = make_uint4(0, 0, 0, 0);
+                    if (lane < fill) si0 = tv.info[sm.p2p[q][lane]];
+                    unsigned long long inter = 0;
+                    for (uint32_t ti = 0; ti < ui.y; ++ti) {
+                        const float4 t = A.xyzm[ui.x + ti];
+                        float ax2 = 0.f, ay2 = 0.f, az2 = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+                        p2p_leaf(A.xyzm, si0, t, A.kahan, ax2, ay2, az2, cx, cy, cz);
+                        if (DEBUG && ti == 0) inter += si0.y;
+                        for (uint32_t c = head; c != kNone; c = A.p2p.next[c]) {
+                            if (lane < A.p2p.cnt[c]) {
+                                const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
+                                p2p_leaf(A.xyzm, si, t, A.kahan, ax2, ay2, az2, cx, cy, cz);
+                                if (DEBUG && ti == 0) inter += si.y;
+                            }
+                        }
+                        // lane partials (compensated) summed in FP64
+                        const double sx = warp_sum((double)ax2 - (double)cx);
+                        const double sy = warp_sum((double)ay2 - (double)cy);
+                        const double sz = warp_sum((double)az2 - (double)cz);
+                        if (lane == 0) {
+                            const size_t gi = (size_t)ui.x + ti;
+                            const double mm = (double)t.w;
+                            A.fx[gi] = (float)(mm * ((double)L.y + sx));
+                            A.fy[gi] = (float)(mm * ((double)L.z + sy));
+                            A.fz[gi] = (float)(mm * ((double)L.w + sz));
+                        }
+                    }
+                    if (DEBUG) {
+                        inter = warp_sum(inter);
+                        if (lane == 0) {
+                            tv.dbg_p2p[u] = sm.dbg_p2p[q];
+                            atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS],
+                                      (unsigned long long)sm.dbg_p2p[q]);
+                            atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+                        }
                     }
                 }
-            }
-            __syncwarp();
-            if (tgt_mask & leaf_mask) {
-                p2p_flush(A, sm, np, tgt_mask & leaf_mask, true, flushed, s_L[threadIdx.x >> 5]);
-                np = 0;
-            }
-            if (A.debug && lane == 0) {
-                unsigned long long m = 0, p = 0;
-                for (int q = 0; q < 8; ++q) {
-                    m += dbg_m2l[q];
-                    p += dbg_p2p[q];
+                if (DEBUG && lane == 0) {
+                    tv.dbg_m2l[u] = sm.dbg_m2l[q];
+                    atomicAdd(&status->stat[PSG_STAT_M2L], (unsigned long long)sm.dbg_m2l[q]);
                 }
-                atomicAdd(&A.status->stat[PSG_STAT_M2L], m);
-                atomicAdd(&A.status->stat[PSG_STAT_P2P_PAIRS], p);
             }
             __syncwarp();
         }
     }
 }
 
-void launch_traverse_level(const TravLaunch& L, int level, const uint32_t* ns_in, uint32_t* ns_out,
-                           int grid, cudaStream_t st) {
-    TravArgs A;
-    A.tv = L.tv;
-    A.xyzm = L.xyzm;
-    A.fx = L.fx;
-    A.fy = L.fy;
-    A.fz = L.fz;
-    A.ns_in = ns_in;
-    A.ns_out = ns_out;
-    A.ns_cap = L.ns_cap;
-    A.facc = L.facc;
-    A.status = L.status;
-    A.theta = L.theta;
+void launch_traverse_internal(const TravArgs& args, int level, int grid, cudaStream_t st) {
+    TravArgs A = args;
     A.level = level;
-    A.debug = L.debug;
-    k_traverse<<<grid, kTravThreads, 0, st>>>(A);
+    if (A.debug) k_trav<MODE_INTERNAL, true><<<grid, kTravThreads, 0, st>>>(A);
+    else k_trav<MODE_INTERNAL, false><<<grid, kTravThreads, 0, st>>>(A);
+}
+
+void launch_traverse_leaves(const TravArgs& args, int grid, cudaStream_t st) {
+    if (args.debug) k_trav<MODE_LEAF, true><<<grid, kTravThreads, 0, st>>>(args);
+    else k_trav<MODE_LEAF, false><<<grid, kTravThreads, 0, st>>>(args);
 }
 
 int traverse_threads() { return kTravThreads; }
-const void* traverse_kernel_ptr() { return (const void*)k_traverse; }
+const void* traverse_kernel_ptr() { return (const void*)k_trav<MODE_LEAF, false>; }
+const void* traverse_internal_kernel_ptr() { return (const void*)k_trav<MODE_INTERNAL, false>; }
 
 }  // namespace psg

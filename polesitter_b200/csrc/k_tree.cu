@@ -272,27 +272,26 @@ __global__ void __launch_bounds__(256) k_tree_link(TreeView tv, const Status* st
         uint4 inf = tv.info[id];
         inf.w = (inf.w & ~0xFu) | (nch & 0xFu);
         tv.info[id] = inf;
+        tv.link[id] = nch ? ((inf.z & kLinkMask) | (nch << 28)) : 0u;
         tv.lt[id] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
-// P2M at every leaf, then M2M up the tree: the last child to finish
-// (arrival counter) combines its parent, so one launch covers all levels.
+// Upward pass, one launch per level from the deepest up: a leaf sums P2M
+// over its particles, an internal node adds its children's multipoles (M2M).
 // Operation order matches polesitter.h:978-1045 exactly (sequential sums over
 // the leaf's particles; children in octant order), every op rounded to nearest.
-__global__ void __launch_bounds__(256) k_upward(TreeView tv, const Status* status,
-                                                const float4* __restrict__ xyzm) {
+__global__ void __launch_bounds__(256) k_upward_level(TreeView tv, const Status* status,
+                                                      const float4* __restrict__ xyzm, int d) {
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
-    const uint32_t total = tv.lvl_base[kLevels];
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
-        int d = 0;
-        while (d < kMaxDepth && id >= tv.lvl_base[d + 1]) ++d;
-        if (id - tv.lvl_base[d] >= status->lvl_count[d]) continue;
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= status->lvl_count[d]) return;
+    const uint32_t id = tv.lvl_base[d] + r;
+    const float4 c = tv.geo[id];
+    const uint32_t link = tv.link[id];
+    float m0 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+    if ((link >> 28) == 0) {
         const uint4 inf = tv.info[id];
-        if (flags_nchild(inf.w) != 0) continue;
-        const float4 c = tv.geo[id];
-        float m0 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
         for (uint32_t k = 0; k < inf.y; ++k) {
             const float4 p = xyzm[inf.x + k];
             m0 = __fadd_rn(m0, p.w);
@@ -300,29 +299,18 @@ __global__ void __launch_bounds__(256) k_upward(TreeView tv, const Status* statu
             my = __fadd_rn(my, __fmul_rn(p.w, __fsub_rn(p.y, c.y)));
             mz = __fadd_rn(mz, __fmul_rn(p.w, __fsub_rn(p.z, c.z)));
         }
-        tv.mp[id] = make_float4(m0, mx, my, mz);
-        uint32_t node = id;
-        while (node != 0) {
-            const uint32_t par = tv.parent[node];
-            __threadfence();
-            const uint32_t nch = flags_nchild(__ldcg(&tv.info[par].w));
-            if (atomicAdd(&tv.arrive[par], 1u) != nch - 1) break;
-            __threadfence();
-            const float4 pc = __ldcg(&tv.geo[par]);
-            const uint32_t fc = __ldcg(&tv.info[par].z);
-            float p0 = 0.f, px = 0.f, py = 0.f, pz = 0.f;
-            for (uint32_t j = 0; j < nch; ++j) {
-                const float4 cm = __ldcg(&tv.mp[fc + j]);
-                const float4 cg = __ldcg(&tv.geo[fc + j]);
-                p0 = __fadd_rn(p0, cm.x);
-                px = __fadd_rn(px, __fadd_rn(cm.y, __fmul_rn(cm.x, __fsub_rn(cg.x, pc.x))));
-                py = __fadd_rn(py, __fadd_rn(cm.z, __fmul_rn(cm.x, __fsub_rn(cg.y, pc.y))));
-                pz = __fadd_rn(pz, __fadd_rn(cm.w, __fmul_rn(cm.x, __fsub_rn(cg.z, pc.z))));
-            }
-            tv.mp[par] = make_float4(p0, px, py, pz);
-            node = par;
+    } else {
+        const uint32_t fc = link & kLinkMask, nch = link >> 28;
+        for (uint32_t j = 0; j < nch; ++j) {
+            const float4 cm = tv.mp[fc + j];
+            const float4 cg = tv.geo[fc + j];
+            m0 = __fadd_rn(m0, cm.x);
+            mx = __fadd_rn(mx, __fadd_rn(cm.y, __fmul_rn(cm.x, __fsub_rn(cg.x, c.x))));
+            my = __fadd_rn(my, __fadd_rn(cm.z, __fmul_rn(cm.x, __fsub_rn(cg.y, c.y))));
+            mz = __fadd_rn(mz, __fadd_rn(cm.w, __fmul_rn(cm.x, __fsub_rn(cg.z, c.z))));
         }
     }
+    tv.mp[id] = make_float4(m0, mx, my, mz);
 }
 
 void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView tv,
@@ -337,7 +325,11 @@ void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView t
 
 void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int grid,
                    cudaStream_t st) {
-    k_upward<<<grid, 256, 0, st>>>(tv, status, xyzm);
+    (void)grid;
+    for (int d = kMaxDepth; d >= 0; --d) {
+        const int g = (int)((tv.lvl_cap[d] + 255) / 256);
+        k_upward_level<<<g, 256, 0, st>>>(tv, status, xyzm, d);
+    }
 }
 
 }  // namespace psg

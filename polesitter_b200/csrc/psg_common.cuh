@@ -24,6 +24,11 @@ namespace psg {
 constexpr int kMaxDepth = 10;   // PS_MAX_DEPTH, polesitter.h:882-883
 constexpr int kLevels = kMaxDepth + 1;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+// node link word: first child id in the low 28 bits, child count (0..8,
+// 0 = leaf) in the top 4
+constexpr uint32_t kLinkMask = (1u << 28) - 1u;
+// sources of a leaf's P2P list are stored in chained chunks of this size
+constexpr int kP2PChunk = 32;
 
 // info.w packing: nchild (4 bits) | depth << 4 (4 bits) | octant << 8 (3 bits)
 __host__ __device__ inline uint32_t pack_flags(uint32_t nchild, uint32_t depth,
@@ -43,6 +48,8 @@ struct TreeView {
     uint32_t* parent;
     uint32_t* arrive;      // upward-pass arrival counters
     uint32_t* cbase;       // first-child rank per node (tree link step)
+    uint32_t* link;        // first child | nchild << 28
+    uint32_t* p2p_head;    // per leaf: last chunk of its P2P source list
     uint32_t* ns_off;      // per node: offset of its near-source list
     uint32_t* ns_cnt;      // per node: length of its near-source list
     uint32_t* dbg_m2l;     // per node M2L pair count (debug builds of a tick)
@@ -59,9 +66,19 @@ struct Status {
     unsigned long long ns_cap;             // capacity of one near-list region
     uint32_t work[kLevels + 1];            // traversal work counters
     float bbox[4];                         // min, max, range, scale (prepare)
-    unsigned long long stat[8];            // debug totals (see PSG_STAT_*)
+    unsigned long long stat[16];           // debug totals (see PSG_STAT_*)
     uint32_t max_stack;                    // deepest DFS stack seen (debug)
+    uint32_t p2p_chunks;                   // P2P chunks used this tick
     uint32_t sort_tiles[4];                // onesweep tile tickets
+};
+
+// P2P source lists: chunk c holds cnt[c] source-leaf ids in
+// src[c * kP2PChunk ...] and links to the leaf's previous chunk via next[c].
+struct P2PStore {
+    uint32_t* src;
+    uint32_t* next;
+    uint32_t* cnt;
+    uint32_t cap_chunks;
 };
 
 // The four float ops of the MAC, each rounded to nearest and never fused,

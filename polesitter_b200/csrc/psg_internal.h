@@ -26,13 +26,20 @@ extern "C" {
 #define PSG_ERR_NS_OVERFLOW 0x2u  /* near-list region too small: regrow, rerun */
 #define PSG_ERR_STACK 0x4u        /* traversal stack bound violated */
 #define PSG_ERR_NODES 0x8u        /* tree level over its capacity */
-#define PSG_ERR_P2P_BUF 0x10u     /* P2P staging bound violated */
+#define PSG_ERR_P2P_OVERFLOW 0x10u /* P2P chunk store too small: regrow, rerun */
 
 /* debug statistics slots (Status.stat) */
 #define PSG_STAT_MAC 0
 #define PSG_STAT_M2L 1
 #define PSG_STAT_P2P_PAIRS 2
 #define PSG_STAT_P2P_INTER 3
+#define PSG_STAT_CHUNKS_A 4     /* candidate chunks from near lists / root */
+#define PSG_STAT_CHUNKS_DFS 5   /* candidate chunks from the DFS stack */
+#define PSG_STAT_TESTS_A 6      /* (candidate, child) MAC tests, first pass */
+#define PSG_STAT_TESTS_DFS 7    /* MAC tests inside the leaf descents */
+#define PSG_STAT_LANES 8        /* occupied candidate lanes over all chunks */
+#define PSG_STAT_GROUPS 9       /* groups processed (leaf mode) */
+#define PSG_STAT_DFS_STEPS 10
 
 /* Morton quantisation variants of polesitter.h:2013-2157 */
 #define PSG_MORTON_AVX2 0
@@ -87,6 +94,7 @@ const char* psg_last_error(void);
 #define PSG_OPT_MORTON_VARIANT 3
 #define PSG_OPT_TIMING 4         /* 1: time phases with CUDA events */
 #define PSG_OPT_USE_GRAPH 5      /* 1: replay calc_forces as a CUDA graph */
+#define PSG_OPT_KAHAN 6          /* 1: compensated FP32 sums in P2P */
 
 #ifdef __cplusplus
 }

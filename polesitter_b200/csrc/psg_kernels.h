@@ -9,6 +9,7 @@ namespace psg {
 
 struct TreeView;
 struct Status;
+struct P2PStore;
 
 // k_prepare.cu -- bbox + Morton codes (polesitter.h:1911-2170)
 void launch_prepare(const float* x, const float* y, const float* z, size_t n, float2* partial,
@@ -42,12 +43,15 @@ void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView t
 void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int grid,
                    cudaStream_t st);
 
-// k_traverse.cu -- fused M2L / L2L / L2P / P2P (polesitter.h:1050-1494)
-struct TravLaunch;
+// k_traverse.cu -- fused MAC / M2L / L2L, and L2P + P2P for the leaves
+// (polesitter.h:1050-1146, :1224-1254, :1258-1494)
+struct TravArgs;
 int traverse_threads();
 const void* traverse_kernel_ptr();
-void launch_traverse_level(const TravLaunch& L, int level, const uint32_t* ns_in,
-                           uint32_t* ns_out, int grid, cudaStream_t st);
+const void* traverse_internal_kernel_ptr();
+void launch_traverse_internal(const TravArgs& A, int level, int grid, cudaStream_t st);
+void launch_traverse_leaves(const TravArgs& A, int grid, cudaStream_t st);
+
 
 // k_direct.cu -- FP64 direct-sum forces for sampled targets (tests/accuracy.c:42-72)
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
@@ -58,16 +62,19 @@ void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, si
 #include "psg_common.cuh"
 
 namespace psg {
-struct TravLaunch {
+struct TravArgs {
     TreeView tv;
-    const float4* xyzm;
-    float* fx;
+    P2PStore p2p;       // spill chunks of P2P source lists longer than a chunk
+    uint32_t* ns;       // near lists of all levels
+    unsigned long long ns_cap;
+    const float4* xyzm;  // sorted particles
+    float* fx;          // output forces, sorted order
     float* fy;
     float* fz;
-    unsigned long long ns_cap;
-    double* facc;
     Status* status;
     float theta;
+    int level;
     int debug;
+    int kahan;          // compensated FP32 sums in P2P
 };
 }  // namespace psg

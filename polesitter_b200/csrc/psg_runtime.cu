@@ -42,7 +42,7 @@ static void note(const char* what, cudaError_t e) {
     } while (0)
 
 constexpr uint32_t kMagic = 0x50534732u;  // "PSG2"
-constexpr int kPhases = 8;
+constexpr int kPhases = 8;  // timing events
 enum Phase { PH_SORT = 0, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END, PH_BEGIN };
 
 struct Mirror {
@@ -56,6 +56,7 @@ struct State {
     int device;
     int sms;
     int trav_grid;
+    int trav_int_grid;
     size_t max_particles;
     float theta;
     int morton_variant;
@@ -67,15 +68,16 @@ struct State {
     SortBuffers sort;
     uint32_t* tree_tiles;
     TreeView tv;
-    uint32_t* ns[2];
+    uint32_t* ns;
     unsigned long long ns_cap;
-    double* facc;
+    P2PStore p2p;
+    int kahan;
     Status* d_status;
     Status* h_status;
     Mirror mir;
     cudaEvent_t ev[kPhases];
     float ms[kPhases];
-    unsigned long long stats[16];
+    unsigned long long stats[24];
     uint32_t last_nodes;
 };
 
@@ -87,12 +89,22 @@ static int grid_for(const State* s, size_t n, int per_block_items) {
 }
 
 static int alloc_ns(State* s, unsigned long long cap) {
-    for (int r = 0; r < 2; ++r) {
-        if (s->ns[r]) cudaFree(s->ns[r]);
-        s->ns[r] = nullptr;
-        PSG_ALLOC(s->ns[r], cap * sizeof(uint32_t));
-    }
+    if (s->ns) cudaFree(s->ns);
+    s->ns = nullptr;
+    PSG_ALLOC(s->ns, cap * sizeof(uint32_t));
     s->ns_cap = cap;
+    return PSG_OK;
+}
+
+static int alloc_p2p(State* s, uint32_t chunks) {
+    void* ps[3] = {s->p2p.src, s->p2p.next, s->p2p.cnt};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    s->p2p.src = s->p2p.next = s->p2p.cnt = nullptr;
+    PSG_ALLOC(s->p2p.src, (size_t)chunks * kP2PChunk * 4);
+    PSG_ALLOC(s->p2p.next, (size_t)chunks * 4);
+    PSG_ALLOC(s->p2p.cnt, (size_t)chunks * 4);
+    s->p2p.cap_chunks = chunks;
     return PSG_OK;
 }
 
@@ -136,8 +148,9 @@ static void free_state(State* s) {
     void* ps[] = {s->xyzm, s->ids, s->sort.key_a, s->sort.key_b, s->sort.val_a, s->sort.val_b,
                   s->sort.hist, s->sort.offs, s->sort.lookback, s->tree_tiles, s->tv.geo,
                   s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
-                  s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->ns[0], s->ns[1],
-                  s->facc, s->d_status};
+                  s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->tv.link,
+                  s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.next, s->p2p.cnt,
+                  s->d_status};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->h_status) cudaFreeHost(s->h_status);
@@ -194,15 +207,21 @@ static int init_state(State* s, size_t maxp, float theta) {
     PSG_ALLOC(s->tv.ns_cnt, nodes * 4);
     PSG_ALLOC(s->tv.dbg_m2l, nodes * 4);
     PSG_ALLOC(s->tv.dbg_p2p, nodes * 4);
-    PSG_ALLOC(s->facc, n * 3 * sizeof(double));
+    PSG_ALLOC(s->tv.link, nodes * 4);
+    PSG_ALLOC(s->tv.p2p_head, nodes * 4);
     PSG_ALLOC(s->d_status, sizeof(Status));
     PSG_CHECK(cudaMallocHost((void**)&s->h_status, sizeof(Status)));
     int r = alloc_ns(s, (unsigned long long)(n < 1024 ? 1024 : n) * 48ull);
+    if (r != PSG_OK) return r;
+    r = alloc_p2p(s, (uint32_t)(n < 4096 ? 4096 : n));
     if (r != PSG_OK) return r;
     int bps = 0;
     PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, traverse_kernel_ptr(),
                                                             traverse_threads(), 0));
     s->trav_grid = s->sms * (bps > 0 ? bps : 1);
+    PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, traverse_internal_kernel_ptr(),
+                                                            traverse_threads(), 0));
+    s->trav_int_grid = s->sms * (bps > 0 ? bps : 1);
     s->magic = kMagic;
     return PSG_OK;
 }
@@ -211,47 +230,62 @@ static void record(State* s, int ph) {
     if (s->timing) cudaEventRecord(s->ev[ph], s->stream);
 }
 
-// traversal of all levels; returns the status error bits (after sync)
+// traversal of all levels + P2P/L2P; regrows the near-list regions or the
+// P2P chunk store and reruns when a capacity flag comes back
 static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, float* fz,
-                         size_t n, uint32_t* err_out) {
-    for (int attempt = 0; attempt < 4; ++attempt) {
+                         uint32_t* err_out) {
+    for (int attempt = 0; attempt < 6; ++attempt) {
         PSG_CHECK(cudaMemsetAsync(&s->d_status->work[0], 0, sizeof(s->d_status->work), s->stream));
         PSG_CHECK(cudaMemsetAsync(&s->d_status->ns_used[0], 0, sizeof(s->d_status->ns_used),
                                   s->stream));
-        TravLaunch L;
-        L.tv = s->tv;
-        L.xyzm = xyzm;
-        L.fx = fx;
-        L.fy = fy;
-        L.fz = fz;
-        L.ns_cap = s->ns_cap;
-        L.facc = s->facc;
-        L.status = s->d_status;
-        L.theta = s->theta;
-        L.debug = s->debug;
-        for (int k = 1; k <= kMaxDepth; ++k)
-            launch_traverse_level(L, k, s->ns[(k - 1) & 1], s->ns[k & 1], s->trav_grid, s->stream);
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->p2p_chunks, 0, 4, s->stream));
+        TravArgs A;
+        A.tv = s->tv;
+        A.p2p = s->p2p;
+        A.ns = s->ns;
+        A.ns_cap = s->ns_cap;
+        A.status = s->d_status;
+        A.theta = s->theta;
+        A.level = 0;
+        A.debug = s->debug;
+        A.kahan = s->kahan;
+        A.xyzm = xyzm;
+        A.fx = fx;
+        A.fy = fy;
+        A.fz = fz;
+        for (int k = 2; k <= kMaxDepth; ++k)
+            launch_traverse_internal(A, k, s->trav_int_grid, s->stream);
+        record(s, PH_TRAV);
+        launch_traverse_leaves(A, s->trav_grid, s->stream);
         record(s, PH_END);
         PSG_CHECK(cudaGetLastError());
         PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
                                   cudaMemcpyDeviceToHost, s->stream));
         PSG_CHECK(cudaStreamSynchronize(s->stream));
-        uint32_t err = s->h_status->err;
-        if (!(err & PSG_ERR_NS_OVERFLOW)) {
+        const uint32_t err = s->h_status->err;
+        if (!(err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW))) {
             *err_out = err;
             return PSG_OK;
         }
-        unsigned long long need = 0;
-        for (int k = 0; k <= kLevels; ++k)
-            if (s->h_status->ns_used[k] > need) need = s->h_status->ns_used[k];
-        need = need + need / 4 + 1024;
-        if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
-        int r = alloc_ns(s, need);
-        if (r != PSG_OK) return r;
+        if (err & PSG_ERR_NS_OVERFLOW) {
+            unsigned long long need = s->h_status->ns_used[0];
+            need = need + need / 4 + 1024;
+            if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
+            int r = alloc_ns(s, need);
+            if (r != PSG_OK) return r;
+        }
+        if (err & PSG_ERR_P2P_OVERFLOW) {
+            unsigned long long need = s->h_status->p2p_chunks;
+            need = need + need / 4 + 1024;
+            if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
+            int r = alloc_p2p(s, (uint32_t)need);
+            if (r != PSG_OK) return r;
+        }
         PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, s->stream));
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->stat[0], 0, sizeof(s->d_status->stat), s->stream));
         if (s->timing) cudaEventRecord(s->ev[PH_UP], s->stream);
     }
-    note("near-list regrow", cudaErrorMemoryAllocation);
+    note("traversal capacity regrow", cudaErrorMemoryAllocation);
     return PSG_EOOM;
 }
 
@@ -304,16 +338,20 @@ static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, f
         launch_gather(s->sort.perm, x, y, z, m, id, n, s->xyzm, s->ids, g, st);
         launch_writeback(s->xyzm, s->ids, n, x, y, z, m, id, g, st);
         record(s, PH_GATHER);
-        const int gt = grid_for(s, s->tv.lvl_base[kLevels], 256);
+        const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
+        if (s->debug) {
+            PSG_CHECK(cudaMemsetAsync(s->tv.dbg_m2l, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
+            PSG_CHECK(cudaMemsetAsync(s->tv.dbg_p2p, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
+        }
         launch_tree(codes, n, s->tree_tiles, s->tv, s->d_status, cx, cy, cz, hw, gt, st);
         record(s, PH_TREE);
         launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
         record(s, PH_UP);
         PSG_CHECK(cudaGetLastError());
         uint32_t err = 0;
-        int r = run_traversal(s, s->xyzm, fx, fy, fz, n, &err);
+        int r = run_traversal(s, s->xyzm, fx, fy, fz, &err);
         if (r != PSG_OK) return r;
-        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_P2P_BUF)) {
+        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK)) {
             std::snprintf(g_err, sizeof(g_err), "device status error 0x%x", err);
             return PSG_EDEVICE;
         }
@@ -327,11 +365,13 @@ static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, f
         for (int i = 0; i < 8; ++i) s->stats[i] = s->h_status->stat[i];
         s->stats[8] = nodes;
         s->stats[9] = s->h_status->max_stack;
+        for (int i = 8; i < 16; ++i) s->stats[i + 8] = s->h_status->stat[i];
+        s->stats[10] = s->h_status->p2p_chunks;
         if (s->timing) {
-            const int order[6] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_END};
-            for (int i = 0; i + 1 < 6; ++i)
+            const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END};
+            for (int i = 0; i + 1 < 7; ++i)
                 cudaEventElapsedTime(&s->ms[i], s->ev[order[i]], s->ev[order[i + 1]]);
-            cudaEventElapsedTime(&s->ms[5], s->ev[PH_BEGIN], s->ev[PH_END]);
+            cudaEventElapsedTime(&s->ms[6], s->ev[PH_BEGIN], s->ev[PH_END]);
         }
     }
     if (any_host) {
@@ -456,6 +496,7 @@ int psg_set_option(void* mem, int key, double value) {
             s->morton_variant = (int)value;
             return PSG_OK;
         case PSG_OPT_TIMING: s->timing = value != 0.0; return PSG_OK;
+        case PSG_OPT_KAHAN: s->kahan = value != 0.0; return PSG_OK;
         default: return PSG_EINVAL;
     }
 }
@@ -463,7 +504,7 @@ int psg_set_option(void* mem, int key, double value) {
 int psg_get_stats(void* mem, uint64_t* out, size_t n_out) {
     State* s = static_cast<State*>(mem);
     if (!s || s->magic != psg::kMagic || !out) return PSG_EINVAL;
-    for (size_t i = 0; i < n_out && i < 16; ++i) out[i] = s->stats[i];
+    for (size_t i = 0; i < n_out && i < 24; ++i) out[i] = s->stats[i];
     return PSG_OK;
 }
 
