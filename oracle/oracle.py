@@ -54,6 +54,10 @@ class Oracle:
         lib.pso_tree.argtypes = [vp] + [vp] * 14
         lib.pso_p2p_list.argtypes = [vp, vp, vp]
         lib.pso_direct_f64.argtypes = [sz, vp, vp, vp, vp, vp, sz, vp, vp, vp]
+        lib.pso_p2m.argtypes = [sz, vp, vp, vp, vp, f32, f32, f32, vp]
+        lib.pso_m2l_pair.restype = C.c_int
+        lib.pso_m2l_pair.argtypes = [vp, vp, vp, f32, vp]
+        lib.pso_p2p_pair.argtypes = [vp] * 7 + [C.c_uint32] * 4
         self.lib = lib
 
     def morton_encode(self, x, y, z) -> int:
@@ -123,6 +127,24 @@ class Oracle:
                         accum_mode, want_tree, want_p2p)
         out.update(codes=codes, min=mn, max=mx, range=rg, root_c=float(c), root_hw=float(hw))
         return out
+
+    def p2m(self, x, y, z, m, centre=(0.0, 0.0, 0.0)):
+        a = [np.ascontiguousarray(v, np.float32) for v in (x, y, z, m)]
+        out = np.zeros(4, np.float32)
+        self.lib.pso_p2m(len(a[0]), *(_ptr(v) for v in a), *centre, _ptr(out))
+        return out
+
+    def m2l_pair(self, tgt_geo, src_geo, src_mp, theta):
+        tg = np.asarray(tgt_geo, np.float32)
+        sg = np.asarray(src_geo, np.float32)
+        sm = np.asarray(src_mp, np.float32)
+        out = np.zeros(4, np.float32)
+        hit = self.lib.pso_m2l_pair(_ptr(tg), _ptr(sg), _ptr(sm), theta, _ptr(out))
+        return bool(hit), out
+
+    def p2p_pair(self, p, t0, tn, s0, sn):
+        self.lib.pso_p2p_pair(_ptr(p.x), _ptr(p.y), _ptr(p.z), _ptr(p.mass), _ptr(p.fx),
+                              _ptr(p.fy), _ptr(p.fz), t0, tn, s0, sn)
 
     def direct_f64(self, p, targets=None):
         """FP64 direct-sum forces (tests/accuracy.c:42-72) for ``targets``

@@ -484,7 +484,7 @@ static void pso_dispatch(pso_ctx_t* c, uint32_t ti, int depth, int mt) {
  * sums reduced in lane order) and the remainder with the scalar formula
  * (:1424-1444: ((dx^2+dy^2)+dz^2)+eps, 1/sqrtf).  accum_mode 1 uses the
  * scalar formula for every source particle. */
-static void pso_p2p_pair(pso_ctx_t* c, const pso_node_t* t,
+static void pso_p2p_leaves(pso_ctx_t* c, const pso_node_t* t,
                          const pso_node_t* s, float* fx, float* fy,
                          float* fz) {
     for (uint32_t i = 0; i < t->count; ++i) {
@@ -595,7 +595,7 @@ PSO_API int pso_calc(void* h, size_t n, const uint32_t* codes, const float* x,
         const pso_node_t* t = &c->nodes[c->p2p_t[k]];
         const pso_node_t* s = &c->nodes[c->p2p_s[k]];
         c->p2p_interactions += (uint64_t)t->count * s->count;
-        pso_p2p_pair(c, t, s, fx, fy, fz);
+        pso_p2p_leaves(c, t, s, fx, fy, fz);
     }
     return 0;
 }
@@ -686,4 +686,77 @@ PSO_API void pso_direct_f64(size_t n, const float* x, const float* y,
         fy[k] = ay;
         fz[k] = az;
     }
+}
+
+/* ---------------------------------------------------------------------
+ * Single-pass helpers mirroring the hand-built node tests of the reference
+ * (tests/main.c:235-476, tests/accuracy.c:74-109).
+ * ------------------------------------------------------------------- */
+
+/* P2M of one leaf centred at (cx, cy, cz) (polesitter.h:978-1004) */
+PSO_API void pso_p2m(size_t n, const float* x, const float* y, const float* z,
+                     const float* m, float cx, float cy, float cz, float* out4) {
+    pso_node_t nd;
+    memset(&nd, 0, sizeof(nd));
+    nd.x = cx;
+    nd.y = cy;
+    nd.z = cz;
+    nd.count = (uint32_t)n;
+    pso_ctx_t c;
+    memset(&c, 0, sizeof(c));
+    c.x = x;
+    c.y = y;
+    c.z = z;
+    c.m = m;
+    c.nodes = &nd;
+    c.n_nodes = 1;
+    pso_upward(&c);
+    memcpy(out4, nd.mp, sizeof(nd.mp));
+}
+
+/* one MAC + M2L step on a (target, source) pair of leaves
+ * (polesitter.h:1056-1094); returns 1 when the pair was separated */
+PSO_API int pso_m2l_pair(const float* tgt_geo, const float* src_geo,
+                         const float* src_mp, float theta, float* out_local) {
+    pso_node_t nodes[2];
+    memset(nodes, 0, sizeof(nodes));
+    nodes[0].x = tgt_geo[0];
+    nodes[0].y = tgt_geo[1];
+    nodes[0].z = tgt_geo[2];
+    nodes[0].hw = tgt_geo[3];
+    nodes[1].x = src_geo[0];
+    nodes[1].y = src_geo[1];
+    nodes[1].z = src_geo[2];
+    nodes[1].hw = src_geo[3];
+    memcpy(nodes[1].mp, src_mp, 4 * sizeof(float));
+    pso_ctx_t c;
+    memset(&c, 0, sizeof(c));
+    c.nodes = nodes;
+    c.n_nodes = 2;
+    c.theta = theta;
+    pso_interact(&c, 0, 1);
+    free(c.p2p_t);
+    free(c.p2p_s);
+    memcpy(out_local, nodes[0].l_m2l, 4 * sizeof(float));
+    return nodes[0].m2l_cnt > 0;
+}
+
+/* direct leaf x leaf sum of particles [t0, t0+tn) from [s0, s0+sn)
+ * (polesitter.h:1279-1449), accumulated into fx, fy, fz */
+PSO_API void pso_p2p_pair(const float* x, const float* y, const float* z,
+                          const float* m, float* fx, float* fy, float* fz,
+                          uint32_t t0, uint32_t tn, uint32_t s0, uint32_t sn) {
+    pso_node_t nodes[2];
+    memset(nodes, 0, sizeof(nodes));
+    nodes[0].start = t0;
+    nodes[0].count = tn;
+    nodes[1].start = s0;
+    nodes[1].count = sn;
+    pso_ctx_t c;
+    memset(&c, 0, sizeof(c));
+    c.x = x;
+    c.y = y;
+    c.z = z;
+    c.m = m;
+    pso_p2p_leaves(&c, &nodes[0], &nodes[1], fx, fy, fz);
 }

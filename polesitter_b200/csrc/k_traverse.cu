@@ -17,29 +17,25 @@
 //
 // B200 formulation (target-major, no interaction lists in HBM).  The pairs
 // an internal target t hands to its children are its "near list" NS(t) =
-// the sources it was not separated from, so all children of an internal node
-// p (a "group") see the same candidates
+// the sources it was not separated from, so every child u of an internal
+// node p starts from the same candidates
 //   cand(p) = {root}                                         if depth(p) <= 1
 //   cand(p) = U_{s in NS(p)} (s leaf ? {s} : children(s))    otherwise.
-// One warp processes a group.  Candidates are staged 32 at a time in shared
-// memory together with the set of children each must be tested against; the
-// (candidate, child) pairs are flattened so every lane runs one MAC test per
-// step, and M2L results accumulate in lane-private shared-memory slots (one
-// per child), reduced once at the end.  Two kinds of launch:
+// One warp owns a parent p and takes its target children one after the
+// other; for a child u the lanes test 32 candidates at a time with the MAC,
+// accumulate M2L in registers, and deal with the near ones:
 //
-//  * MODE_INTERNAL, one per level k = 2..10: the internal children of the
-//    depth-(k-1) groups.  Non-separated candidates go to NS(u) in HBM for
-//    level k+1; L(u) = M2L(u) + L(p) is stored.
-//  * MODE_LEAF, one launch after all levels: the leaf children of every
-//    group.  A non-separated leaf candidate is a P2P source, staged in shared
-//    memory (chunks spill to HBM only past 32 sources); a non-separated
-//    internal candidate is the "t leaf" recursion -- it goes onto a DFS stack
-//    in shared memory whose entries carry the set of sibling leaves that
-//    still need it opened, so siblings share one descent.  At the end the
-//    warp finishes each leaf: L(u) = M2L(u) + L(p) and, per particle,
-//    F = m * (L(u) + sum of its P2P terms) -- written once, no atomics.
-//    Running all levels' leaves in one launch lets the long descents of
-//    shallow leaves overlap with everything else.
+//  * MODE_INTERNAL, one launch per level k = 2..10, targets = the internal
+//    children of the depth-(k-1) nodes: near candidates form NS(u) in HBM for
+//    level k+1, and L(u) = M2L(u) + L(p) is stored.
+//  * MODE_LEAF, one launch after all levels, targets = the leaf children of
+//    every node: a near leaf candidate is a P2P source (staged in shared
+//    memory, spilled to HBM chunks only past 32), a near internal candidate
+//    is the "t leaf" recursion and goes onto a DFS stack in shared memory
+//    that is drained the same way.  The warp then finishes u:
+//    L(u) = M2L(u) + L(p) and, per particle, F = m * (L(u) + its P2P sum) --
+//    written once, no atomics.  Running all levels' leaves in one launch lets
+//    the long descents of shallow leaves overlap with everything else.
 //
 // The MAC replays the reference's rounded float sequence exactly
 // (mac_separated), so the interaction set is identical, ties included.
@@ -52,42 +48,26 @@ namespace psg {
 
 constexpr int kTravWarps = 4;
 constexpr int kTravThreads = kTravWarps * 32;
-constexpr int kExpand = 16;               // near-list / stack entries opened per batch
-constexpr int kCandBuf = kExpand * 8;     // their children
-constexpr int kStackCap = 256;            // DFS stack entries (node, child mask)
+constexpr int kCandBuf = 256;             // children of 32 opened entries
+constexpr int kStackCap = 384;            // DFS stack (node ids)
 constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-entry descent
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
 
 enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
-struct SmemCommon {
-    float4 cgeo[8];        // the group's children: centre + half width
-    float4 sgeo[32];       // staged candidates
-    float4 smp[32];
-    uint32_t slink[32];
-    uint32_t snode[32];
-    uint32_t near[32];     // per candidate: children it is NOT separated from
-    uint32_t dbg_m2l[8];
-    float acc[8][3][32];   // per child, per component, per lane M2L partial sums
-    uint32_t cand_node[kCandBuf];
-    uint8_t cand_mask[kCandBuf];
-    uint8_t pair[32 * 8];  // (candidate << 3 | child) tests of the staged chunk
-};
-
-struct SmemInternal : SmemCommon {
-    uint32_t ns_cnt[8];
+struct SmemInternal {
+    float4 cgeo[8];  // the parent's children: centre + half width
+    uint32_t cand[kCandBuf];
     unsigned long long ns_next, ns_end;
 };
 
-struct SmemLeaf : SmemCommon {
-    uint32_t dbg_p2p[8];
-    uint32_t p2p_fill[8];
-    uint32_t p2p_head[8];
+struct SmemLeaf {
+    float4 cgeo[8];
+    uint32_t cand[kCandBuf];
+    uint32_t stk[kStackCap];
+    uint32_t p2p[kP2PChunk];
     uint32_t chunk_next, chunk_end;
-    uint32_t p2p[8][kP2PChunk];
-    uint32_t stk_node[kStackCap];
-    uint8_t stk_mask[kStackCap];
 };
 
 template <int MODE>
@@ -110,12 +90,11 @@ __device__ __forceinline__ void m2l_field(float dx, float dy, float dz, float d2
     fz = fmaf(dz, a, mp.w * ir3);
 }
 
-// Spill slot q's staged P2P sources as one chunk, chained to the leaf's
-// previous chunk.  Warp-collective; chunk ids come from a per-warp pool.
-__device__ __noinline__ void flush_p2p(SmemLeaf& sm, uint32_t q, P2PStore st, Status* status) {
+// Spill the staged P2P sources of the current leaf as one chunk chained to
+// its previous one.  Warp-collective; chunk ids come from a per-warp pool.
+__device__ __noinline__ uint32_t spill_p2p(SmemLeaf& sm, uint32_t fill, uint32_t head,
+                                           P2PStore st, Status* status) {
     const uint32_t lane = lane_id();
-    const uint32_t fill = sm.p2p_fill[q];
-    if (fill == 0) return;
     if (sm.chunk_next >= sm.chunk_end) {
         uint32_t c = 0;
         if (lane == 0) c = atomicAdd(&status->p2p_chunks, kChunkPool);
@@ -130,25 +109,22 @@ __device__ __noinline__ void flush_p2p(SmemLeaf& sm, uint32_t q, P2PStore st, St
     const uint32_t c = sm.chunk_next;
     const bool ok = c < st.cap_chunks;
     if (ok) {
-        if (lane < fill) st.src[(size_t)c * kP2PChunk + lane] = sm.p2p[q][lane];
+        if (lane < fill) st.src[(size_t)c * kP2PChunk + lane] = sm.p2p[lane];
         if (lane == 0) {
-            st.next[c] = sm.p2p_head[q];
+            st.next[c] = head;
             st.cnt[c] = fill;
         }
     } else if (lane == 0) {
         set_err(status, PSG_ERR_P2P_OVERFLOW);
     }
     __syncwarp();
-    if (lane == 0) {
-        sm.chunk_next = c + 1;
-        if (ok) sm.p2p_head[q] = c;
-        sm.p2p_fill[q] = 0;
-    }
+    if (lane == 0) sm.chunk_next = c + 1;
     __syncwarp();
+    return ok ? c : head;
 }
 
-// Direct sum of source leaf `s` on target particle t (polesitter.h:1424-1444
-// with rsqrt), optionally Kahan-compensated.
+// Direct sum of the particles of source leaf si on target particle t
+// (polesitter.h:1424-1444 with rsqrt), optionally Kahan-compensated.
 __device__ __forceinline__ void p2p_leaf(const float4* __restrict__ xyzm, uint4 si, float4 t,
                                          bool kahan, float& ax, float& ay, float& az, float& cx,
                                          float& cy, float& cz) {
@@ -191,7 +167,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
     const float theta2 = __fmul_rn(A.theta, A.theta);
 
-    // group index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
+    // parent index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
     // the nodes at depths 0..9, level after level
     uint32_t cum[kMaxDepth + 1];
     uint32_t total = 0;
@@ -257,22 +233,6 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             const uint32_t tgt_mask =
                 MODE == MODE_INTERNAL ? (((1u << nc) - 1u) & ~leaf_mask) : leaf_mask;
             if (tgt_mask == 0) continue;
-            if (lane < 8) {
-                if (DEBUG) sm.dbg_m2l[lane] = 0;
-                if constexpr (MODE == MODE_INTERNAL) {
-                    sm.ns_cnt[lane] = 0;
-                } else {
-                    sm.p2p_fill[lane] = 0;
-                    sm.p2p_head[lane] = kNone;
-                    if (DEBUG) sm.dbg_p2p[lane] = 0;
-                }
-            }
-            for (uint32_t m = tgt_mask; m; m &= m - 1) {
-                const uint32_t q = __ffs(m) - 1;
-                sm.acc[q][0][lane] = 0.f;
-                sm.acc[q][1][lane] = 0.f;
-                sm.acc[q][2][lane] = 0.f;
-            }
             const float4 Lp = tv.lt[pid];
             const bool root_only = dp <= 1;
             const uint32_t* nsl = nullptr;
@@ -281,7 +241,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 nsl = A.ns + tv.ns_off[pid];
                 nsn = tv.ns_cnt[pid];
             }
-            // MODE_INTERNAL: reserve n_int x |cand| near-list entries
+            // MODE_INTERNAL: reserve |cand| near-list entries per target child
             uint32_t cand_total = 1;
             unsigned long long ns_base = 0;
             bool ns_ok = true;
@@ -296,7 +256,6 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 }
                 const unsigned long long need =
                     (unsigned long long)__popc(tgt_mask) * cand_total;
-                __syncwarp();
                 if (need && sm.ns_next + need > sm.ns_end) {
                     const unsigned long long take = need > kNsPool ? need : kNsPool;
                     unsigned long long b = 0;
@@ -314,230 +273,171 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 if (!ns_ok && lane == 0) set_err(status, PSG_ERR_NS_OVERFLOW);
                 __syncwarp();
                 if (lane == 0) sm.ns_next = ns_base + need;
-            }
-            __syncwarp();
-
-            uint32_t ssize = 0, e0 = 0;
-            bool root_pending = root_only;
-            for (;;) {
-                // ---- next batch of candidates into cand[0, tot) ----
-                uint32_t tot = 0;
-                bool from_dfs = false;
-                if (root_pending) {
-                    if (lane == 0) {
-                        sm.cand_node[0] = 0;  // the root
-                        sm.cand_mask[0] = (uint8_t)tgt_mask;
-                    }
-                    tot = 1;
-                    root_pending = false;
-                } else if (e0 < nsn && (MODE == MODE_INTERNAL ||
-                                        ssize <= (uint32_t)(kStackCap - kStackSlack - kCandBuf))) {
-                    const uint32_t e = e0 + lane;
-                    uint32_t s0 = 0, c = 0, link = 0;
-                    if (lane < (uint32_t)kExpand && e < nsn) {
-                        s0 = nsl[e];
-                        link = tv.link[s0];
-                        const uint32_t nch = link >> 28;
-                        c = nch ? nch : 1u;
-                    }
-                    const uint32_t inc = warp_incl_scan(c);
-                    tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
-                    const uint32_t ex = inc - c;
-                    const bool lf = (link >> 28) == 0;
-                    for (uint32_t i = 0; i < c; ++i) {
-                        sm.cand_node[ex + i] = lf ? s0 : (link & kLinkMask) + i;
-                        sm.cand_mask[ex + i] = (uint8_t)tgt_mask;
-                    }
-                    e0 += kExpand;
-                } else if (MODE == MODE_LEAF && ssize > 0) {
-                    // pop entries (bounded so the stack cannot overflow), open them
-                    const int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
-                    const uint32_t kp =
-                        (uint32_t)min(kExpand, min((int)ssize, max(1, room)));
-                    const bool act = lane < kp;
-                    uint32_t node = 0, mask = 0;
-                    if constexpr (MODE == MODE_LEAF) {
-                        if (act) {
-                            node = sm.stk_node[ssize - kp + lane];
-                            mask = sm.stk_mask[ssize - kp + lane];
-                        }
-                    }
-                    __syncwarp();
-                    ssize -= kp;
-                    from_dfs = true;
-                    if (DEBUG && lane == 0) atomicAdd(&status->stat[PSG_STAT_DFS_STEPS], 1ull);
-                    const uint32_t link = act ? tv.link[node] : 0u;
-                    const uint32_t nch = link >> 28;
-                    const uint32_t inc = warp_incl_scan(nch);
-                    tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
-                    const uint32_t ex = inc - nch;
-                    for (uint32_t i = 0; i < nch; ++i) {
-                        sm.cand_node[ex + i] = (link & kLinkMask) + i;
-                        sm.cand_mask[ex + i] = (uint8_t)mask;
-                    }
-                } else {
-                    break;
-                }
                 __syncwarp();
-
-                // ---- test the candidates, 32 at a time ----
-#pragma unroll 1
-                for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
-                    const uint32_t cnt = min(32u, tot - j0);
-                    uint32_t node = 0, mask = 0;
-                    if (lane < cnt) {
-                        node = sm.cand_node[j0 + lane];
-                        mask = sm.cand_mask[j0 + lane] & tgt_mask;
-                        sm.sgeo[lane] = tv.geo[node];
-                        sm.smp[lane] = tv.mp[node];
-                        sm.slink[lane] = tv.link[node];
-                        sm.near[lane] = 0;
-                    }
-                    const uint32_t npair = __popc(mask);
-                    const uint32_t pinc = warp_incl_scan(npair);
-                    const uint32_t T = __shfl_sync(0xFFFFFFFFu, pinc, 31);
-                    uint32_t pe = pinc - npair;
-                    for (uint32_t m = mask; m; m &= m - 1) sm.pair[pe++] = (uint8_t)((lane << 3) | (__ffs(m) - 1));
-                    if (MODE == MODE_LEAF && DEBUG && lane == 0) {
-                        atomicAdd(&status->stat[from_dfs ? PSG_STAT_CHUNKS_DFS : PSG_STAT_CHUNKS_A], 1ull);
-                        atomicAdd(&status->stat[from_dfs ? PSG_STAT_TESTS_DFS : PSG_STAT_TESTS_A],
-                                  (unsigned long long)T);
-                        atomicAdd(&status->stat[PSG_STAT_LANES], (unsigned long long)cnt);
-                    }
-                    __syncwarp();
-#pragma unroll 1
-                    for (uint32_t p0 = 0; p0 < T; p0 += 32) {
-                        const uint32_t i = p0 + lane;
-                        if (i < T) {
-                            const uint32_t pr = sm.pair[i];
-                            const uint32_t j = pr >> 3, q = pr & 7u;
-                            const float4 ug = sm.cgeo[q];
-                            const float4 sg = sm.sgeo[j];
-                            float dx, dy, dz, d2;
-                            if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w,
-                                              theta2, dx, dy, dz, d2)) {
-                                float fx, fy, fz;
-                                m2l_field(dx, dy, dz, d2, sm.smp[j], fx, fy, fz);
-                                sm.acc[q][0][lane] += fx;
-                                sm.acc[q][1][lane] += fy;
-                                sm.acc[q][2][lane] += fz;
-                                if (DEBUG) atomicAdd(&sm.dbg_m2l[q], 1u);
-                            } else {
-                                atomicOr(&sm.near[j], 1u << q);
-                            }
-                        }
-                    }
-                    __syncwarp();
-                    // near candidates: near lists (internal targets), P2P
-                    // sources and descents (leaf targets)
-                    const uint32_t nb = lane < cnt ? sm.near[lane] : 0u;
-                    const bool sleaf = (sm.slink[lane] >> 28) == 0;
-                    const uint32_t s = node;
-                    if constexpr (MODE == MODE_INTERNAL) {
-                        const uint32_t near_any = __reduce_or_sync(0xFFFFFFFFu, nb);
-#pragma unroll 1
-                        for (uint32_t m = near_any; m; m &= m - 1) {
-                            const uint32_t q = __ffs(m) - 1;
-                            const bool nr = (nb >> q) & 1u;
-                            const uint32_t nm = __ballot_sync(0xFFFFFFFFu, nr);
-                            const uint32_t base = sm.ns_cnt[q];
-                            if (ns_ok && nr) {
-                                const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
-                                A.ns[ns_base + (unsigned long long)sub * cand_total + base +
-                                     __popc(nm & lt_mask)] = s;
-                            }
-                            __syncwarp();
-                            if (lane == 0) sm.ns_cnt[q] = base + __popc(nm);
-                            __syncwarp();
-                        }
-                    } else {
-                        const uint32_t pp_bits = sleaf ? nb : 0u;
-                        const uint32_t pp_any = __reduce_or_sync(0xFFFFFFFFu, pp_bits);
-#pragma unroll 1
-                        for (uint32_t m = pp_any; m; m &= m - 1) {
-                            const uint32_t q = __ffs(m) - 1;
-                            uint32_t rem = __ballot_sync(0xFFFFFFFFu, (pp_bits >> q) & 1u);
-                            if (DEBUG && lane == 0) sm.dbg_p2p[q] += __popc(rem);
-                            while (rem) {
-                                const uint32_t fill = sm.p2p_fill[q];
-                                const uint32_t space = kP2PChunk - fill;
-                                if (space == 0) {
-                                    flush_p2p(sm, q, A.p2p, status);
-                                    continue;
-                                }
-                                const uint32_t rank = __popc(rem & lt_mask);
-                                const bool take = ((rem >> lane) & 1u) && rank < space;
-                                if (take) sm.p2p[q][fill + rank] = s;
-                                const uint32_t taken = __ballot_sync(0xFFFFFFFFu, take);
-                                rem &= ~taken;
-                                __syncwarp();
-                                if (lane == 0) sm.p2p_fill[q] = fill + __popc(taken);
-                                __syncwarp();
-                            }
-                        }
-                        // internal near sources: open them later for these leaves
-                        const uint32_t push = sleaf ? 0u : nb;
-                        const uint32_t pm = __ballot_sync(0xFFFFFFFFu, push != 0);
-                        if (pm) {
-                            const uint32_t pos = ssize + __popc(pm & lt_mask);
-                            if (push && pos < (uint32_t)kStackCap) {
-                                sm.stk_node[pos] = s;
-                                sm.stk_mask[pos] = (uint8_t)push;
-                            }
-                            ssize += __popc(pm);
-                            if (ssize > (uint32_t)kStackCap) {
-                                if (lane == 0) set_err(status, PSG_ERR_STACK);
-                                ssize = kStackCap;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
-                if (MODE == MODE_LEAF && DEBUG && lane == 0) atomicMax(&status->max_stack, ssize);
             }
 
-            // ---- L2L, and for leaves L2P + P2P: per-child outputs ----
+            uint32_t sub = 0;  // rank of the target child among the targets
 #pragma unroll 1
-            for (uint32_t m = tgt_mask; m; m &= m - 1) {
-                const uint32_t q = __ffs(m) - 1;
+            for (uint32_t tm = tgt_mask; tm; tm &= tm - 1, ++sub) {
+                const uint32_t q = __ffs(tm) - 1;
                 const uint32_t u = fc + q;
-                const float ax = warp_sum(sm.acc[q][0][lane]);
-                const float ay = warp_sum(sm.acc[q][1][lane]);
-                const float az = warp_sum(sm.acc[q][2][lane]);
+                const float4 ug = sm.cgeo[q];
+                float ax = 0.f, ay = 0.f, az = 0.f;
+                uint32_t n_near = 0;   // MODE_INTERNAL: entries of NS(u)
+                uint32_t fill = 0;     // MODE_LEAF: staged P2P sources
+                uint32_t head = kNone; // MODE_LEAF: last spilled chunk
+                uint32_t dbg_m2l = 0, dbg_p2p = 0;
+                uint32_t ssize = 0, e0 = 0;
+                bool root_pending = root_only;
+                for (;;) {
+                    // ---- next batch of candidates into cand[0, tot) ----
+                    uint32_t tot;
+                    if (root_pending) {
+                        if (lane == 0) sm.cand[0] = 0;  // the root
+                        tot = 1;
+                        root_pending = false;
+                    } else if (e0 < nsn &&
+                               (MODE == MODE_INTERNAL ||
+                                ssize <= (uint32_t)(kStackCap - kStackSlack - kCandBuf))) {
+                        const uint32_t e = e0 + lane;
+                        uint32_t s0 = 0, c = 0, link = 0;
+                        if (e < nsn) {
+                            s0 = nsl[e];
+                            link = tv.link[s0];
+                            const uint32_t nch = link >> 28;
+                            c = nch ? nch : 1u;
+                        }
+                        const uint32_t inc = warp_incl_scan(c);
+                        tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+                        const uint32_t ex = inc - c;
+                        const bool lf = (link >> 28) == 0;
+                        for (uint32_t i = 0; i < c; ++i)
+                            sm.cand[ex + i] = lf ? s0 : (link & kLinkMask) + i;
+                        e0 += 32;
+                    } else if (MODE == MODE_LEAF && ssize > 0) {
+                        // pop entries (bounded so the stack cannot overflow), open them
+                        const int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
+                        const uint32_t kp = (uint32_t)min(32, min((int)ssize, max(1, room)));
+                        uint32_t node = 0;
+                        if constexpr (MODE == MODE_LEAF) {
+                            if (lane < kp) node = sm.stk[ssize - kp + lane];
+                        }
+                        __syncwarp();
+                        ssize -= kp;
+                        const uint32_t link = lane < kp ? tv.link[node] : 0u;
+                        const uint32_t nch = link >> 28;
+                        const uint32_t inc = warp_incl_scan(nch);
+                        tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+                        const uint32_t ex = inc - nch;
+                        for (uint32_t i = 0; i < nch; ++i) sm.cand[ex + i] = (link & kLinkMask) + i;
+                    } else {
+                        break;
+                    }
+                    __syncwarp();
+
+                    // ---- test the candidates, one per lane ----
+#pragma unroll 1
+                    for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
+                        const uint32_t j = j0 + lane;
+                        const bool valid = j < tot;
+                        uint32_t s = 0, slink = 0;
+                        float4 sg = make_float4(0.f, 0.f, 0.f, 0.f), smp = sg;
+                        if (valid) {
+                            s = sm.cand[j];
+                            sg = tv.geo[s];
+                            smp = tv.mp[s];
+                            slink = tv.link[s];
+                        }
+                        float dx, dy, dz, d2;
+                        const bool sep = mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z,
+                                                       sg.w, theta2, dx, dy, dz, d2) && valid;
+                        if (sep) {
+                            float fx, fy, fz;
+                            m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
+                            ax += fx;
+                            ay += fy;
+                            az += fz;
+                        }
+                        if (DEBUG) dbg_m2l += __popc(__ballot_sync(0xFFFFFFFFu, sep));
+                        const bool near = valid && !sep;
+                        if constexpr (MODE == MODE_INTERNAL) {
+                            const uint32_t nm = __ballot_sync(0xFFFFFFFFu, near);
+                            if (near && ns_ok)
+                                A.ns[ns_base + (unsigned long long)sub * cand_total + n_near +
+                                     __popc(nm & lt_mask)] = s;
+                            n_near += __popc(nm);
+                        } else {
+                            const bool sleaf = (slink >> 28) == 0;
+                            // near leaf: P2P source
+                            uint32_t pm = __ballot_sync(0xFFFFFFFFu, near && sleaf);
+                            if (DEBUG) dbg_p2p += __popc(pm);
+                            while (pm) {
+                                if (fill == (uint32_t)kP2PChunk) {
+                                    head = spill_p2p(sm, fill, head, A.p2p, status);
+                                    fill = 0;
+                                }
+                                const uint32_t space = kP2PChunk - fill;
+                                const uint32_t rank = __popc(pm & lt_mask);
+                                const bool take = ((pm >> lane) & 1u) && rank < space;
+                                if (take) sm.p2p[fill + rank] = s;
+                                const uint32_t taken = __ballot_sync(0xFFFFFFFFu, take);
+                                pm &= ~taken;
+                                fill += __popc(taken);
+                                __syncwarp();
+                            }
+                            // near internal source: open it later (the "t leaf" recursion)
+                            const bool push = near && !sleaf;
+                            const uint32_t qm = __ballot_sync(0xFFFFFFFFu, push);
+                            if (qm) {
+                                const uint32_t pos = ssize + __popc(qm & lt_mask);
+                                if (push && pos < (uint32_t)kStackCap) sm.stk[pos] = s;
+                                ssize += __popc(qm);
+                                if (ssize > (uint32_t)kStackCap) {
+                                    if (lane == 0) set_err(status, PSG_ERR_STACK);
+                                    ssize = kStackCap;
+                                }
+                            }
+                        }
+                        __syncwarp();
+                    }
+                    if (MODE == MODE_LEAF && DEBUG && lane == 0) atomicMax(&status->max_stack, ssize);
+                }
+
+                // ---- L2L; for leaves L2P + P2P ----
+                ax = warp_sum(ax);
+                ay = warp_sum(ay);
+                az = warp_sum(az);
                 // L(u) = M2L(u) + L(parent)  (polesitter.h:1248-1250)
                 const float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
                                              __fadd_rn(az, Lp.w));
                 if (lane == 0) tv.lt[u] = L;
                 if constexpr (MODE == MODE_INTERNAL) {
                     if (lane == 0) {
-                        const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
                         tv.ns_off[u] = (uint32_t)(ns_base + (unsigned long long)sub * cand_total);
-                        tv.ns_cnt[u] = ns_ok ? sm.ns_cnt[q] : 0u;
+                        tv.ns_cnt[u] = ns_ok ? n_near : 0u;
                     }
                 } else {
-                    // sources: the staged ones (lane < fill) and spilled chunks
+                    // P2P sources: the staged ones (lane < fill) and spilled chunks
                     const uint4 ui = tv.info[u];
-                    const uint32_t fill = sm.p2p_fill[q];
-                    const uint32_t head = sm.p2p_head[q];
                     uint4 si0 = make_uint4(0, 0, 0, 0);
-                    if (lane < fill) si0 = tv.info[sm.p2p[q][lane]];
+                    if (lane < fill) si0 = tv.info[sm.p2p[lane]];
                     unsigned long long inter = 0;
                     for (uint32_t ti = 0; ti < ui.y; ++ti) {
                         const float4 t = A.xyzm[ui.x + ti];
-                        float ax2 = 0.f, ay2 = 0.f, az2 = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-                        p2p_leaf(A.xyzm, si0, t, A.kahan, ax2, ay2, az2, cx, cy, cz);
-                        if (DEBUG && ti == 0) inter += si0.y;
+                        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+                        p2p_leaf(A.xyzm, si0, t, A.kahan, bx, by, bz, cx, cy, cz);
+                        if (DEBUG) inter += si0.y;
                         for (uint32_t c = head; c != kNone; c = A.p2p.next[c]) {
                             if (lane < A.p2p.cnt[c]) {
                                 const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
-                                p2p_leaf(A.xyzm, si, t, A.kahan, ax2, ay2, az2, cx, cy, cz);
-                                if (DEBUG && ti == 0) inter += si.y;
+                                p2p_leaf(A.xyzm, si, t, A.kahan, bx, by, bz, cx, cy, cz);
+                                if (DEBUG) inter += si.y;
                             }
                         }
                         // lane partials (compensated) summed in FP64
-                        const double sx = warp_sum((double)ax2 - (double)cx);
-                        const double sy = warp_sum((double)ay2 - (double)cy);
-                        const double sz = warp_sum((double)az2 - (double)cz);
+                        const double sx = warp_sum((double)bx - (double)cx);
+                        const double sy = warp_sum((double)by - (double)cy);
+                        const double sz = warp_sum((double)bz - (double)cz);
                         if (lane == 0) {
                             const size_t gi = (size_t)ui.x + ti;
                             const double mm = (double)t.w;
@@ -549,16 +449,16 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     if (DEBUG) {
                         inter = warp_sum(inter);
                         if (lane == 0) {
-                            tv.dbg_p2p[u] = sm.dbg_p2p[q];
-                            atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS],
-                                      (unsigned long long)sm.dbg_p2p[q]);
+                            tv.dbg_p2p[u] = dbg_p2p;
+                            atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS], (unsigned long long)dbg_p2p);
                             atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
                         }
                     }
+                    __syncwarp();
                 }
                 if (DEBUG && lane == 0) {
-                    tv.dbg_m2l[u] = sm.dbg_m2l[q];
-                    atomicAdd(&status->stat[PSG_STAT_M2L], (unsigned long long)sm.dbg_m2l[q]);
+                    tv.dbg_m2l[u] = dbg_m2l;
+                    atomicAdd(&status->stat[PSG_STAT_M2L], (unsigned long long)dbg_m2l);
                 }
             }
             __syncwarp();

@@ -79,6 +79,7 @@ struct State {
     float ms[kPhases];
     unsigned long long stats[24];
     uint32_t last_nodes;
+    uint32_t lvl_count[kLevels];  // node counts of the last completed tick
 };
 
 static int grid_for(const State* s, size_t n, int per_block_items) {
@@ -211,6 +212,7 @@ static int init_state(State* s, size_t maxp, float theta) {
     PSG_ALLOC(s->tv.p2p_head, nodes * 4);
     PSG_ALLOC(s->d_status, sizeof(Status));
     PSG_CHECK(cudaMallocHost((void**)&s->h_status, sizeof(Status)));
+    std::memset(s->h_status, 0, sizeof(Status));
     int r = alloc_ns(s, (unsigned long long)(n < 1024 ? 1024 : n) * 48ull);
     if (r != PSG_OK) return r;
     r = alloc_p2p(s, (uint32_t)(n < 4096 ? 4096 : n));
@@ -325,13 +327,7 @@ static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, f
     }
     record(s, PH_BEGIN);
     PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
-    if (n == 1) {
-        // a single particle: the root is a leaf and its only P2P term is
-        // the zero self-interaction (polesitter.h:1279-1449)
-        PSG_CHECK(cudaMemsetAsync(fx, 0, 4, st));
-        PSG_CHECK(cudaMemsetAsync(fy, 0, 4, st));
-        PSG_CHECK(cudaMemsetAsync(fz, 0, 4, st));
-    } else {
+    {
         const int g = grid_for(s, n, 1024);
         launch_sort(s->sort, codes, n, g, s->d_status, st);
         record(s, PH_SORT);
@@ -349,8 +345,22 @@ static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, f
         record(s, PH_UP);
         PSG_CHECK(cudaGetLastError());
         uint32_t err = 0;
-        int r = run_traversal(s, s->xyzm, fx, fy, fz, &err);
-        if (r != PSG_OK) return r;
+        if (n == 1) {
+            // a single particle: the root is a leaf and its only P2P term is
+            // the zero self-interaction (polesitter.h:1279-1449)
+            PSG_CHECK(cudaMemsetAsync(fx, 0, 4, st));
+            PSG_CHECK(cudaMemsetAsync(fy, 0, 4, st));
+            PSG_CHECK(cudaMemsetAsync(fz, 0, 4, st));
+            record(s, PH_TRAV);
+            record(s, PH_END);
+            PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
+                                      cudaMemcpyDeviceToHost, st));
+            PSG_CHECK(cudaStreamSynchronize(st));
+            err = s->h_status->err;
+        } else {
+            int r = run_traversal(s, s->xyzm, fx, fy, fz, &err);
+            if (r != PSG_OK) return r;
+        }
         if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK)) {
             std::snprintf(g_err, sizeof(g_err), "device status error 0x%x", err);
             return PSG_EDEVICE;
@@ -360,7 +370,10 @@ static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, f
             return PSG_EINVAL;
         }
         uint32_t nodes = 0;
-        for (int d = 0; d <= kMaxDepth; ++d) nodes += s->h_status->lvl_count[d];
+        for (int d = 0; d <= kMaxDepth; ++d) {
+            s->lvl_count[d] = s->h_status->lvl_count[d];
+            nodes += s->lvl_count[d];
+        }
         s->last_nodes = nodes;
         for (int i = 0; i < 8; ++i) s->stats[i] = s->h_status->stat[i];
         s->stats[8] = nodes;
@@ -527,18 +540,18 @@ int psg_tree_dump(void* mem, size_t cap, int32_t* depth, uint32_t* start, uint32
                   float* geo, float* mp, float* lt, uint32_t* m2l_cnt, uint32_t* p2p_cnt) {
     State* s = static_cast<State*>(mem);
     if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
-    if (cap < s->last_nodes) return PSG_EOOM;
+    if (cap < s->last_nodes || s->last_nodes == 0) return cap < s->last_nodes ? PSG_EOOM : PSG_OK;
     PSG_CHECK(cudaSetDevice(s->device));
     // global (capacity-strided) ids -> compact level-major ids
     uint32_t cstart[psg::kLevels + 1];
     cstart[0] = 0;
-    for (int d = 0; d <= psg::kMaxDepth; ++d) cstart[d + 1] = cstart[d] + s->h_status->lvl_count[d];
+    for (int d = 0; d <= psg::kMaxDepth; ++d) cstart[d + 1] = cstart[d] + s->lvl_count[d];
     auto compact = [&](uint32_t g, int d) -> uint32_t {
         return g - s->tv.lvl_base[d] + cstart[d];
     };
     size_t k = 0;
     for (int d = 0; d <= psg::kMaxDepth; ++d) {
-        const uint32_t cnt = s->h_status->lvl_count[d];
+        const uint32_t cnt = s->lvl_count[d];
         const uint32_t b = s->tv.lvl_base[d];
         if (!cnt) continue;
         uint4* inf = new uint4[cnt];

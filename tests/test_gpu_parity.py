@@ -1,0 +1,220 @@
+"""Parity of the B200 path with the reference, through the C ABI.
+
+Every case runs ps_prepare_particles + ps_calc_forces of libpolesitter_b200.so
+and compares with (a) the golden fixtures produced by the reference itself
+and (b) the oracle on the same inputs.  Bar: Morton codes, bounding box, sort
+order, ids, sorted arrays, tree topology and node centres bit-exact; the
+per-node M2L and P2P pair counts (the interaction set) identical; forces
+within 1e-5 relative L2 (and each particle within 1e-4 relative)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import polesitter_b200 as P
+from conftest import golden_names, golden_particles, load_golden, rel_l2
+from polesitter_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FORCE_REL_L2 = 1e-5
+FORCE_REL_MAX = 1e-4
+TOPO = ("depth", "start", "count", "nchild", "octant")
+
+
+def gpu_tick(p, theta, debug=True, kahan=False, max_particles=None):
+    with P.Context(max_particles or p.n, theta=theta) as ctx:
+        if debug:
+            ctx.set_option(P.OPT_DEBUG, 1)
+        if kahan:
+            ctx.set_option(P.OPT_KAHAN, 1)
+        codes = np.zeros(p.n, np.uint32)
+        mn, mx, rg = ctx.tick(p, codes)
+        return {"codes": codes, "bbox": np.array([mn, mx, rg], np.float32),
+                "tree": ctx.tree(), "stats": ctx.stats()}
+
+
+def forces(p):
+    return np.stack([p.fx, p.fy, p.fz], axis=1).astype(np.float64)
+
+
+def assert_forces_close(F, G, l2=FORCE_REL_L2, mx=FORCE_REL_MAX):
+    assert rel_l2(F, G) < l2
+    nrm = np.linalg.norm(G, axis=1)
+    big = nrm > 1e-6 * nrm.max()
+    per = np.linalg.norm(F - G, axis=1)[big] / nrm[big]
+    assert per.max() < mx, per.max()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden(name):
+    g = load_golden(name)
+    p = golden_particles(g)
+    r = gpu_tick(p, float(g["theta"]))
+    assert np.array_equal(r["codes"], g["codes"])
+    assert np.array_equal(r["bbox"], g["bbox"])
+    assert np.array_equal(p.id, g["id"])
+    for k in ("x", "y", "z", "mass"):
+        assert np.array_equal(getattr(p, k), g[k]), k
+    t = r["tree"]
+    for k in TOPO:
+        assert np.array_equal(t[k], g["t_" + k]), k
+    assert np.array_equal(t["leaf"], g["t_leaf"])
+    assert np.array_equal(t["geo"], g["t_geo"])
+    assert rel_l2(t["mp"], g["t_mp"]) < 1e-6
+    assert rel_l2(t["local_exp"], g["t_loc"]) < FORCE_REL_L2
+    assert_forces_close(forces(p), np.stack([g["fx"], g["fy"], g["fz"]], axis=1))
+
+
+CASES = [
+    ("uniform1024", lambda: W.uniform_cube(1024, 1), 2.0),
+    ("plummer65536", lambda: W.plummer(65536, 3), 2.0),
+    ("plummer65536_t1", lambda: W.plummer(65536, 3), 1.0),
+    ("plummer20000_t8", lambda: W.plummer(20000, 4), 8.0),
+    ("clusters4096", lambda: W.lcg_two_clusters(4096), 2.0),
+    ("ragged12345", lambda: W.uniform_cube(12345, 6), 2.0),
+    ("cube100_30000", lambda: W.benchmark_cube(30000), 1.0),
+]
+
+
+def _vs_oracle(oracle, p, theta):
+    a, b = p.copy(), p.copy()
+    ro = oracle.tick(a, theta=theta)
+    rg = gpu_tick(b, theta)
+    assert np.array_equal(rg["codes"], ro["codes"])
+    assert np.array_equal(b.id, a.id)
+    t, o = rg["tree"], ro["tree"]
+    for k in TOPO + ("first_child", "parent"):
+        assert np.array_equal(t[k], o[k]), k
+    assert np.array_equal(t["geo"], o["geo"])
+    # P2M / M2M replay the reference's rounded order: bit-exact
+    assert np.array_equal(t["mp"], o["mp"])
+    # the interaction set: every node's M2L and P2P pair counts as target
+    assert np.array_equal(t["m2l_cnt"], o["m2l_cnt"])
+    assert np.array_equal(t["p2p_cnt"], o["p2p_cnt"])
+    assert rg["stats"]["m2l_pairs"] == ro["stats"]["m2l_pairs"]
+    assert rg["stats"]["p2p_pairs"] == ro["stats"]["p2p_pairs"]
+    assert rel_l2(t["local_exp"], o["l_tot"]) < FORCE_REL_L2
+    assert_forces_close(forces(b), forces(a))
+    return rg, ro
+
+
+@pytest.mark.parametrize("name,gen,theta", CASES, ids=[c[0] for c in CASES])
+def test_vs_oracle(oracle, name, gen, theta):
+    _vs_oracle(oracle, gen(), theta)
+
+
+def test_plummer_1m_full_size(oracle):
+    # the benchmark workload itself: N = 2^20 Plummer, theta = 2
+    rg, ro = _vs_oracle(oracle, W.plummer(1 << 20, 42), 2.0)
+    assert ro["stats"]["m2l_pairs"] > 100_000_000
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 8, 9, 17])
+def test_tiny_counts(oracle, n):
+    p = W.uniform_cube(n, 100 + n)
+    a, b = p.copy(), p.copy()
+    oracle.tick(a, theta=2.0)
+    gpu_tick(b, 2.0)
+    assert np.array_equal(a.id, b.id)
+    assert_forces_close(forces(b), forces(a)) if np.abs(forces(a)).max() > 0 else \
+        np.testing.assert_array_equal(forces(b), 0.0)
+
+
+def test_duplicate_positions_fill_depth10_leaves(oracle):
+    # many particles on a few identical positions: leaves at depth 10 hold
+    # dozens of particles (the one place leaves exceed one particle)
+    rng = np.random.default_rng(5)
+    base = rng.uniform(-1, 1, size=(50, 3)).astype(np.float32)
+    pick = rng.integers(0, 50, 3000)
+    pos = base[pick]
+    p = W.Particles(pos[:, 0], pos[:, 1], pos[:, 2], rng.uniform(0.5, 1.5, 3000))
+    rg, ro = _vs_oracle(oracle, p, 2.0)
+    assert rg["tree"]["count"][rg["tree"]["nchild"] == 0].max() > 32
+
+
+def test_device_pointers_match_host_pointers(oracle):
+    torch = pytest.importorskip("torch")
+    p = W.plummer(50000, 9)
+    host = p.copy()
+    gpu_tick(host, 2.0, debug=False)
+
+    class D:
+        pass
+    d = D()
+    for k in ("x", "y", "z", "mass", "fx", "fy", "fz"):
+        setattr(d, k, torch.from_numpy(getattr(p, k).copy()).cuda())
+    d.id = torch.from_numpy(p.id.view(np.int32).copy()).cuda()
+    codes = torch.zeros(p.n, dtype=torch.int32, device="cuda")
+    with P.Context(p.n, theta=2.0) as ctx:
+        ctx.tick(d, codes)
+    torch.cuda.synchronize()
+    for k in ("x", "y", "z", "mass", "fx", "fy", "fz"):
+        assert np.array_equal(getattr(d, k).cpu().numpy(), getattr(host, k)), k
+    assert np.array_equal(d.id.cpu().numpy().view(np.uint32), host.id)
+
+
+def test_repeated_ticks_are_deterministic_and_ids_compose(oracle):
+    p = W.plummer(30000, 12)
+    a, b = p.copy(), p.copy()
+    with P.Context(p.n, theta=2.0) as ctx:
+        codes = np.zeros(p.n, np.uint32)
+        ctx.tick(b, codes)
+        f1 = forces(b).copy()
+        ctx.tick(b, codes)  # re-sorting sorted data is the identity
+        assert np.array_equal(forces(b), f1)
+        # perturb and tick again without resetting ids: ids compose like the
+        # reference's (the caller resets them, README.md:66-70)
+        b.x += np.float32(1e-3)
+        ctx.tick(b, codes)
+    oracle.tick(a, theta=2.0)
+    oracle.tick(a, theta=2.0)
+    a.x += np.float32(1e-3)
+    oracle.tick(a, theta=2.0)
+    assert np.array_equal(a.id, b.id)
+    assert_forces_close(forces(b), forces(a))
+
+
+def test_error_results():
+    p = W.uniform_cube(100, 1)
+    with P.Context(50, theta=2.0) as ctx:
+        codes = np.zeros(p.n, np.uint32)
+        with pytest.raises(P.PolesitterError) as e:
+            ctx.tick(p, codes)  # cnt above max_particles
+        assert e.value.code == P.PS_EINVAL
+
+
+def test_kahan_option_is_at_least_as_accurate(oracle):
+    p = W.plummer(20000, 21)
+    src = p.copy()
+    a, b = p.copy(), p.copy()
+    gpu_tick(a, 8.0, debug=False)
+    gpu_tick(b, 8.0, debug=False, kahan=True)
+    assert_forces_close(forces(b), forces(a), l2=1e-6, mx=1e-5)
+    f64 = oracle.direct_f64(src)
+    err_a = rel_l2(forces(a), f64[a.id])
+    err_b = rel_l2(forces(b), f64[b.id])
+    assert err_b <= err_a * 1.0001
+
+
+def test_fp64_direct_sum_on_gpu(oracle):
+    p = W.plummer(20000, 31)
+    tg = np.arange(0, p.n, 37, dtype=np.uint32)
+    want = oracle.direct_f64(p, tg)
+    with P.Context(p.n) as ctx:
+        got = ctx.direct_f64(p, tg)
+    assert np.abs(got - want).max() <= 1e-10 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("variant", [P.MORTON_NEON, P.MORTON_SCALAR])
+def test_other_morton_variants(oracle, variant):
+    p = W.uniform_cube(10001, 14)
+    _, codes_o, *_ = oracle.prepare(p, variant)
+    codes = np.zeros(p.n, np.uint32)
+    try:
+        P.set_morton_variant(variant)
+        P.prepare_particles(p.copy(), codes)
+    finally:
+        P.set_morton_variant(P.MORTON_AVX2)
+    assert np.array_equal(codes, codes_o)

@@ -1,0 +1,178 @@
+"""The oracle (oracle/ps_oracle.c) against the reference's own known answers,
+the golden fixtures made by the reference, and -- where the checker's build of
+the reference exists -- the reference itself, live.
+
+Known answers restated from the reference's tests (tests/main.c:50-476,
+tests/accuracy.c:74-109, :427-568)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, golden_particles, load_golden, rel_l2
+from polesitter_b200 import workloads as W
+
+THETA_SQRT12 = 3.4641  # tests/main.c:11
+
+
+# ---- known answers of tests/main.c ------------------------------------------
+
+def test_morton_bit_positions(oracle):
+    # tests/main.c:50-72
+    assert oracle.morton_encode(1, 0, 0) == 1
+    assert oracle.morton_encode(0, 1, 0) == 2
+    assert oracle.morton_encode(0, 0, 1) == 4
+    assert oracle.morton_encode(3, 0, 0) == 9
+    assert oracle.morton_encode(1023, 1023, 1023) == (1 << 30) - 1
+
+
+def test_radix_sort_co_sorts(oracle):
+    # tests/main.c:192-233
+    p = W.Particles([9, 1, 5, 4], [9, 1, 5, 4], [9, 1, 5, 4], [9, 1, 5, 4])
+    codes = np.array([999, 10, 500, 42], np.uint32)
+    oracle.sort(p, codes)
+    assert codes.tolist() == [10, 42, 500, 999]
+    assert p.mass.tolist() == [1.0, 4.0, 5.0, 9.0]
+    assert p.id.tolist() == [1, 3, 2, 0]
+
+
+def test_octree_two_corner_particles(oracle):
+    # tests/main.c:125-190: codes of (0,0,0) and (1023,1023,1023) end in the
+    # leaves down child 0 and child 7, one particle each
+    lo, hi = oracle.morton_encode(0, 0, 0), oracle.morton_encode(1023, 1023, 1023)
+    p = W.Particles([0, 1], [0, 1], [0, 1], [1, 1])
+    r = oracle.calc(p, np.array([lo, hi], np.uint32), 0.0, 0.0, 0.0, 10.0, THETA_SQRT12)
+    t = r["tree"]
+    assert t["nchild"][0] == 2 and t["leaf"][0] == 0
+    kids = t["first_child"][0] + np.arange(2)
+    assert t["octant"][kids].tolist() == [0, 7]
+    assert t["leaf"][kids].tolist() == [1, 1]
+    assert t["count"][kids].tolist() == [1, 1]
+    assert t["start"][kids].tolist() == [0, 1]
+
+
+def test_p2m(oracle):
+    # tests/main.c:235-280
+    mp = oracle.p2m([2.0, -1.0], [3.0, -2.0], [4.0, -3.0], [2.0, 3.0])
+    np.testing.assert_allclose(mp, [5.0, 1.0, 0.0, -1.0], atol=1e-4)
+
+
+def test_m2l_field(oracle):
+    # tests/main.c:282-323: unit mass at (10,10,10) from the target
+    hit, loc = oracle.m2l_pair([-5, -5, -5, 1], [5, 5, 5, 1], [1, 0, 0, 0], THETA_SQRT12)
+    assert hit
+    np.testing.assert_allclose(loc[1:], [0.00192354] * 3, atol=1e-6)
+
+
+def test_m2l_dipole_orientation(oracle):
+    # tests/accuracy.c:74-109
+    hit, loc = oracle.m2l_pair([0, 0, 0, 1], [100, 0, 0, 1], [1, 1, 0, 0], 2.0)
+    assert hit
+    assert abs(float(loc[1]) - 0.00009799856) <= 5e-9
+
+
+def test_mac_not_separated_is_not_applied(oracle):
+    hit, loc = oracle.m2l_pair([0, 0, 0, 1], [3, 0, 0, 1], [1, 0, 0, 0], 2.0)
+    assert not hit and not loc.any()
+
+
+def test_p2p_pair_force(oracle):
+    # tests/main.c:427-476: two particles one unit apart
+    p = W.Particles([0.0, 1.0], [0.0, 0.0], [0.0, 0.0], [2.0, 3.0])
+    oracle.p2p_pair(p, 0, 2, 0, 2)
+    expected = (2.0 * 3.0) * 1.1 ** -1.5
+    assert abs(p.fx[0] - expected) < 1e-4 and abs(p.fx[1] + expected) < 1e-4
+    assert abs(p.fy).max() < 1e-6 and abs(p.fz).max() < 1e-6
+
+
+@pytest.mark.parametrize("fill,name", [(W.lcg_uniform, "uniform-512"),
+                                       (W.lcg_two_clusters, "two-clusters-512")])
+def test_accuracy_gate(oracle, fill, name):
+    # tests/accuracy.c:427-568: RMS relative error vs the FP64 direct sum < 0.10
+    p = fill(512)
+    ref_in = p.copy()
+    oracle.tick(p, theta=2.0)
+    f64 = oracle.direct_f64(ref_in)
+    got = np.zeros_like(f64)
+    got[p.id] = np.stack([p.fx, p.fy, p.fz], axis=1)
+    d = got - f64
+    rms = np.sqrt((d * d).sum() / (f64 * f64).sum())
+    assert rms < 0.10, (name, rms)
+
+
+# ---- golden fixtures made by the reference ----------------------------------
+
+@pytest.mark.parametrize("name", golden_names())
+def test_matches_golden(oracle, name):
+    g = load_golden(name)
+    p = golden_particles(g)
+    r = oracle.tick(p, theta=float(g["theta"]))
+    assert np.array_equal(r["codes"], g["codes"])
+    assert np.array_equal(np.array([r["min"], r["max"], r["range"]], np.float32), g["bbox"])
+    assert np.array_equal(p.id, g["id"])
+    for k in ("x", "y", "z", "mass"):
+        assert np.array_equal(getattr(p, k), g[k])
+    t = r["tree"]
+    for k in ("depth", "start", "count", "leaf", "nchild", "octant"):
+        assert np.array_equal(t[k], g["t_" + k]), k
+    assert np.array_equal(t["geo"], g["t_geo"])
+    # the fixtures come from the reference's fast-math build: sums may be
+    # reassociated, so values agree to rounding, not bit for bit
+    assert rel_l2(t["mp"], g["t_mp"]) < 1e-6
+    assert rel_l2(t["l_tot"], g["t_loc"]) < 1e-5
+    F = np.stack([p.fx, p.fy, p.fz])
+    G = np.stack([g["fx"], g["fy"], g["fz"]])
+    assert rel_l2(F, G) < 2e-6
+
+
+# ---- the reference itself, where its checker build exists ------------------
+
+def _ref_or_skip(variant):
+    from oracle import refbind
+    if not refbind.available(variant):
+        pytest.skip("oracle/_ref not built (needs the reference checkout)")
+    return refbind.RefLib(variant)
+
+
+@pytest.mark.parametrize("n,seed,theta", [(1500, 3, 2.0), (777, 4, 1.0), (2048, 5, 3.4641)])
+def test_bit_exact_vs_strict_reference(oracle, n, seed, theta):
+    ref = _ref_or_skip("_strict")
+    p = W.plummer(n, seed)
+    a, b = p.copy(), p.copy()
+    ro = oracle.tick(a, theta=theta)
+    rr = ref.tick(b, theta=theta, thrd_cnt=4, dump_tree=True)
+    assert np.array_equal(ro["codes"], rr["codes"])
+    assert np.array_equal(a.id, b.id)
+    t = rr["tree"]
+    for k in ("depth", "start", "count", "leaf", "nchild", "octant"):
+        assert np.array_equal(ro["tree"][k], t[k])
+    for k_o, k_r in (("geo", "geo"), ("mp", "mp"), ("l_tot", "loc")):
+        assert np.array_equal(ro["tree"][k_o], t[k_r]), k_o
+    for k in ("fx", "fy", "fz"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_other_morton_variants_vs_formula(oracle, variant):
+    # NEON truncation (:2101-2113) and the scalar formula (:2133-2153)
+    p = W.uniform_cube(1001, 8)
+    rc, codes, mn, mx, rg = oracle.prepare(p, variant)
+    f = np.float32
+    lanes = 4 if variant == 1 else 0
+    vec_end = (p.n // lanes) * lanes if lanes else 0
+    scale = f(1023.0) / f(rg)
+    want = []
+    for i in range(p.n):
+        q = []
+        for v in (p.x[i], p.y[i], p.z[i]):
+            if i < vec_end:
+                t = (f(v) - f(mn)) * scale
+                t = t if t < f(1023) else f(1023)
+                t = f(0) if f(0) > t else t
+                q.append(int(t))
+            else:
+                t = int(((f(v) - f(mn)) / f(rg)) * f(1023.0))
+                q.append(min(max(t, 0), 1023))
+        want.append(oracle.morton_encode(*q))
+    assert codes.tolist() == want
