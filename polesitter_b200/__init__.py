@@ -30,7 +30,8 @@ MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
             "ps_b200_context_size", "ps_b200_set_option", "ps_b200_set_morton_variant",
             "ps_b200_get_stats", "ps_b200_last_timing", "ps_b200_tree_nodes",
-            "ps_b200_tree_dump", "ps_b200_direct_f64", "ps_b200_last_error")
+            "ps_b200_tree_dump", "ps_b200_direct_f64", "ps_b200_last_error",
+            "ps_b200_prepare_particles_noalloc")
 
 
 class ParticleArrs(C.Structure):
@@ -93,6 +94,9 @@ def lib() -> C.CDLL:
     L.ps_b200_direct_f64.restype = C.c_int
     L.ps_b200_direct_f64.argtypes = [vp, C.POINTER(ParticleArrs), vp, sz, vp]
     L.ps_b200_last_error.restype = C.c_char_p
+    L.ps_b200_prepare_particles_noalloc.restype = C.c_int
+    L.ps_b200_prepare_particles_noalloc.argtypes = [C.POINTER(ParticleArrs), vp, C.POINTER(f32),
+                                                    C.POINTER(f32), C.POINTER(f32)]
     _LIB = L
     return L
 

@@ -88,6 +88,12 @@ int psg_last_timing(void* state, float* out_ms, size_t n_out);
 int psg_direct_f64(void* state, const psg_arrays_t* a, const uint32_t* targets, size_t n_t,
                    double* out);
 const char* psg_last_error(void);
+void psg_set_error(const char* msg);
+
+/* ps_prepare_particles with a fixed static scratch (k_noalloc.cu) */
+int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n,
+                        uint32_t* codes, float* out_min, float* out_max, float* out_range,
+                        int variant);
 
 #define PSG_OPT_DEBUG 1          /* 1: record per-node interaction counts */
 #define PSG_OPT_THETA 2

@@ -621,4 +621,6 @@ int psg_direct_f64(void* mem, const psg_arrays_t* a, const uint32_t* targets, si
 
 const char* psg_last_error(void) { return psg::g_err; }
 
+void psg_set_error(const char* msg) { std::snprintf(psg::g_err, sizeof(psg::g_err), "%s", msg); }
+
 }  // extern "C"

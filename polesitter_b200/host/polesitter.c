@@ -191,3 +191,13 @@ ps_result_t ps_b200_direct_f64(ps_context_t* ctx, const ps_particle_arrs_t* arrs
 }
 
 const char* ps_b200_last_error(void) { return psg_last_error(); }
+
+ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,
+                                              uint32_t* out_morton_codes, float* out_min_b,
+                                              float* out_max_b, float* out_range) {
+    if (!arrs || !out_morton_codes || arrs->cnt == 0) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_prepare_noalloc(arrs->x, arrs->y, arrs->z, arrs->cnt, out_morton_codes,
+                                     out_min_b, out_max_b, out_range, g_morton_variant));
+}
