@@ -56,7 +56,7 @@ WORKLOAD = ("plain FMM tick (ps_prepare_particles + ps_calc_forces), Plummer sph
 KERNELS_PER_TICK = 35  # 2 prepare + 6 sort + gather + write-back + 4 tree + 11 upward + 10 traversal
 # DRAM bytes (read + write) of one leaf-pass launch at this workload, from the
 # ncu capture summarised in profiles/traversal_leaf_plummer1m.md
-LEAF_PASS_DRAM_BYTES = 252.0e6
+LEAF_PASS_DRAM_BYTES = 254.3e6
 FLOP_M2L = 35   # per M2L pair: polesitter.h:1065-1092
 FLOP_P2P = 20   # per particle pair: polesitter.h:1424-1444
 
