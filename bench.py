@@ -262,11 +262,8 @@ def run_b200(args):
         torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    total = sum(step_s)
-    if world > 1:
-        t = torch.tensor([total], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total = float(t.item())
+    from polesitter_b200.replicas import job_time
+    total = job_time(sum(step_s), dev)
     value = world * args.steps / total
 
     # accuracy of the last tick against an FP64 direct sum (GPU) on 4096
@@ -310,11 +307,7 @@ def run_b200(args):
         t0 = time.perf_counter()
         ctx.tick(hp, pin_codes)
         e2e_s.append(time.perf_counter() - t0)
-    e2e_total = sum(e2e_s)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = job_time(sum(e2e_s), dev)
     e2e = {"value": world * e2e_steps / e2e_total, "unit": UNIT,
            # prepare: x,y,z in / codes out; calc: x,y,z,mass,id,codes in /
            # x,y,z,mass,id,codes,fx,fy,fz out -- 4 bytes per particle each
