@@ -17,25 +17,29 @@
 //
 // B200 formulation (target-major, no interaction lists in HBM).  The pairs
 // an internal target t hands to its children are its "near list" NS(t) =
-// the sources it was not separated from, so every child u of an internal
-// node p starts from the same candidates
+// the sources it was not separated from, so all children of an internal
+// node p (a "group") start from the same candidates
 //   cand(p) = {root}                                         if depth(p) <= 1
 //   cand(p) = U_{s in NS(p)} (s leaf ? {s} : children(s))    otherwise.
-// One warp owns a parent p and takes its target children one after the
-// other; for a child u the lanes test 32 candidates at a time with the MAC,
-// accumulate M2L in registers, and deal with the near ones:
+// One warp owns a group.  Candidates are tested 32 at a time, one per lane;
+// each carries the set of the group's children it must be tested against,
+// and the lane loads the candidate once and runs the MAC (and M2L, into
+// per-child register accumulators) for each of those children.  What is
+// not separated is dealt with once per chunk:
 //
 //  * MODE_INTERNAL, one launch per level k = 2..10, targets = the internal
 //    children of the depth-(k-1) nodes: near candidates form NS(u) in HBM for
-//    level k+1, and L(u) = M2L(u) + L(p) is stored.
+//    level k+1; L(u) = M2L(u) + L(p) is stored.
 //  * MODE_LEAF, one launch after all levels, targets = the leaf children of
-//    every node: a near leaf candidate is a P2P source (staged in shared
-//    memory, spilled to HBM chunks only past 32), a near internal candidate
-//    is the "t leaf" recursion and goes onto a DFS stack in shared memory
-//    that is drained the same way.  The warp then finishes u:
-//    L(u) = M2L(u) + L(p) and, per particle, F = m * (L(u) + its P2P sum) --
-//    written once, no atomics.  Running all levels' leaves in one launch lets
-//    the long descents of shallow leaves overlap with everything else.
+//    every node: a near leaf candidate is a P2P source, staged in shared
+//    memory with the set of children it serves (spilled to HBM chunks past
+//    128); a near internal candidate is the "t leaf" recursion -- it goes
+//    onto a DFS stack in shared memory with the set of children that still
+//    need it opened, so sibling leaves share every descent.  The warp then
+//    finishes each leaf: L(u) = M2L(u) + L(p) and, per particle,
+//    F = m * (L(u) + its P2P sum) -- written once, no atomics.  Running all
+//    levels' leaves in one launch lets the long descents of shallow leaves
+//    overlap with everything else.
 //
 // The MAC replays the reference's rounded float sequence exactly
 // (mac_separated), so the interaction set is identical, ties included.
@@ -49,25 +53,37 @@ namespace psg {
 constexpr int kTravWarps = 4;
 constexpr int kTravThreads = kTravWarps * 32;
 constexpr int kCandBuf = 256;             // children of 32 opened entries
-constexpr int kStackCap = 384;            // DFS stack (node ids)
+constexpr int kStackCap = 384;            // DFS stack (node, child mask)
 constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-entry descent
+constexpr int kP2PCap = 128;              // staged P2P sources of a group
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
 
 enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
 struct SmemInternal {
-    float4 cgeo[8];  // the parent's children: centre + half width
-    uint32_t cand[kCandBuf];
+    float4 cgeo[8];  // the group's children: centre + half width
+    uint32_t cand_node[kCandBuf];
+    uint32_t ns_cnt[8];
+    uint32_t dbg_m2l[8];
     unsigned long long ns_next, ns_end;
+    uint8_t cand_mask[kCandBuf];
 };
 
 struct SmemLeaf {
     float4 cgeo[8];
-    uint32_t cand[kCandBuf];
-    uint32_t stk[kStackCap];
-    uint32_t p2p[kP2PChunk];
+    float4 sL[8];           // the children's local fields
+    uint2 cpart[8];         // the children's particle ranges
+    uint2 p2p_range[kP2PCap];
+    uint32_t cand_node[kCandBuf];
+    uint32_t stk_node[kStackCap];
+    uint32_t p2p_node[kP2PCap];
     uint32_t chunk_next, chunk_end;
+    uint32_t dbg_m2l[8];
+    uint32_t dbg_p2p[8];
+    uint8_t cand_mask[kCandBuf];
+    uint8_t stk_mask[kStackCap];
+    uint8_t p2p_mask[kP2PCap];
 };
 
 template <int MODE>
@@ -90,46 +106,54 @@ __device__ __forceinline__ void m2l_field(float dx, float dy, float dz, float d2
     fz = fmaf(dz, a, mp.w * ir3);
 }
 
-// Spill the staged P2P sources of the current leaf as one chunk chained to
-// its previous one.  Warp-collective; chunk ids come from a per-warp pool.
+// Spill the group's staged P2P sources [0, fill) to HBM chunks of
+// kP2PChunk (node, child mask) entries, chained to the group's earlier
+// chunks.  Warp-collective; chunk ids come from a per-warp pool.  Returns the
+// new chain head.
 __device__ __noinline__ uint32_t spill_p2p(SmemLeaf& sm, uint32_t fill, uint32_t head,
                                            P2PStore st, Status* status) {
     const uint32_t lane = lane_id();
-    if (sm.chunk_next >= sm.chunk_end) {
-        uint32_t c = 0;
-        if (lane == 0) c = atomicAdd(&status->p2p_chunks, kChunkPool);
-        c = __shfl_sync(0xFFFFFFFFu, c, 0);
-        __syncwarp();
-        if (lane == 0) {
-            sm.chunk_next = c;
-            sm.chunk_end = c + kChunkPool;
+    for (uint32_t e0 = 0; e0 < fill; e0 += kP2PChunk) {
+        if (sm.chunk_next >= sm.chunk_end) {
+            uint32_t c = 0;
+            if (lane == 0) c = atomicAdd(&status->p2p_chunks, kChunkPool);
+            c = __shfl_sync(0xFFFFFFFFu, c, 0);
+            __syncwarp();
+            if (lane == 0) {
+                sm.chunk_next = c;
+                sm.chunk_end = c + kChunkPool;
+            }
+            __syncwarp();
+        }
+        const uint32_t c = sm.chunk_next;
+        const uint32_t cnt = min((uint32_t)kP2PChunk, fill - e0);
+        if (c < st.cap_chunks) {
+            if (lane < cnt) {
+                st.src[(size_t)c * kP2PChunk + lane] = sm.p2p_node[e0 + lane];
+                st.mask[(size_t)c * kP2PChunk + lane] = sm.p2p_mask[e0 + lane];
+            }
+            if (lane == 0) {
+                st.next[c] = head;
+                st.cnt[c] = cnt;
+            }
+            head = c;
+        } else if (lane == 0) {
+            set_err(status, PSG_ERR_P2P_OVERFLOW);
         }
         __syncwarp();
+        if (lane == 0) sm.chunk_next = c + 1;
+        __syncwarp();
     }
-    const uint32_t c = sm.chunk_next;
-    const bool ok = c < st.cap_chunks;
-    if (ok) {
-        if (lane < fill) st.src[(size_t)c * kP2PChunk + lane] = sm.p2p[lane];
-        if (lane == 0) {
-            st.next[c] = head;
-            st.cnt[c] = fill;
-        }
-    } else if (lane == 0) {
-        set_err(status, PSG_ERR_P2P_OVERFLOW);
-    }
-    __syncwarp();
-    if (lane == 0) sm.chunk_next = c + 1;
-    __syncwarp();
-    return ok ? c : head;
+    return head;
 }
 
-// Direct sum of the particles of source leaf si on target particle t
+// Direct sum of the particles [r.x, r.x + r.y) on target particle t
 // (polesitter.h:1424-1444 with rsqrt), optionally Kahan-compensated.
-__device__ __forceinline__ void p2p_leaf(const float4* __restrict__ xyzm, uint4 si, float4 t,
-                                         bool kahan, float& ax, float& ay, float& az, float& cx,
-                                         float& cy, float& cz) {
-    for (uint32_t j = 0; j < si.y; ++j) {
-        const float4 p = xyzm[si.x + j];
+__device__ __forceinline__ void p2p_range(const float4* __restrict__ xyzm, uint2 r, float4 t,
+                                          bool kahan, float& ax, float& ay, float& az, float& cx,
+                                          float& cy, float& cz) {
+    for (uint32_t j = 0; j < r.y; ++j) {
+        const float4 p = xyzm[r.x + j];
         const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
         const float inv = rsqrtf(r2);
@@ -167,7 +191,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
     const float theta2 = __fmul_rn(A.theta, A.theta);
 
-    // parent index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
+    // group index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
     // the nodes at depths 0..9, level after level
     uint32_t cum[kMaxDepth + 1];
     uint32_t total = 0;
@@ -233,6 +257,20 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             const uint32_t tgt_mask =
                 MODE == MODE_INTERNAL ? (((1u << nc) - 1u) & ~leaf_mask) : leaf_mask;
             if (tgt_mask == 0) continue;
+            if constexpr (MODE == MODE_LEAF) {
+                if ((tgt_mask >> lane) & 1u) {
+                    const uint4 ci = tv.info[fc + lane];
+                    sm.cpart[lane] = make_uint2(ci.x, ci.y);
+                }
+            }
+            if (lane < 8) {
+                if (DEBUG) sm.dbg_m2l[lane] = 0;
+                if constexpr (MODE == MODE_INTERNAL) {
+                    sm.ns_cnt[lane] = 0;
+                } else {
+                    if (DEBUG) sm.dbg_p2p[lane] = 0;
+                }
+            }
             const float4 Lp = tv.lt[pid];
             const bool root_only = dp <= 1;
             const uint32_t* nsl = nullptr;
@@ -256,6 +294,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 }
                 const unsigned long long need =
                     (unsigned long long)__popc(tgt_mask) * cand_total;
+                __syncwarp();
                 if (need && sm.ns_next + need > sm.ns_end) {
                     const unsigned long long take = need > kNsPool ? need : kNsPool;
                     unsigned long long b = 0;
@@ -273,195 +312,269 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 if (!ns_ok && lane == 0) set_err(status, PSG_ERR_NS_OVERFLOW);
                 __syncwarp();
                 if (lane == 0) sm.ns_next = ns_base + need;
-                __syncwarp();
             }
+            __syncwarp();
 
-            uint32_t sub = 0;  // rank of the target child among the targets
-#pragma unroll 1
-            for (uint32_t tm = tgt_mask; tm; tm &= tm - 1, ++sub) {
-                const uint32_t q = __ffs(tm) - 1;
-                const uint32_t u = fc + q;
-                const float4 ug = sm.cgeo[q];
-                float ax = 0.f, ay = 0.f, az = 0.f;
-                uint32_t n_near = 0;   // MODE_INTERNAL: entries of NS(u)
-                uint32_t fill = 0;     // MODE_LEAF: staged P2P sources
-                uint32_t head = kNone; // MODE_LEAF: last spilled chunk
-                uint32_t dbg_m2l = 0, dbg_p2p = 0;
-                uint32_t ssize = 0, e0 = 0;
-                bool root_pending = root_only;
-                for (;;) {
-                    // ---- next batch of candidates into cand[0, tot) ----
-                    uint32_t tot;
-                    if (root_pending) {
-                        if (lane == 0) sm.cand[0] = 0;  // the root
-                        tot = 1;
-                        root_pending = false;
-                    } else if (e0 < nsn &&
-                               (MODE == MODE_INTERNAL ||
-                                ssize <= (uint32_t)(kStackCap - kStackSlack - kCandBuf))) {
-                        const uint32_t e = e0 + lane;
-                        uint32_t s0 = 0, c = 0, link = 0;
-                        if (e < nsn) {
-                            s0 = nsl[e];
-                            link = tv.link[s0];
-                            const uint32_t nch = link >> 28;
-                            c = nch ? nch : 1u;
-                        }
-                        const uint32_t inc = warp_incl_scan(c);
-                        tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
-                        const uint32_t ex = inc - c;
-                        const bool lf = (link >> 28) == 0;
-                        for (uint32_t i = 0; i < c; ++i)
-                            sm.cand[ex + i] = lf ? s0 : (link & kLinkMask) + i;
-                        e0 += 32;
-                    } else if (MODE == MODE_LEAF && ssize > 0) {
-                        // pop entries (bounded so the stack cannot overflow), open them
-                        const int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
-                        const uint32_t kp = (uint32_t)min(32, min((int)ssize, max(1, room)));
-                        uint32_t node = 0;
-                        if constexpr (MODE == MODE_LEAF) {
-                            if (lane < kp) node = sm.stk[ssize - kp + lane];
-                        }
-                        __syncwarp();
-                        ssize -= kp;
-                        const uint32_t link = lane < kp ? tv.link[node] : 0u;
+            float acc[8][3];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.f;
+            uint32_t ssize = 0, e0 = 0;
+            uint32_t pfill = 0, phead = kNone;  // MODE_LEAF: staged / spilled P2P sources
+            bool root_pending = root_only;
+
+            for (;;) {
+                // ---- next batch of candidates into cand[0, tot) ----
+                uint32_t tot;
+                if (root_pending) {
+                    if (lane == 0) {
+                        sm.cand_node[0] = 0;  // the root
+                        sm.cand_mask[0] = (uint8_t)tgt_mask;
+                    }
+                    tot = 1;
+                    root_pending = false;
+                } else if (e0 < nsn &&
+                           (MODE == MODE_INTERNAL ||
+                            ssize <= (uint32_t)(kStackCap - kStackSlack - kCandBuf))) {
+                    const uint32_t e = e0 + lane;
+                    uint32_t s0 = 0, c = 0, link = 0;
+                    if (e < nsn) {
+                        s0 = nsl[e];
+                        link = tv.link[s0];
                         const uint32_t nch = link >> 28;
-                        const uint32_t inc = warp_incl_scan(nch);
-                        tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
-                        const uint32_t ex = inc - nch;
-                        for (uint32_t i = 0; i < nch; ++i) sm.cand[ex + i] = (link & kLinkMask) + i;
-                    } else {
-                        break;
+                        c = nch ? nch : 1u;
+                    }
+                    const uint32_t inc = warp_incl_scan(c);
+                    tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+                    const uint32_t ex = inc - c;
+                    const bool lf = (link >> 28) == 0;
+                    for (uint32_t i = 0; i < c; ++i) {
+                        sm.cand_node[ex + i] = lf ? s0 : (link & kLinkMask) + i;
+                        sm.cand_mask[ex + i] = (uint8_t)tgt_mask;
+                    }
+                    e0 += 32;
+                } else if (MODE == MODE_LEAF && ssize > 0) {
+                    // pop entries (bounded so the stack cannot overflow), open them
+                    const int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
+                    const uint32_t kp = (uint32_t)min(32, min((int)ssize, max(1, room)));
+                    uint32_t node = 0, mask = 0;
+                    if constexpr (MODE == MODE_LEAF) {
+                        if (lane < kp) {
+                            node = sm.stk_node[ssize - kp + lane];
+                            mask = sm.stk_mask[ssize - kp + lane];
+                        }
                     }
                     __syncwarp();
-
-                    // ---- test the candidates, one per lane ----
-#pragma unroll 1
-                    for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
-                        const uint32_t j = j0 + lane;
-                        const bool valid = j < tot;
-                        uint32_t s = 0, slink = 0;
-                        float4 sg = make_float4(0.f, 0.f, 0.f, 0.f), smp = sg;
-                        if (valid) {
-                            s = sm.cand[j];
-                            sg = tv.geo[s];
-                            smp = tv.mp[s];
-                            slink = tv.link[s];
-                        }
-                        float dx, dy, dz, d2;
-                        const bool sep = mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z,
-                                                       sg.w, theta2, dx, dy, dz, d2) && valid;
-                        if (sep) {
-                            float fx, fy, fz;
-                            m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
-                            ax += fx;
-                            ay += fy;
-                            az += fz;
-                        }
-                        if (DEBUG) dbg_m2l += __popc(__ballot_sync(0xFFFFFFFFu, sep));
-                        const bool near = valid && !sep;
-                        if constexpr (MODE == MODE_INTERNAL) {
-                            const uint32_t nm = __ballot_sync(0xFFFFFFFFu, near);
-                            if (near && ns_ok)
-                                A.ns[ns_base + (unsigned long long)sub * cand_total + n_near +
-                                     __popc(nm & lt_mask)] = s;
-                            n_near += __popc(nm);
-                        } else {
-                            const bool sleaf = (slink >> 28) == 0;
-                            // near leaf: P2P source
-                            uint32_t pm = __ballot_sync(0xFFFFFFFFu, near && sleaf);
-                            if (DEBUG) dbg_p2p += __popc(pm);
-                            while (pm) {
-                                if (fill == (uint32_t)kP2PChunk) {
-                                    head = spill_p2p(sm, fill, head, A.p2p, status);
-                                    fill = 0;
-                                }
-                                const uint32_t space = kP2PChunk - fill;
-                                const uint32_t rank = __popc(pm & lt_mask);
-                                const bool take = ((pm >> lane) & 1u) && rank < space;
-                                if (take) sm.p2p[fill + rank] = s;
-                                const uint32_t taken = __ballot_sync(0xFFFFFFFFu, take);
-                                pm &= ~taken;
-                                fill += __popc(taken);
-                                __syncwarp();
-                            }
-                            // near internal source: open it later (the "t leaf" recursion)
-                            const bool push = near && !sleaf;
-                            const uint32_t qm = __ballot_sync(0xFFFFFFFFu, push);
-                            if (qm) {
-                                const uint32_t pos = ssize + __popc(qm & lt_mask);
-                                if (push && pos < (uint32_t)kStackCap) sm.stk[pos] = s;
-                                ssize += __popc(qm);
-                                if (ssize > (uint32_t)kStackCap) {
-                                    if (lane == 0) set_err(status, PSG_ERR_STACK);
-                                    ssize = kStackCap;
-                                }
-                            }
-                        }
-                        __syncwarp();
-                    }
-                    if (MODE == MODE_LEAF && DEBUG && lane == 0) atomicMax(&status->max_stack, ssize);
-                }
-
-                // ---- L2L; for leaves L2P + P2P ----
-                ax = warp_sum(ax);
-                ay = warp_sum(ay);
-                az = warp_sum(az);
-                // L(u) = M2L(u) + L(parent)  (polesitter.h:1248-1250)
-                const float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
-                                             __fadd_rn(az, Lp.w));
-                if (lane == 0) tv.lt[u] = L;
-                if constexpr (MODE == MODE_INTERNAL) {
-                    if (lane == 0) {
-                        tv.ns_off[u] = (uint32_t)(ns_base + (unsigned long long)sub * cand_total);
-                        tv.ns_cnt[u] = ns_ok ? n_near : 0u;
+                    ssize -= kp;
+                    const uint32_t link = lane < kp ? tv.link[node] : 0u;
+                    const uint32_t nch = link >> 28;
+                    const uint32_t inc = warp_incl_scan(nch);
+                    tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+                    const uint32_t ex = inc - nch;
+                    for (uint32_t i = 0; i < nch; ++i) {
+                        sm.cand_node[ex + i] = (link & kLinkMask) + i;
+                        sm.cand_mask[ex + i] = (uint8_t)mask;
                     }
                 } else {
-                    // P2P sources: the staged ones (lane < fill) and spilled chunks
-                    const uint4 ui = tv.info[u];
-                    uint4 si0 = make_uint4(0, 0, 0, 0);
-                    if (lane < fill) si0 = tv.info[sm.p2p[lane]];
-                    unsigned long long inter = 0;
-                    for (uint32_t ti = 0; ti < ui.y; ++ti) {
-                        const float4 t = A.xyzm[ui.x + ti];
-                        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-                        p2p_leaf(A.xyzm, si0, t, A.kahan, bx, by, bz, cx, cy, cz);
-                        if (DEBUG) inter += si0.y;
-                        for (uint32_t c = head; c != kNone; c = A.p2p.next[c]) {
-                            if (lane < A.p2p.cnt[c]) {
-                                const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
-                                p2p_leaf(A.xyzm, si, t, A.kahan, bx, by, bz, cx, cy, cz);
-                                if (DEBUG) inter += si.y;
-                            }
-                        }
-                        // lane partials (compensated) summed in FP64
-                        const double sx = warp_sum((double)bx - (double)cx);
-                        const double sy = warp_sum((double)by - (double)cy);
-                        const double sz = warp_sum((double)bz - (double)cz);
-                        if (lane == 0) {
-                            const size_t gi = (size_t)ui.x + ti;
-                            const double mm = (double)t.w;
-                            A.fx[gi] = (float)(mm * ((double)L.y + sx));
-                            A.fy[gi] = (float)(mm * ((double)L.z + sy));
-                            A.fz[gi] = (float)(mm * ((double)L.w + sz));
+                    break;
+                }
+                __syncwarp();
+
+                // ---- test the candidates, one per lane; the next chunk's node
+                // records are loaded while the current one is processed ----
+                uint32_t n_s = 0, n_mask = 0, n_link = 0;
+                float4 n_g = make_float4(0.f, 0.f, 0.f, 0.f), n_mp = n_g;
+                if (lane < tot) {
+                    n_s = sm.cand_node[lane];
+                    n_mask = sm.cand_mask[lane];
+                    n_g = tv.geo[n_s];
+                    n_mp = tv.mp[n_s];
+                    n_link = tv.link[n_s];
+                }
+#pragma unroll 1
+                for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
+                    const uint32_t s = n_s, smask = n_mask, slink = n_link;
+                    const float4 sg = n_g, smp = n_mp;
+                    {
+                        const uint32_t jn = j0 + 32 + lane;
+                        n_mask = 0;
+                        if (jn < tot) {
+                            n_s = sm.cand_node[jn];
+                            n_mask = sm.cand_mask[jn];
+                            n_g = tv.geo[n_s];
+                            n_mp = tv.mp[n_s];
+                            n_link = tv.link[n_s];
                         }
                     }
-                    if (DEBUG) {
-                        inter = warp_sum(inter);
-                        if (lane == 0) {
-                            tv.dbg_p2p[u] = dbg_p2p;
-                            atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS], (unsigned long long)dbg_p2p);
-                            atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+                    const uint32_t chunk_mask = __reduce_or_sync(0xFFFFFFFFu, smask);
+                    uint32_t near_bits = 0;
+#pragma unroll
+                    for (uint32_t q = 0; q < 8; ++q) {
+                        if (!((chunk_mask >> q) & 1u)) continue;
+                        const float4 ug = sm.cgeo[q];
+                        float dx, dy, dz, d2;
+                        const bool act = (smask >> q) & 1u;
+                        const bool sep = mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z,
+                                                       sg.w, theta2, dx, dy, dz, d2) && act;
+                        // branch-free: every lane evaluates, only separated pairs add
+                        float fx, fy, fz;
+                        m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
+                        acc[q][0] += sep ? fx : 0.f;
+                        acc[q][1] += sep ? fy : 0.f;
+                        acc[q][2] += sep ? fz : 0.f;
+                        if (act && !sep) near_bits |= 1u << q;
+                        if (DEBUG) {
+                            const uint32_t bm = __ballot_sync(0xFFFFFFFFu, sep);
+                            if (lane == 0) sm.dbg_m2l[q] += __popc(bm);
+                        }
+                    }
+                    if constexpr (MODE == MODE_INTERNAL) {
+                        // near candidates of internal children: their near lists
+                        const uint32_t near_any = __reduce_or_sync(0xFFFFFFFFu, near_bits);
+#pragma unroll 1
+                        for (uint32_t m = near_any; m; m &= m - 1) {
+                            const uint32_t q = __ffs(m) - 1;
+                            const bool nr = (near_bits >> q) & 1u;
+                            const uint32_t nm = __ballot_sync(0xFFFFFFFFu, nr);
+                            const uint32_t base = sm.ns_cnt[q];
+                            if (ns_ok && nr) {
+                                const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
+                                A.ns[ns_base + (unsigned long long)sub * cand_total + base +
+                                     __popc(nm & lt_mask)] = s;
+                            }
+                            __syncwarp();
+                            if (lane == 0) sm.ns_cnt[q] = base + __popc(nm);
+                            __syncwarp();
+                        }
+                    } else {
+                        const bool sleaf = (slink >> 28) == 0;
+                        // near leaf candidate: a P2P source of these children
+                        const uint32_t pbits = sleaf ? near_bits : 0u;
+                        const uint32_t pb = __ballot_sync(0xFFFFFFFFu, pbits != 0);
+                        if (pb) {
+                            if (pfill + __popc(pb) > (uint32_t)kP2PCap) {
+                                phead = spill_p2p(sm, pfill, phead, A.p2p, status);
+                                pfill = 0;
+                            }
+                            if (pbits) {
+                                const uint32_t pos = pfill + __popc(pb & lt_mask);
+                                sm.p2p_node[pos] = s;
+                                sm.p2p_mask[pos] = (uint8_t)pbits;
+                            }
+                            pfill += __popc(pb);
+                            if (DEBUG) {
+                                const uint32_t pany = __reduce_or_sync(0xFFFFFFFFu, pbits);
+                                for (uint32_t m = pany; m; m &= m - 1) {
+                                    const uint32_t q = __ffs(m) - 1;
+                                    const uint32_t c =
+                                        __popc(__ballot_sync(0xFFFFFFFFu, (pbits >> q) & 1u));
+                                    if (lane == 0) sm.dbg_p2p[q] += c;
+                                }
+                            }
+                        }
+                        // near internal candidate: open it later for these children
+                        const uint32_t qbits = sleaf ? 0u : near_bits;
+                        const uint32_t qb = __ballot_sync(0xFFFFFFFFu, qbits != 0);
+                        if (qb) {
+                            const uint32_t pos = ssize + __popc(qb & lt_mask);
+                            if (qbits && pos < (uint32_t)kStackCap) {
+                                sm.stk_node[pos] = s;
+                                sm.stk_mask[pos] = (uint8_t)qbits;
+                            }
+                            ssize += __popc(qb);
+                            if (ssize > (uint32_t)kStackCap) {
+                                if (lane == 0) set_err(status, PSG_ERR_STACK);
+                                ssize = kStackCap;
+                            }
                         }
                     }
                     __syncwarp();
                 }
-                if (DEBUG && lane == 0) {
-                    tv.dbg_m2l[u] = dbg_m2l;
-                    atomicAdd(&status->stat[PSG_STAT_M2L], (unsigned long long)dbg_m2l);
+                if (MODE == MODE_LEAF && DEBUG && lane == 0) atomicMax(&status->max_stack, ssize);
+            }
+
+            // ---- L2L: L(u) = M2L(u) + L(parent)  (polesitter.h:1248-1250) ----
+#pragma unroll
+            for (uint32_t q = 0; q < 8; ++q) {
+                if (!((tgt_mask >> q) & 1u)) continue;
+                const float ax = warp_sum(acc[q][0]);
+                const float ay = warp_sum(acc[q][1]);
+                const float az = warp_sum(acc[q][2]);
+                const float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
+                                             __fadd_rn(az, Lp.w));
+                if (lane == 0) {
+                    const uint32_t u = fc + q;
+                    tv.lt[u] = L;
+                    if constexpr (MODE == MODE_LEAF) {
+                        sm.sL[q] = L;
+                    } else {
+                        const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
+                        tv.ns_off[u] = (uint32_t)(ns_base + (unsigned long long)sub * cand_total);
+                        tv.ns_cnt[u] = ns_ok ? sm.ns_cnt[q] : 0u;
+                    }
+                    if (DEBUG) {
+                        tv.dbg_m2l[u] = sm.dbg_m2l[q];
+                        atomicAdd(&status->stat[PSG_STAT_M2L], (unsigned long long)sm.dbg_m2l[q]);
+                    }
                 }
             }
             __syncwarp();
+
+            if constexpr (MODE == MODE_LEAF) {
+                // ---- L2P + P2P: F = m * (L(u) + sum of u's P2P sources) ----
+                for (uint32_t e = lane; e < pfill; e += 32) {
+                    const uint4 si = tv.info[sm.p2p_node[e]];
+                    sm.p2p_range[e] = make_uint2(si.x, si.y);
+                }
+                __syncwarp();
+                unsigned long long inter = 0;
+#pragma unroll 1
+                for (uint32_t m = tgt_mask; m; m &= m - 1) {
+                    const uint32_t q = __ffs(m) - 1;
+                    const uint2 up = sm.cpart[q];
+                    const float4 L = sm.sL[q];
+                    for (uint32_t ti = 0; ti < up.y; ++ti) {
+                        const float4 t = A.xyzm[up.x + ti];
+                        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+                        for (uint32_t e = lane; e < pfill; e += 32) {
+                            if ((sm.p2p_mask[e] >> q) & 1u) {
+                                const uint2 r = sm.p2p_range[e];
+                                p2p_range(A.xyzm, r, t, A.kahan, bx, by, bz, cx, cy, cz);
+                                if (DEBUG) inter += r.y;
+                            }
+                        }
+                        for (uint32_t c = phead; c != kNone; c = A.p2p.next[c]) {
+                            if (lane < A.p2p.cnt[c] &&
+                                ((A.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
+                                const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
+                                p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz,
+                                          cx, cy, cz);
+                                if (DEBUG) inter += si.y;
+                            }
+                        }
+                        const float sx = warp_sum(bx - cx);
+                        const float sy = warp_sum(by - cy);
+                        const float sz = warp_sum(bz - cz);
+                        if (lane == 0) {
+                            // final per-particle accumulation in FP64
+                            const size_t gi = (size_t)up.x + ti;
+                            const double mm = (double)t.w;
+                            A.fx[gi] = (float)(mm * ((double)L.y + (double)sx));
+                            A.fy[gi] = (float)(mm * ((double)L.z + (double)sy));
+                            A.fz[gi] = (float)(mm * ((double)L.w + (double)sz));
+                        }
+                    }
+                    if (DEBUG && lane == 0) {
+                        tv.dbg_p2p[fc + q] = sm.dbg_p2p[q];
+                        atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS],
+                                  (unsigned long long)sm.dbg_p2p[q]);
+                    }
+                }
+                if (DEBUG) {
+                    inter = warp_sum(inter);
+                    if (lane == 0) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+                }
+                __syncwarp();
+            }
         }
     }
 }

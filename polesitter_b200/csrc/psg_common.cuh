@@ -72,10 +72,12 @@ struct Status {
     uint32_t sort_tiles[4];                // onesweep tile tickets
 };
 
-// P2P source lists: chunk c holds cnt[c] source-leaf ids in
-// src[c * kP2PChunk ...] and links to the leaf's previous chunk via next[c].
+// P2P sources spilled from the traversal: chunk c holds cnt[c] source-leaf
+// ids in src[c * kP2PChunk ...], each with the set of the group's children it
+// serves in mask[...], and links to the group's previous chunk via next[c].
 struct P2PStore {
     uint32_t* src;
+    uint8_t* mask;
     uint32_t* next;
     uint32_t* cnt;
     uint32_t cap_chunks;

@@ -98,11 +98,13 @@ static int alloc_ns(State* s, unsigned long long cap) {
 }
 
 static int alloc_p2p(State* s, uint32_t chunks) {
-    void* ps[3] = {s->p2p.src, s->p2p.next, s->p2p.cnt};
+    void* ps[4] = {s->p2p.src, s->p2p.mask, s->p2p.next, s->p2p.cnt};
     for (void* p : ps)
         if (p) cudaFree(p);
     s->p2p.src = s->p2p.next = s->p2p.cnt = nullptr;
+    s->p2p.mask = nullptr;
     PSG_ALLOC(s->p2p.src, (size_t)chunks * kP2PChunk * 4);
+    PSG_ALLOC(s->p2p.mask, (size_t)chunks * kP2PChunk);
     PSG_ALLOC(s->p2p.next, (size_t)chunks * 4);
     PSG_ALLOC(s->p2p.cnt, (size_t)chunks * 4);
     s->p2p.cap_chunks = chunks;
@@ -150,7 +152,7 @@ static void free_state(State* s) {
                   s->sort.hist, s->sort.offs, s->sort.lookback, s->tree_tiles, s->tv.geo,
                   s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
                   s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->tv.link,
-                  s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.next, s->p2p.cnt,
+                  s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.mask, s->p2p.next, s->p2p.cnt,
                   s->d_status};
     for (void* p : ps)
         if (p) cudaFree(p);
@@ -215,7 +217,7 @@ static int init_state(State* s, size_t maxp, float theta) {
     std::memset(s->h_status, 0, sizeof(Status));
     int r = alloc_ns(s, (unsigned long long)(n < 1024 ? 1024 : n) * 48ull);
     if (r != PSG_OK) return r;
-    r = alloc_p2p(s, (uint32_t)(n < 4096 ? 4096 : n));
+    r = alloc_p2p(s, (uint32_t)(n < 4096 ? 4096 : n / 4));
     if (r != PSG_OK) return r;
     int bps = 0;
     PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, traverse_kernel_ptr(),
