@@ -79,6 +79,24 @@ ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,
                                               uint32_t* out_morton_codes, float* out_min_b,
                                               float* out_max_b, float* out_range);
 
+/* `ticks` iterations of the tick loop every polesitter caller writes around
+ * ps_calc_forces (README.md:65-111, demo/unary.c:117-189), run without
+ * leaving the device.  Each iteration:
+ *   ids[i] = i; ps_prepare_particles; ps_calc_forces with the root
+ *   c = min + range / 2, hw = range / 2 (README.md:76-80);
+ *   v[i] = v_before[ids[i]] for vx, vy, vz (README.md:82-93);
+ *   if mass[i] > 0: v += (f / m) * dt; x += v * dt (README.md:98-110).
+ * On return the arrays hold the state after the last iteration: positions,
+ * masses, ids and codes sorted as its calc left them, its forces, and the
+ * velocities in that order.  Every step rounds as the C loop does, so a
+ * loop over ps_prepare_particles + ps_calc_forces + the C update gives the
+ * same positions up to the forces' own rounding.  Arrays may be host memory
+ * (copied in once and out once) or device memory.  The first call
+ * allocates 6 x 4 B x max_particles of velocity scratch on ctx's device. */
+ps_result_t ps_b200_run_ticks(ps_context_t* ctx, const ps_particle_arrs_t* arrs,
+                              uint32_t* morton_codes, float* vx, float* vy, float* vz,
+                              float dt, uint32_t ticks);
+
 /* message of the last CUDA-side failure on this thread */
 const char* ps_b200_last_error(void);
 

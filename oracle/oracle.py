@@ -58,6 +58,7 @@ class Oracle:
         lib.pso_m2l_pair.restype = C.c_int
         lib.pso_m2l_pair.argtypes = [vp, vp, vp, f32, vp]
         lib.pso_p2p_pair.argtypes = [vp] * 7 + [C.c_uint32] * 4
+        lib.pso_euler_step.argtypes = [sz] + [vp] * 11 + [f32, vp]
         self.lib = lib
 
     def morton_encode(self, x, y, z) -> int:
@@ -127,6 +128,24 @@ class Oracle:
                         accum_mode, want_tree, want_p2p)
         out.update(codes=codes, min=mn, max=mx, range=rg, root_c=float(c), root_hw=float(hw))
         return out
+
+    def euler_step(self, p, vx, vy, vz, dt):
+        """The caller's update after a tick (README.md:82-111): permute the
+        velocities through ``p.id``, then semi-implicit Euler, in place."""
+        tmp = np.zeros(3 * p.n, np.float32)
+        self.lib.pso_euler_step(p.n, _ptr(p.id), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(p.x),
+                                _ptr(p.y), _ptr(p.z), _ptr(p.mass), _ptr(p.fx), _ptr(p.fy),
+                                _ptr(p.fz), dt, _ptr(tmp))
+
+    def run_ticks(self, p, vx, vy, vz, dt, ticks, theta=2.0):
+        """``ticks`` iterations of README.md:65-111: ids reset, prepare +
+        calc, velocity permutation, Euler.  Returns the last tick's codes."""
+        codes = None
+        for _ in range(ticks):
+            p.id[:] = np.arange(p.n, dtype=np.uint32)
+            codes = self.tick(p, theta=theta, want_tree=False)["codes"]
+            self.euler_step(p, vx, vy, vz, dt)
+        return codes
 
     def p2m(self, x, y, z, m, centre=(0.0, 0.0, 0.0)):
         a = [np.ascontiguousarray(v, np.float32) for v in (x, y, z, m)]

@@ -689,6 +689,40 @@ PSO_API void pso_direct_f64(size_t n, const float* x, const float* y,
 }
 
 /* ---------------------------------------------------------------------
+ * The caller's update after a tick (README.md:82-111, demo/unary.c:
+ * 146-184): velocities permuted through ids (v_new[i] = v[ids[i]]), then
+ * semi-implicit Euler for particles with positive mass.  vtmp holds 3 x n
+ * floats of scratch.
+ * ------------------------------------------------------------------- */
+PSO_API void pso_euler_step(size_t n, const uint32_t* ids, float* vx, float* vy,
+                            float* vz, float* x, float* y, float* z,
+                            const float* m, const float* fx, const float* fy,
+                            const float* fz, float dt, float* vtmp) {
+    for (size_t i = 0; i < n; ++i) {
+        uint32_t old   = ids[i];
+        vtmp[i]        = vx[old];
+        vtmp[n + i]    = vy[old];
+        vtmp[2 * n + i] = vz[old];
+    }
+    for (size_t i = 0; i < n; ++i) {
+        vx[i] = vtmp[i];
+        vy[i] = vtmp[n + i];
+        vz[i] = vtmp[2 * n + i];
+    }
+    for (size_t i = 0; i < n; ++i) {
+        if (m[i] <= 0.0F) {
+            continue;
+        }
+        vx[i] += (fx[i] / m[i]) * dt;
+        vy[i] += (fy[i] / m[i]) * dt;
+        vz[i] += (fz[i] / m[i]) * dt;
+        x[i] += vx[i] * dt;
+        y[i] += vy[i] * dt;
+        z[i] += vz[i] * dt;
+    }
+}
+
+/* ---------------------------------------------------------------------
  * Single-pass helpers mirroring the hand-built node tests of the reference
  * (tests/main.c:235-476, tests/accuracy.c:74-109).
  * ------------------------------------------------------------------- */

@@ -31,7 +31,7 @@ EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
             "ps_b200_context_size", "ps_b200_set_option", "ps_b200_set_morton_variant",
             "ps_b200_get_stats", "ps_b200_last_timing", "ps_b200_tree_nodes",
             "ps_b200_tree_dump", "ps_b200_direct_f64", "ps_b200_last_error",
-            "ps_b200_prepare_particles_noalloc")
+            "ps_b200_prepare_particles_noalloc", "ps_b200_run_ticks")
 
 
 class ParticleArrs(C.Structure):
@@ -97,6 +97,8 @@ def lib() -> C.CDLL:
     L.ps_b200_prepare_particles_noalloc.restype = C.c_int
     L.ps_b200_prepare_particles_noalloc.argtypes = [C.POINTER(ParticleArrs), vp, C.POINTER(f32),
                                                     C.POINTER(f32), C.POINTER(f32)]
+    L.ps_b200_run_ticks.restype = C.c_int
+    L.ps_b200_run_ticks.argtypes = [vp, C.POINTER(ParticleArrs), vp, vp, vp, vp, f32, C.c_uint32]
     _LIB = L
     return L
 
@@ -176,6 +178,14 @@ class Context:
         c, hw = root_box(mn, rg)
         self.calc_forces(p, codes, c, c, c, hw)
         return mn, mx, rg
+
+    def run_ticks(self, p, codes, vx, vy, vz, dt: float, ticks: int):
+        """``ticks`` iterations of the caller's tick loop on the device
+        (README.md:65-111): ids reset, prepare, calc, velocity permutation
+        through ids, semi-implicit Euler (ps_b200_run_ticks)."""
+        arrs = arrs_of(p)
+        _check("ps_b200_run_ticks", lib().ps_b200_run_ticks(
+            self.ptr, C.byref(arrs), _addr(codes), _addr(vx), _addr(vy), _addr(vz), dt, ticks))
 
     def set_option(self, key: int, value: float):
         _check("ps_b200_set_option", lib().ps_b200_set_option(self.ptr, key, value))

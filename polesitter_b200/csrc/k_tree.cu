@@ -173,7 +173,15 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
                                                            const uint32_t* __restrict__ tile_off,
                                                            TreeView tv, const Status* status,
                                                            float cx, float cy, float cz,
-                                                           float hw) {
+                                                           float hw,
+                                                           const float* __restrict__ bbox) {
+    if (bbox) {
+        // root from a device-side bounding box (min, max, range), as the
+        // caller's loop derives it: c = min + range / 2, hw = range / 2
+        // (README.md:76-78)
+        hw = __fdiv_rn(bbox[2], 2.0f);
+        cx = cy = cz = __fadd_rn(bbox[0], hw);
+    }
     const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
     uint32_t f[kTreePer];
     thread_flags(codes, n, p0, f);
@@ -315,11 +323,12 @@ __global__ void __launch_bounds__(256) k_upward_level(TreeView tv, const Status*
 
 void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView tv,
                  Status* status, float cx, float cy, float cz, float hw, int grid,
-                 cudaStream_t st) {
+                 cudaStream_t st, const float* bbox) {
     const int tiles = (int)((n + kTreeTile - 1) / kTreeTile);
     k_tree_count<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf);
     k_tree_scan<<<1, 1024, 0, st>>>(tile_buf, tiles, tv, status);
-    k_tree_emit<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf, tv, status, cx, cy, cz, hw);
+    k_tree_emit<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf, tv, status, cx, cy, cz, hw,
+                                                bbox);
     k_tree_link<<<grid, 256, 0, st>>>(tv, status);
 }
 

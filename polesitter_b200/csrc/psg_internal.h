@@ -87,6 +87,9 @@ int psg_tree_dump(void* state, size_t cap, int32_t* depth, uint32_t* start,
 int psg_last_timing(void* state, float* out_ms, size_t n_out);
 int psg_direct_f64(void* state, const psg_arrays_t* a, const uint32_t* targets, size_t n_t,
                    double* out);
+/* the caller's tick loop on the device (k_tick.cu) */
+int psg_run_ticks(void* state, const psg_arrays_t* a, float* vx, float* vy, float* vz, float dt,
+                  uint32_t ticks, int morton_variant);
 const char* psg_last_error(void);
 void psg_set_error(const char* msg);
 

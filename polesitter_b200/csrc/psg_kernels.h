@@ -39,7 +39,7 @@ void launch_writeback(const float4* xyzm, const uint32_t* ids, size_t n, float* 
 int tree_tile_size();
 void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView tv,
                  Status* status, float cx, float cy, float cz, float hw, int grid,
-                 cudaStream_t st);
+                 cudaStream_t st, const float* bbox = nullptr);
 void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int grid,
                    cudaStream_t st);
 
@@ -52,6 +52,26 @@ const void* traverse_internal_kernel_ptr();
 void launch_traverse_internal(const TravArgs& A, int level, int grid, cudaStream_t st);
 void launch_traverse_leaves(const TravArgs& A, int grid, cudaStream_t st);
 
+
+// k_tick.cu -- the caller's tick loop on the device (README.md:65-111)
+struct TickState {
+    const uint32_t* id;   // sorted -> pre-sort index, from this tick's sort
+    const float* vx_in;   // velocities in the previous tick's order
+    const float* vy_in;
+    const float* vz_in;
+    float* vx_out;        // velocities in this tick's (sorted) order
+    float* vy_out;
+    float* vz_out;
+    float* x;             // sorted positions, advanced in place
+    float* y;
+    float* z;
+    const float* m;
+    const float* fx;
+    const float* fy;
+    const float* fz;
+};
+void launch_tick_reset_ids(uint32_t* id, size_t n, int grid, cudaStream_t st);
+void launch_tick_euler(const TickState& t, size_t n, float dt, int grid, cudaStream_t st);
 
 // k_direct.cu -- FP64 direct-sum forces for sampled targets (tests/accuracy.c:42-72)
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,

@@ -80,6 +80,12 @@ struct State {
     unsigned long long stats[24];
     uint32_t last_nodes;
     uint32_t lvl_count[kLevels];  // node counts of the last completed tick
+    // device tick loop scratch (allocated by its first call)
+    int tk_grid;
+    float2* tk_partial;
+    float* tk_bbox;
+    float* tk_v[3];
+    float* tk_vmir[3];
 };
 
 static int grid_for(const State* s, size_t n, int per_block_items) {
@@ -153,7 +159,8 @@ static void free_state(State* s) {
                   s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
                   s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->tv.link,
                   s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.mask, s->p2p.next, s->p2p.cnt,
-                  s->d_status};
+                  s->d_status, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
+                  s->tk_vmir[0], s->tk_vmir[1], s->tk_vmir[2]};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->h_status) cudaFreeHost(s->h_status);
@@ -293,110 +300,208 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
     return PSG_EOOM;
 }
 
+// the caller's arrays as the GPU sees them: in place when it can reach them,
+// else device mirrors in the context
+struct DevArrays {
+    float *x, *y, *z, *m, *fx, *fy, *fz;
+    uint32_t *id, *codes;
+    bool dev[9];
+    bool any_host;
+};
+
+static int map_arrays(State* s, const psg_arrays_t* a, DevArrays& d, bool upload_codes) {
+    const size_t n = a->n;
+    d.x = a->x; d.y = a->y; d.z = a->z; d.m = a->mass;
+    d.fx = a->fx; d.fy = a->fy; d.fz = a->fz; d.id = a->id; d.codes = a->codes;
+    void* ps[9] = {d.x, d.y, d.z, d.m, d.fx, d.fy, d.fz, d.id, d.codes};
+    d.any_host = false;
+    for (int i = 0; i < 9; ++i) {
+        d.dev[i] = on_device(ps[i]);
+        d.any_host |= !d.dev[i];
+    }
+    if (!d.any_host) return PSG_OK;
+    int r = ensure_mirror(s->mir, s->max_particles);
+    if (r != PSG_OK) return r;
+    struct { void* h; void* dv; bool in; } io[9] = {
+        {a->x, s->mir.x, true}, {a->y, s->mir.y, true}, {a->z, s->mir.z, true},
+        {a->mass, s->mir.m, true}, {a->fx, s->mir.fx, false}, {a->fy, s->mir.fy, false},
+        {a->fz, s->mir.fz, false}, {a->id, s->mir.id, true}, {a->codes, s->mir.codes, upload_codes}};
+    for (int i = 0; i < 9; ++i)
+        if (!d.dev[i] && io[i].in)
+            PSG_CHECK(cudaMemcpyAsync(io[i].dv, io[i].h, n * 4, cudaMemcpyHostToDevice, s->stream));
+    if (!d.dev[0]) d.x = s->mir.x;
+    if (!d.dev[1]) d.y = s->mir.y;
+    if (!d.dev[2]) d.z = s->mir.z;
+    if (!d.dev[3]) d.m = s->mir.m;
+    if (!d.dev[4]) d.fx = s->mir.fx;
+    if (!d.dev[5]) d.fy = s->mir.fy;
+    if (!d.dev[6]) d.fz = s->mir.fz;
+    if (!d.dev[7]) d.id = s->mir.id;
+    if (!d.dev[8]) d.codes = s->mir.codes;
+    return PSG_OK;
+}
+
+static int unmap_arrays(State* s, const psg_arrays_t* a, const DevArrays& d) {
+    if (!d.any_host) return PSG_OK;
+    struct { void* h; void* dv; } out[9] = {
+        {a->x, d.x}, {a->y, d.y}, {a->z, d.z}, {a->mass, d.m}, {a->fx, d.fx},
+        {a->fy, d.fy}, {a->fz, d.fz}, {a->id, d.id}, {a->codes, d.codes}};
+    for (int i = 0; i < 9; ++i)
+        if (!d.dev[i])
+            PSG_CHECK(cudaMemcpyAsync(out[i].h, out[i].dv, a->n * 4, cudaMemcpyDeviceToHost,
+                                      s->stream));
+    return PSG_OK;
+}
+
+// ps_calc_forces on device-resident arrays: sort -> gather -> tree -> upward
+// -> traversal (polesitter.h:1840-1909).  The root is (cx, cy, cz, hw), or,
+// when bbox is set, derived on the device from this tick's bounding box.
+static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy, float cz,
+                     float hw, const float* bbox) {
+    cudaStream_t st = s->stream;
+    record(s, PH_BEGIN);
+    PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
+    const int g = grid_for(s, n, 1024);
+    launch_sort(s->sort, d.codes, n, g, s->d_status, st);
+    record(s, PH_SORT);
+    launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
+    launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
+    record(s, PH_GATHER);
+    const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
+    if (s->debug) {
+        PSG_CHECK(cudaMemsetAsync(s->tv.dbg_m2l, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
+        PSG_CHECK(cudaMemsetAsync(s->tv.dbg_p2p, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
+    }
+    launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, cx, cy, cz, hw, gt, st, bbox);
+    record(s, PH_TREE);
+    launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
+    record(s, PH_UP);
+    PSG_CHECK(cudaGetLastError());
+    uint32_t err = 0;
+    if (n == 1) {
+        // a single particle: the root is a leaf and its only P2P term is
+        // the zero self-interaction (polesitter.h:1279-1449)
+        PSG_CHECK(cudaMemsetAsync(d.fx, 0, 4, st));
+        PSG_CHECK(cudaMemsetAsync(d.fy, 0, 4, st));
+        PSG_CHECK(cudaMemsetAsync(d.fz, 0, 4, st));
+        record(s, PH_TRAV);
+        record(s, PH_END);
+        PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
+                                  cudaMemcpyDeviceToHost, st));
+        PSG_CHECK(cudaStreamSynchronize(st));
+        err = s->h_status->err;
+    } else {
+        int r = run_traversal(s, s->xyzm, d.fx, d.fy, d.fz, &err);
+        if (r != PSG_OK) return r;
+    }
+    if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK)) {
+        std::snprintf(g_err, sizeof(g_err), "device status error 0x%x", err);
+        return PSG_EDEVICE;
+    }
+    if (err & PSG_ERR_NODES) {
+        std::snprintf(g_err, sizeof(g_err), "morton codes not sorted/30-bit (0x%x)", err);
+        return PSG_EINVAL;
+    }
+    uint32_t nodes = 0;
+    for (int k = 0; k <= kMaxDepth; ++k) {
+        s->lvl_count[k] = s->h_status->lvl_count[k];
+        nodes += s->lvl_count[k];
+    }
+    s->last_nodes = nodes;
+    for (int i = 0; i < 8; ++i) s->stats[i] = s->h_status->stat[i];
+    s->stats[8] = nodes;
+    s->stats[9] = s->h_status->max_stack;
+    for (int i = 8; i < 16; ++i) s->stats[i + 8] = s->h_status->stat[i];
+    s->stats[10] = s->h_status->p2p_chunks;
+    if (s->timing) {
+        const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END};
+        for (int i = 0; i + 1 < 7; ++i)
+            cudaEventElapsedTime(&s->ms[i], s->ev[order[i]], s->ev[order[i + 1]]);
+        cudaEventElapsedTime(&s->ms[6], s->ev[PH_BEGIN], s->ev[PH_END]);
+    }
+    return PSG_OK;
+}
+
 static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, float hw) {
     const size_t n = a->n;
     if (n > s->max_particles) return PSG_EINVAL;
     if (n == 0) return PSG_OK;
     PSG_CHECK(cudaSetDevice(s->device));
+    DevArrays d;
+    int r = map_arrays(s, a, d, true);
+    if (r != PSG_OK) return r;
+    r = tick_core(s, d, n, cx, cy, cz, hw, nullptr);
+    if (r != PSG_OK) return r;
+    r = unmap_arrays(s, a, d);
+    if (r != PSG_OK) return r;
+    PSG_CHECK(cudaStreamSynchronize(s->stream));
+    return PSG_OK;
+}
+
+// `ticks` iterations of the caller's loop (README.md:65-111) without leaving
+// the device: ids reset, prepare, calc with the root derived on the device,
+// velocities permuted through ids, semi-implicit Euler.  Host arrays are
+// copied in once and out once.
+static int run_ticks(State* s, const psg_arrays_t* a, float* vx, float* vy, float* vz, float dt,
+                     uint32_t ticks, int variant) {
+    const size_t n = a->n;
+    if (n > s->max_particles) return PSG_EINVAL;
+    if (n == 0 || ticks == 0) return PSG_OK;
+    PSG_CHECK(cudaSetDevice(s->device));
     cudaStream_t st = s->stream;
-    // caller arrays: use them in place when the GPU can reach them, else mirror
-    float* x = a->x; float* y = a->y; float* z = a->z; float* m = a->mass;
-    float* fx = a->fx; float* fy = a->fy; float* fz = a->fz;
-    uint32_t* id = a->id; uint32_t* codes = a->codes;
-    const bool dev[9] = {on_device(x), on_device(y), on_device(z), on_device(m), on_device(fx),
-                         on_device(fy), on_device(fz), on_device(id), on_device(codes)};
-    bool any_host = false;
-    for (bool d : dev) any_host |= !d;
-    if (any_host) {
-        int r = ensure_mirror(s->mir, s->max_particles);
-        if (r != PSG_OK) return r;
-        struct { void* h; void* d; bool in; } io[9] = {
-            {x, s->mir.x, true}, {y, s->mir.y, true}, {z, s->mir.z, true}, {m, s->mir.m, true},
-            {fx, s->mir.fx, false}, {fy, s->mir.fy, false}, {fz, s->mir.fz, false},
-            {id, s->mir.id, true}, {codes, s->mir.codes, true}};
-        for (int i = 0; i < 9; ++i)
-            if (!dev[i] && io[i].in)
-                PSG_CHECK(cudaMemcpyAsync(io[i].d, io[i].h, n * 4, cudaMemcpyHostToDevice, st));
-        if (!dev[0]) x = s->mir.x;
-        if (!dev[1]) y = s->mir.y;
-        if (!dev[2]) z = s->mir.z;
-        if (!dev[3]) m = s->mir.m;
-        if (!dev[4]) fx = s->mir.fx;
-        if (!dev[5]) fy = s->mir.fy;
-        if (!dev[6]) fz = s->mir.fz;
-        if (!dev[7]) id = s->mir.id;
-        if (!dev[8]) codes = s->mir.codes;
+    if (!s->tk_bbox) {
+        s->tk_grid = s->sms * 4;
+        PSG_ALLOC(s->tk_partial, s->tk_grid * sizeof(float2));
+        PSG_ALLOC(s->tk_bbox, 4 * sizeof(float));
+        for (int c = 0; c < 3; ++c) PSG_ALLOC(s->tk_v[c], s->max_particles * 4);
+        for (int c = 0; c < 3; ++c) PSG_ALLOC(s->tk_vmir[c], s->max_particles * 4);
     }
-    record(s, PH_BEGIN);
-    PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
-    {
-        const int g = grid_for(s, n, 1024);
-        launch_sort(s->sort, codes, n, g, s->d_status, st);
-        record(s, PH_SORT);
-        launch_gather(s->sort.perm, x, y, z, m, id, n, s->xyzm, s->ids, g, st);
-        launch_writeback(s->xyzm, s->ids, n, x, y, z, m, id, g, st);
-        record(s, PH_GATHER);
-        const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
-        if (s->debug) {
-            PSG_CHECK(cudaMemsetAsync(s->tv.dbg_m2l, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
-            PSG_CHECK(cudaMemsetAsync(s->tv.dbg_p2p, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
-        }
-        launch_tree(codes, n, s->tree_tiles, s->tv, s->d_status, cx, cy, cz, hw, gt, st);
-        record(s, PH_TREE);
-        launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
-        record(s, PH_UP);
-        PSG_CHECK(cudaGetLastError());
-        uint32_t err = 0;
-        if (n == 1) {
-            // a single particle: the root is a leaf and its only P2P term is
-            // the zero self-interaction (polesitter.h:1279-1449)
-            PSG_CHECK(cudaMemsetAsync(fx, 0, 4, st));
-            PSG_CHECK(cudaMemsetAsync(fy, 0, 4, st));
-            PSG_CHECK(cudaMemsetAsync(fz, 0, 4, st));
-            record(s, PH_TRAV);
-            record(s, PH_END);
-            PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
-                                      cudaMemcpyDeviceToHost, st));
-            PSG_CHECK(cudaStreamSynchronize(st));
-            err = s->h_status->err;
+    DevArrays d;
+    int r = map_arrays(s, a, d, false);
+    if (r != PSG_OK) return r;
+    float* vh[3] = {vx, vy, vz};
+    float* vin[3];
+    float* vout[3];
+    for (int c = 0; c < 3; ++c) {
+        if (on_device(vh[c])) {
+            vin[c] = vh[c];
         } else {
-            int r = run_traversal(s, s->xyzm, fx, fy, fz, &err);
-            if (r != PSG_OK) return r;
+            vin[c] = s->tk_vmir[c];
+            PSG_CHECK(cudaMemcpyAsync(vin[c], vh[c], n * 4, cudaMemcpyHostToDevice, st));
         }
-        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK)) {
-            std::snprintf(g_err, sizeof(g_err), "device status error 0x%x", err);
-            return PSG_EDEVICE;
-        }
-        if (err & PSG_ERR_NODES) {
-            std::snprintf(g_err, sizeof(g_err), "morton codes not sorted/30-bit (0x%x)", err);
-            return PSG_EINVAL;
-        }
-        uint32_t nodes = 0;
-        for (int d = 0; d <= kMaxDepth; ++d) {
-            s->lvl_count[d] = s->h_status->lvl_count[d];
-            nodes += s->lvl_count[d];
-        }
-        s->last_nodes = nodes;
-        for (int i = 0; i < 8; ++i) s->stats[i] = s->h_status->stat[i];
-        s->stats[8] = nodes;
-        s->stats[9] = s->h_status->max_stack;
-        for (int i = 8; i < 16; ++i) s->stats[i + 8] = s->h_status->stat[i];
-        s->stats[10] = s->h_status->p2p_chunks;
-        if (s->timing) {
-            const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END};
-            for (int i = 0; i + 1 < 7; ++i)
-                cudaEventElapsedTime(&s->ms[i], s->ev[order[i]], s->ev[order[i + 1]]);
-            cudaEventElapsedTime(&s->ms[6], s->ev[PH_BEGIN], s->ev[PH_END]);
+        vout[c] = s->tk_v[c];
+    }
+    float* const vdst[3] = {vin[0], vin[1], vin[2]};
+    const int g = grid_for(s, n, 1024);
+    int gp = (int)((n + 1023) / 1024);
+    if (gp > s->tk_grid) gp = s->tk_grid;
+    for (uint32_t t = 0; t < ticks; ++t) {
+        launch_tick_reset_ids(d.id, n, g, st);
+        launch_prepare(d.x, d.y, d.z, n, s->tk_partial, gp, d.codes, s->tk_bbox, variant, st);
+        r = tick_core(s, d, n, 0.f, 0.f, 0.f, 0.f, s->tk_bbox);
+        if (r != PSG_OK) return r;
+        TickState ts;
+        ts.id = d.id;
+        ts.vx_in = vin[0]; ts.vy_in = vin[1]; ts.vz_in = vin[2];
+        ts.vx_out = vout[0]; ts.vy_out = vout[1]; ts.vz_out = vout[2];
+        ts.x = d.x; ts.y = d.y; ts.z = d.z; ts.m = d.m;
+        ts.fx = d.fx; ts.fy = d.fy; ts.fz = d.fz;
+        launch_tick_euler(ts, n, dt, g, st);
+        PSG_CHECK(cudaGetLastError());
+        for (int c = 0; c < 3; ++c) {
+            float* tmp = vin[c];
+            vin[c] = vout[c];
+            vout[c] = tmp;
         }
     }
-    if (any_host) {
-        struct { void* h; void* d; } out[9] = {
-            {a->x, x}, {a->y, y}, {a->z, z}, {a->mass, m}, {a->fx, fx},
-            {a->fy, fy}, {a->fz, fz}, {a->id, id}, {a->codes, codes}};
-        for (int i = 0; i < 9; ++i)
-            if (!dev[i]) PSG_CHECK(cudaMemcpyAsync(out[i].h, out[i].d, n * 4,
-                                                   cudaMemcpyDeviceToHost, st));
+    for (int c = 0; c < 3; ++c) {
+        if (vin[c] != vdst[c])
+            PSG_CHECK(cudaMemcpyAsync(vdst[c], vin[c], n * 4, cudaMemcpyDeviceToDevice, st));
+        if (vdst[c] != vh[c])
+            PSG_CHECK(cudaMemcpyAsync(vh[c], vdst[c], n * 4, cudaMemcpyDeviceToHost, st));
     }
+    r = unmap_arrays(s, a, d);
+    if (r != PSG_OK) return r;
     PSG_CHECK(cudaStreamSynchronize(st));
     return PSG_OK;
 }
@@ -498,6 +603,13 @@ int psg_calc(void* mem, const psg_arrays_t* a, float cx, float cy, float cz, flo
     State* s = static_cast<State*>(mem);
     if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
     return psg::calc(s, a, cx, cy, cz, hw);
+}
+
+int psg_run_ticks(void* mem, const psg_arrays_t* a, float* vx, float* vy, float* vz, float dt,
+                  uint32_t ticks, int variant) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
+    return psg::run_ticks(s, a, vx, vy, vz, dt, ticks, variant);
 }
 
 int psg_set_option(void* mem, int key, double value) {

@@ -190,6 +190,33 @@ ps_result_t ps_b200_direct_f64(ps_context_t* ctx, const ps_particle_arrs_t* arrs
     return to_ps(psg_direct_f64(ctx_state(ctx), &a, targets, n_targets, out));
 }
 
+ps_result_t ps_b200_run_ticks(ps_context_t* ctx, const ps_particle_arrs_t* arrs,
+                              uint32_t* morton_codes, float* vx, float* vy, float* vz,
+                              float dt, uint32_t ticks) {
+    if (!ctx || !arrs || ctx->magic != PS_CTX_MAGIC) {
+        return PS_EINVAL;
+    }
+    if (arrs->cnt == 0 || ticks == 0) {
+        return PS_OK;
+    }
+    if (!morton_codes || !arrs->x || !arrs->y || !arrs->z || !arrs->mass || !arrs->fx ||
+        !arrs->fy || !arrs->fz || !arrs->id || !vx || !vy || !vz) {
+        return PS_EINVAL;
+    }
+    psg_arrays_t a;
+    a.x = arrs->x;
+    a.y = arrs->y;
+    a.z = arrs->z;
+    a.mass = arrs->mass;
+    a.fx = arrs->fx;
+    a.fy = arrs->fy;
+    a.fz = arrs->fz;
+    a.id = arrs->id;
+    a.codes = morton_codes;
+    a.n = arrs->cnt;
+    return to_ps(psg_run_ticks(ctx_state(ctx), &a, vx, vy, vz, dt, ticks, g_morton_variant));
+}
+
 const char* ps_b200_last_error(void) { return psg_last_error(); }
 
 ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,

@@ -176,3 +176,30 @@ def test_other_morton_variants_vs_formula(oracle, variant):
                 q.append(min(max(t, 0), 1023))
         want.append(oracle.morton_encode(*q))
     assert codes.tolist() == want
+
+
+def test_euler_step_follows_the_readme_loop(oracle):
+    # README.md:82-111: v_new[i] = v[ids[i]]; massive particles get
+    # v += (f / m) * dt and x += v * dt, rounded as written
+    f = np.float32
+    rng = np.random.default_rng(3)
+    n = 257
+    p = W.uniform_cube(n, 4)
+    p.id[:] = rng.permutation(n).astype(np.uint32)
+    p.mass[::5] = 0.0
+    for k in ("fx", "fy", "fz"):
+        getattr(p, k)[:] = rng.normal(size=n).astype(np.float32)
+    v = [rng.normal(size=n).astype(np.float32) for _ in range(3)]
+    dt = f(0.016)
+    want_v = [vv[p.id].copy() for vv in v]
+    want_x = [p.x.copy(), p.y.copy(), p.z.copy()]
+    for i in range(n):
+        if p.mass[i] <= 0:
+            continue
+        for c, fc in enumerate((p.fx, p.fy, p.fz)):
+            want_v[c][i] = f(want_v[c][i] + f(f(fc[i] / p.mass[i]) * dt))
+            want_x[c][i] = f(want_x[c][i] + f(want_v[c][i] * dt))
+    oracle.euler_step(p, *v, float(dt))
+    for c in range(3):
+        assert np.array_equal(v[c], want_v[c])
+    assert np.array_equal(p.x, want_x[0]) and np.array_equal(p.z, want_x[2])
