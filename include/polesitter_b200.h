@@ -20,6 +20,8 @@ size_t ps_b200_context_size(void);
 #define PS_B200_OPT_THETA 2          /* change theta after ps_init */
 #define PS_B200_OPT_TIMING 4         /* time tick phases with CUDA events */
 #define PS_B200_OPT_KAHAN 6          /* compensated (Kahan) FP32 sums in P2P */
+#define PS_B200_OPT_CLOSURE 7        /* learned far-field closure, see below */
+#define PS_B200_OPT_JUDGE 8          /* 1: run the closure's judge in mode 1 too */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
 
 /* Morton quantisation of ps_prepare_particles, process-wide (it takes no
@@ -29,7 +31,9 @@ ps_result_t ps_b200_set_morton_variant(int variant);
 
 /* counters of the last tick: [1] M2L pairs, [2] P2P leaf pairs, [3] P2P
  * particle pairs, [9] deepest traversal stack (these need
- * PS_B200_OPT_DEBUG), [8] nodes, [10] P2P list chunks */
+ * PS_B200_OPT_DEBUG), [8] nodes, [10] P2P list chunks, [11] traversal runs
+ * (> 1 when a capacity had to grow), [12] particles in the fullest leaf,
+ * [13] full-leaf P2P work records */
 ps_result_t ps_b200_get_stats(ps_context_t* ctx, uint64_t* out, size_t n);
 
 /* per-phase device times of the last tick in ms (PS_B200_OPT_TIMING):
@@ -96,6 +100,57 @@ ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,
 ps_result_t ps_b200_run_ticks(ps_context_t* ctx, const ps_particle_arrs_t* arrs,
                               uint32_t* morton_codes, float* vx, float* vy, float* vz,
                               float dt, uint32_t ticks);
+
+/* ---- learned far-field closure (no counterpart in the reference) --------
+ *
+ * PS_B200_OPT_CLOSURE selects the far field of later ticks:
+ *   0  the reference's (default): order-0 local expansion, additive L2L;
+ *      every result is the reference's.
+ *   1  order-1 local expansion: M2L also accumulates the gradient G of each
+ *      monopole's field, L2L shifts the parent's field to the child's centre
+ *      (L += G (c_child - c_parent)) and L2P evaluates L + G (x - c) at each
+ *      particle.  Same interaction set as mode 0.
+ *   2  mode 1 plus a learned correction: an MLP (16 -> 64 -> 64 -> 64 -> 8,
+ *      GELU, BF16 weights, FP32 accumulation, on the tensor cores) maps each
+ *      particle's leaf field, field gradient, offset in the leaf and leaf
+ *      depth to a force correction.  Each tick an FP64 direct sum on a
+ *      sample of 4096 particles judges it: the correction is applied only
+ *      when it lowers the sample's median relative error, else the mode-1
+ *      forces stand.  Needs weights (ps_b200_closure_set_weights).
+ * The parameter vector is PS_B200_CLOSURE_PARAMS floats:
+ *   W1[16][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64][8] b4[8]
+ * (W[in][out]; inputs 13..15 and outputs 3..7 are padding). */
+#define PS_B200_CLOSURE_PARAMS 9928
+ps_result_t ps_b200_closure_set_weights(ps_context_t* ctx, const float* params, size_t n);
+
+/* the judge of the last tick: median relative force error of the sample
+ * without and with the correction, whether it was applied, sample size
+ * (0 when no judge ran) */
+ps_result_t ps_b200_closure_last(ps_context_t* ctx, double* median_base, double* median_mlp,
+                                 int* used, int* samples);
+
+/* after a tick in mode >= 1: the network inputs x (k x 16) and the output
+ * scale m s / 100 (k) of the sorted particles idx[0..k) (host arrays) */
+ps_result_t ps_b200_closure_features(ps_context_t* ctx, const uint32_t* idx, size_t k,
+                                     float* x_out, float* scale_out);
+
+/* after a tick in mode 2: every particle's correction (n x 3, sorted order,
+ * host array), whether or not the judge applied it */
+ps_result_t ps_b200_closure_correction(ps_context_t* ctx, float* out, size_t n);
+
+/* the network on given inputs (host arrays): y (n x 8) = MLP(x (n x 16)) */
+ps_result_t ps_b200_closure_forward(ps_context_t* ctx, const float* x, size_t n,
+                                    const float* params, float* y_out);
+
+/* training on the GPU with the project's own kernels: the mean squared error
+ * over outputs 0..2 of MLP(x) against t (n x 3) and its gradient for one
+ * batch (grad), or Adam over `epochs` shuffled passes of `batch` samples
+ * (params in: initial values, out: trained; loss_out: per-epoch MSE) */
+ps_result_t ps_b200_closure_grad(ps_context_t* ctx, const float* x, const float* t, size_t n,
+                                 const float* params, float* grad_out, float* loss_out);
+ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float* t, size_t n,
+                                  float* params, uint32_t epochs, uint32_t batch, float lr,
+                                  uint64_t seed, float* loss_out);
 
 /* message of the last CUDA-side failure on this thread */
 const char* ps_b200_last_error(void);

@@ -59,6 +59,7 @@ class Oracle:
         lib.pso_m2l_pair.argtypes = [vp, vp, vp, f32, vp]
         lib.pso_p2p_pair.argtypes = [vp] * 7 + [C.c_uint32] * 4
         lib.pso_euler_step.argtypes = [sz] + [vp] * 11 + [f32, vp]
+        lib.pso_set_closure.argtypes = [vp, C.c_int, vp]
         self.lib = lib
 
     def morton_encode(self, x, y, z) -> int:
@@ -76,10 +77,15 @@ class Oracle:
                           _ptr(p.z), _ptr(p.mass))
 
     def calc(self, p, codes, cx, cy, cz, hw, theta=2.0, mt=True, accum_mode=0,
-             want_tree=True, want_p2p=False):
-        """ps_calc_forces on arrays that are already sorted (``sort``)."""
+             want_tree=True, want_p2p=False, order=0, feat=None):
+        """ps_calc_forces on arrays that are already sorted (``sort``).
+        ``order`` 1 selects the closure's order-1 local expansion; ``feat``
+        (n x 16 float32) then receives the raw per-particle closure features."""
         h = self.lib.pso_new()
         try:
+            if order or feat is not None:
+                assert feat is None or (feat.dtype == np.float32 and feat.shape == (p.n, 16))
+                self.lib.pso_set_closure(h, order, None if feat is None else _ptr(feat))
             rc = self.lib.pso_calc(h, p.n, _ptr(codes), _ptr(p.x), _ptr(p.y), _ptr(p.z),
                                    _ptr(p.mass), _ptr(p.fx), _ptr(p.fy), _ptr(p.fz),
                                    cx, cy, cz, hw, theta, int(mt), accum_mode)
@@ -116,7 +122,7 @@ class Oracle:
             self.lib.pso_free(h)
 
     def tick(self, p, theta=2.0, variant=MORTON_AVX2, mt=True, accum_mode=0,
-             want_tree=True, want_p2p=False):
+             want_tree=True, want_p2p=False, order=0, feat=None):
         """prepare + calc on ``p`` in place (arrays end sorted, forces set)."""
         rc, codes, mn, mx, rg = self.prepare(p, variant)
         assert rc == 0
@@ -125,7 +131,7 @@ class Oracle:
         hw = f32(rg) / f32(2.0)
         self.sort(p, codes)
         out = self.calc(p, codes, float(c), float(c), float(c), float(hw), theta, mt,
-                        accum_mode, want_tree, want_p2p)
+                        accum_mode, want_tree, want_p2p, order, feat)
         out.update(codes=codes, min=mn, max=mx, range=rg, root_c=float(c), root_hw=float(hw))
         return out
 

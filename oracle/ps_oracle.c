@@ -206,6 +206,7 @@ typedef struct {
     float    mp[4];              /* multipole (:370) */
     float    l_m2l[4];           /* M2L sum received by this node */
     float    l_tot[4];           /* local_exp after the downward pass */
+    float    g_m2l[6], g_tot[6]; /* closure order 1: field gradient (xx yy zz xy xz yz) */
     uint32_t start, count;       /* particle range */
     uint32_t first_child, nchild;
     uint32_t parent;
@@ -228,6 +229,8 @@ typedef struct {
     const float *x, *y, *z, *m;
     float        theta;
     int          accum_mode; /* 0: reference lane structure; 1: plain */
+    int          order;      /* closure: 0 reference (order-0 local), 1 order-1 */
+    float*       feat;       /* closure: raw per-particle features, 16 each */
 } pso_ctx_t;
 
 PSO_API void* pso_new(void) { return calloc(1, sizeof(pso_ctx_t)); }
@@ -430,6 +433,18 @@ static void pso_interact(pso_ctx_t* c, uint32_t ti, uint32_t si) {
         float fdx   = (mx * inv_r3) - (dx * coeff);
         float fdy   = (my * inv_r3) - (dy * coeff);
         float fdz   = (mz * inv_r3) - (dz * coeff);
+        if (c->order >= 1) {
+            /* closure order 1: gradient of the monopole field at the target
+             * centre, d(m0 d ir3)/d(target) = m0 (3 d d^T ir5 - I ir3) */
+            float g3 = 3.0F * m0 * inv_r5;
+            float gi = m0 * inv_r3;
+            t->g_m2l[0] += g3 * dx * dx - gi;
+            t->g_m2l[1] += g3 * dy * dy - gi;
+            t->g_m2l[2] += g3 * dz * dz - gi;
+            t->g_m2l[3] += g3 * dx * dy;
+            t->g_m2l[4] += g3 * dx * dz;
+            t->g_m2l[5] += g3 * dy * dz;
+        }
         t->l_m2l[1] += fmx + fdx;
         t->l_m2l[2] += fmy + fdy;
         t->l_m2l[3] += fmz + fdz;
@@ -543,6 +558,75 @@ static void pso_p2p_leaves(pso_ctx_t* c, const pso_node_t* t,
     }
 }
 
+/* Closure order 1 (no counterpart in the reference): the downward pass with
+ * an order-1 local expansion.  L2L shifts the parent's field to the child's
+ * centre, L(u) = M2L(u) + L(p) + G(p) (c_u - c_p), G(u) = M2L_G(u) + G(p);
+ * L2P evaluates F_i = m_i (L + G (x_i - c)) at the particle.  With c->feat
+ * set it also records each particle's raw closure features: L (3), G (6),
+ * x_i - c (3), leaf half width, leaf depth, m_i, 0. */
+static void pso_downward_order1(pso_ctx_t* c, size_t n, float* fx, float* fy,
+                                float* fz) {
+    (void)n;
+    for (size_t k = 0; k < c->n_nodes; ++k) {
+        pso_node_t* nd = &c->nodes[k];
+        for (int a = 0; a < 4; ++a) {
+            nd->l_tot[a] = nd->l_m2l[a];
+        }
+        for (int a = 0; a < 6; ++a) {
+            nd->g_tot[a] = nd->g_m2l[a];
+        }
+        if (k > 0) {
+            const pso_node_t* p = &c->nodes[nd->parent];
+            const float*      G = p->g_tot;
+            float ux = nd->x - p->x, uy = nd->y - p->y, uz = nd->z - p->z;
+            nd->l_tot[1] += p->l_tot[1] + (G[0] * ux + G[3] * uy + G[4] * uz);
+            nd->l_tot[2] += p->l_tot[2] + (G[3] * ux + G[1] * uy + G[5] * uz);
+            nd->l_tot[3] += p->l_tot[3] + (G[4] * ux + G[5] * uy + G[2] * uz);
+            for (int a = 0; a < 6; ++a) {
+                nd->g_tot[a] += G[a];
+            }
+        }
+        if (!pso_is_leaf(nd)) {
+            continue;
+        }
+        const float* G = nd->g_tot;
+        for (uint32_t i = 0; i < nd->count; ++i) {
+            uint32_t idx = nd->start + i;
+            float ux = c->x[idx] - nd->x, uy = c->y[idx] - nd->y, uz = c->z[idx] - nd->z;
+            float lx = nd->l_tot[1] + (G[0] * ux + G[3] * uy + G[4] * uz);
+            float ly = nd->l_tot[2] + (G[3] * ux + G[1] * uy + G[5] * uz);
+            float lz = nd->l_tot[3] + (G[4] * ux + G[5] * uy + G[2] * uz);
+            fx[idx] += c->m[idx] * lx;
+            fy[idx] += c->m[idx] * ly;
+            fz[idx] += c->m[idx] * lz;
+            if (c->feat) {
+                float* f = c->feat + 16 * (size_t)idx;
+                f[0] = nd->l_tot[1];
+                f[1] = nd->l_tot[2];
+                f[2] = nd->l_tot[3];
+                for (int a = 0; a < 6; ++a) {
+                    f[3 + a] = G[a];
+                }
+                f[9]  = ux;
+                f[10] = uy;
+                f[11] = uz;
+                f[12] = nd->hw;
+                f[13] = (float)nd->depth;
+                f[14] = c->m[idx];
+                f[15] = 0.0F;
+            }
+        }
+    }
+}
+
+/* closure mode of the next pso_calc: order 0 = the reference, 1 = order-1
+ * local expansion; feat (16 floats per particle) may be NULL */
+PSO_API void pso_set_closure(void* h, int order, float* feat) {
+    pso_ctx_t* c = (pso_ctx_t*)h;
+    c->order = order;
+    c->feat  = feat;
+}
+
 /* ps_calc_forces (polesitter.h:1840-1909) on arrays already sorted by
  * pso_sort: build -> upward -> M2L (MT dispatch unless mt == 0) ->
  * downward L2L (:1238-1251, :1820-1835) + L2P (:1224-1233) -> P2P. */
@@ -571,7 +655,10 @@ PSO_API int pso_calc(void* h, size_t n, const uint32_t* codes, const float* x,
     pso_upward(c);
     pso_dispatch(c, 0, 0, mt);
     /* downward: L_total(child) = L_m2l(child) + L_total(parent) */
-    for (size_t k = 0; k < c->n_nodes; ++k) {
+    if (c->order >= 1) {
+        pso_downward_order1(c, n, fx, fy, fz);
+    }
+    for (size_t k = 0; c->order == 0 && k < c->n_nodes; ++k) {
         pso_node_t* nd = &c->nodes[k];
         for (int a = 0; a < 4; ++a) {
             nd->l_tot[a] = nd->l_m2l[a];

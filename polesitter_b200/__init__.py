@@ -24,14 +24,18 @@ PS_OK, PS_EOOM, PS_EINVAL, PS_ETHRD, PS_EALLOC, PS_EDEVICE = 0, -1, -2, -3, -4, 
 RESULT_NAMES = {0: "PS_OK", -1: "PS_EOOM", -2: "PS_EINVAL", -3: "PS_ETHRD",
                 -4: "PS_EALLOC", -5: "PS_EDEVICE"}
 
-OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN = 1, 2, 4, 6
+OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN, OPT_CLOSURE, OPT_JUDGE = 1, 2, 4, 6, 7, 8
+CLOSURE_PARAMS = 9928
 MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 
 EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
             "ps_b200_context_size", "ps_b200_set_option", "ps_b200_set_morton_variant",
             "ps_b200_get_stats", "ps_b200_last_timing", "ps_b200_tree_nodes",
             "ps_b200_tree_dump", "ps_b200_direct_f64", "ps_b200_last_error",
-            "ps_b200_prepare_particles_noalloc", "ps_b200_run_ticks")
+            "ps_b200_prepare_particles_noalloc", "ps_b200_run_ticks",
+            "ps_b200_closure_set_weights", "ps_b200_closure_last", "ps_b200_closure_features",
+            "ps_b200_closure_correction", "ps_b200_closure_forward", "ps_b200_closure_grad",
+            "ps_b200_closure_train")
 
 
 class ParticleArrs(C.Structure):
@@ -97,6 +101,18 @@ def lib() -> C.CDLL:
     L.ps_b200_prepare_particles_noalloc.restype = C.c_int
     L.ps_b200_prepare_particles_noalloc.argtypes = [C.POINTER(ParticleArrs), vp, C.POINTER(f32),
                                                     C.POINTER(f32), C.POINTER(f32)]
+    L.ps_b200_closure_set_weights.argtypes = [vp, vp, sz]
+    L.ps_b200_closure_last.argtypes = [vp, vp, vp, vp, vp]
+    L.ps_b200_closure_features.argtypes = [vp, vp, sz, vp, vp]
+    L.ps_b200_closure_correction.argtypes = [vp, vp, sz]
+    L.ps_b200_closure_forward.argtypes = [vp, vp, sz, vp, vp]
+    L.ps_b200_closure_grad.argtypes = [vp, vp, vp, sz, vp, vp, vp]
+    L.ps_b200_closure_train.argtypes = [vp, vp, vp, sz, vp, C.c_uint32, C.c_uint32, f32,
+                                        C.c_uint64, vp]
+    for name in ("ps_b200_closure_set_weights", "ps_b200_closure_last", "ps_b200_closure_features",
+                 "ps_b200_closure_correction", "ps_b200_closure_forward", "ps_b200_closure_grad",
+                 "ps_b200_closure_train"):
+        getattr(L, name).restype = C.c_int
     L.ps_b200_run_ticks.restype = C.c_int
     L.ps_b200_run_ticks.argtypes = [vp, C.POINTER(ParticleArrs), vp, vp, vp, vp, f32, C.c_uint32]
     _LIB = L
@@ -187,6 +203,74 @@ class Context:
         _check("ps_b200_run_ticks", lib().ps_b200_run_ticks(
             self.ptr, C.byref(arrs), _addr(codes), _addr(vx), _addr(vy), _addr(vz), dt, ticks))
 
+    # ---- learned far-field closure (ps_b200_closure_*) ----
+    def set_closure(self, mode: int):
+        """0: the reference's far field, 1: order-1 local expansion, 2: order-1
+        plus the learned correction under the sampled FP64 judge."""
+        self.set_option(OPT_CLOSURE, mode)
+
+    def closure_set_weights(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, np.float32)
+        _check("ps_b200_closure_set_weights",
+               lib().ps_b200_closure_set_weights(self.ptr, p.ctypes.data, p.size))
+
+    def closure_last(self) -> dict:
+        mb, mm = C.c_double(), C.c_double()
+        used, smp = C.c_int(), C.c_int()
+        _check("ps_b200_closure_last", lib().ps_b200_closure_last(
+            self.ptr, C.byref(mb), C.byref(mm), C.byref(used), C.byref(smp)))
+        return {"median_base": mb.value, "median_mlp": mm.value, "used": bool(used.value),
+                "samples": smp.value}
+
+    def closure_features(self, idx):
+        import numpy as np
+        ix = np.ascontiguousarray(idx, np.uint32)
+        x = np.zeros((ix.size, 16), np.float32)
+        sc = np.zeros(ix.size, np.float32)
+        _check("ps_b200_closure_features", lib().ps_b200_closure_features(
+            self.ptr, ix.ctypes.data, ix.size, x.ctypes.data, sc.ctypes.data))
+        return x, sc
+
+    def closure_correction(self, n: int):
+        import numpy as np
+        out = np.zeros((n, 3), np.float32)
+        _check("ps_b200_closure_correction",
+               lib().ps_b200_closure_correction(self.ptr, out.ctypes.data, n))
+        return out
+
+    def closure_forward(self, x, params):
+        import numpy as np
+        xx = np.ascontiguousarray(x, np.float32)
+        p = np.ascontiguousarray(params, np.float32)
+        y = np.zeros((xx.shape[0], 8), np.float32)
+        _check("ps_b200_closure_forward", lib().ps_b200_closure_forward(
+            self.ptr, xx.ctypes.data, xx.shape[0], p.ctypes.data, y.ctypes.data))
+        return y
+
+    def closure_grad(self, x, t, params):
+        import numpy as np
+        xx = np.ascontiguousarray(x, np.float32)
+        tt = np.ascontiguousarray(t, np.float32)
+        p = np.ascontiguousarray(params, np.float32)
+        g = np.zeros_like(p)
+        loss = C.c_float()
+        _check("ps_b200_closure_grad", lib().ps_b200_closure_grad(
+            self.ptr, xx.ctypes.data, tt.ctypes.data, xx.shape[0], p.ctypes.data, g.ctypes.data,
+            C.byref(loss)))
+        return g, loss.value
+
+    def closure_train(self, x, t, params, epochs: int, batch: int, lr: float, seed: int = 0):
+        import numpy as np
+        xx = np.ascontiguousarray(x, np.float32)
+        tt = np.ascontiguousarray(t, np.float32)
+        p = np.array(params, np.float32)
+        losses = np.zeros(max(epochs, 1), np.float32)
+        _check("ps_b200_closure_train", lib().ps_b200_closure_train(
+            self.ptr, xx.ctypes.data, tt.ctypes.data, xx.shape[0], p.ctypes.data, epochs, batch,
+            lr, seed, losses.ctypes.data))
+        return p, losses[:epochs]
+
     def set_option(self, key: int, value: float):
         _check("ps_b200_set_option", lib().ps_b200_set_option(self.ptr, key, value))
 
@@ -198,6 +282,8 @@ class Context:
                 "p2p_interactions": int(out[3]), "chunks_first": int(out[4]),
                 "chunks_dfs": int(out[5]), "tests_first": int(out[6]), "tests_dfs": int(out[7]),
                 "nodes": int(out[8]), "max_stack": int(out[9]), "p2p_chunks": int(out[10]),
+                "traversal_runs": int(out[11]), "max_leaf": int(out[12]),
+                "dense_records": int(out[13]),
                 "lanes": int(out[16]), "leaf_groups": int(out[17]), "dfs_steps": int(out[18])}
 
     def timing(self) -> dict:
@@ -206,7 +292,7 @@ class Context:
         _check("ps_b200_last_timing", lib().ps_b200_last_timing(self.ptr, out.ctypes.data, 8))
         return {"sort": float(out[0]), "gather": float(out[1]), "tree": float(out[2]),
                 "upward": float(out[3]), "internal": float(out[4]), "leaves": float(out[5]),
-                "tick": float(out[6])}
+                "tick": float(out[6]), "closure": float(out[7])}
 
     def tree(self) -> dict:
         import numpy as np

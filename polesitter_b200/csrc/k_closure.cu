@@ -1,0 +1,581 @@
+// The learned far-field closure (no counterpart in the reference): per-particle
+// features from the order-1 local expansion, the MLP correction on the tensor
+// cores (BF16 mma.sync m16n8k16, FP32 accumulation), the sampled FP64 judge
+// with fallback to the uncorrected forces, and the training kernels
+// (forward on the tensor cores, backward and Adam in FP32).
+//
+// Features of particle i in leaf u (half width h, depth d), with the leaf's
+// field L and field gradient G after the order-1 downward pass:
+//   s = |L| + h |G|_F
+//   x = (L / s, G h / s [xx yy zz xy xz yz], (x_i - c_u) / h, d / 10, 0, 0, 0)
+// and the correction is dF_i = m_i s kMlpOutScale MLP(x).
+//
+// Bounds: the MLP is ~2 x 9.9K flop per particle on the BF16 tensor pipe and
+// reads ~80 B per particle; the judge is 4096 x N FP64 pair terms.
+#include <cfloat>
+#include <cuda_bf16.h>
+
+#include "psg_closure.cuh"
+#include "psg_common.cuh"
+#include "psg_kernels.h"
+
+namespace psg {
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ float bf16_bits_to_float(uint16_t h) {
+    return __uint_as_float((uint32_t)h << 16);
+}
+
+__device__ __forceinline__ uint16_t float_to_bf16_bits(float f) {
+    __nv_bfloat16 b = __float2bfloat16_rn(f);
+    return *reinterpret_cast<uint16_t*>(&b);
+}
+
+// D += A (16x16, row) . B (16x8, col), BF16 in, FP32 accumulate
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+__device__ __forceinline__ float gelu(float x) {
+    const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+    return 0.5f * x * (1.0f + tanhf(u));
+}
+
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float x2 = x * x;
+    const float u = 0.7978845608028654f * fmaf(0.044715f * x, x2, x);
+    const float th = tanhf(u);
+    return fmaf(0.5f * x * (1.0f - th * th) * 0.7978845608028654f, fmaf(0.134145f, x2, 1.0f),
+                0.5f * (1.0f + th));
+}
+
+// One warp, 16 rows: C[16 x 8 NT] = A[16 x 16 KC] . W, A as m16n8k16
+// A-fragments, W as Wt[out][in] (row stride LD) in shared memory.
+template <int KC, int NT, int LD>
+__device__ __forceinline__ void warp_layer(const uint32_t (&a)[KC][4], const uint16_t* wt,
+                                           float (&c)[NT][4]) {
+    const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
+        const uint16_t* row = wt + (nt * 8 + g) * LD + 2 * t;
+#pragma unroll
+        for (int kc = 0; kc < KC; ++kc) {
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(row + kc * 16);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + kc * 16 + 8);
+            mma_bf16(c[nt], a[kc], b0, b1);
+        }
+    }
+}
+
+// z = c + b; h = GELU(z) rounded to BF16 and repacked as the next layer's
+// A-fragments (k-chunk kc = n-tiles 2kc and 2kc+1).  With STORE, z (FP32) and
+// h (BF16 bits) also go to shared memory rows [16][64] for the backward pass.
+template <bool STORE>
+__device__ __forceinline__ void act_to_frag(float (&c)[8][4], const float* bias,
+                                            uint32_t (&a)[4][4], float* zrow, uint16_t* hrow) {
+    const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const int col = nt * 8 + 2 * t;
+        const float z0 = c[nt][0] + bias[col], z1 = c[nt][1] + bias[col + 1];
+        const float z2 = c[nt][2] + bias[col], z3 = c[nt][3] + bias[col + 1];
+        const uint32_t lo = pack_bf16x2(gelu(z0), gelu(z1));
+        const uint32_t hi = pack_bf16x2(gelu(z2), gelu(z3));
+        const int kc = nt >> 1, half = nt & 1;
+        a[kc][half ? 2 : 0] = lo;
+        a[kc][half ? 3 : 1] = hi;
+        if constexpr (STORE) {
+            zrow[g * kMlpHid + col] = z0;
+            zrow[g * kMlpHid + col + 1] = z1;
+            zrow[(g + 8) * kMlpHid + col] = z2;
+            zrow[(g + 8) * kMlpHid + col + 1] = z3;
+            *reinterpret_cast<uint32_t*>(hrow + g * kMlpHid + col) = lo;
+            *reinterpret_cast<uint32_t*>(hrow + (g + 8) * kMlpHid + col) = hi;
+        }
+    }
+}
+
+// input fragments from feat[16][17] (FP32), rounded to BF16
+__device__ __forceinline__ void input_frag(const float (*feat)[17], uint32_t (&a)[1][4]) {
+    const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+    a[0][0] = pack_bf16x2(feat[g][2 * t], feat[g][2 * t + 1]);
+    a[0][1] = pack_bf16x2(feat[g + 8][2 * t], feat[g + 8][2 * t + 1]);
+    a[0][2] = pack_bf16x2(feat[g][2 * t + 8], feat[g][2 * t + 9]);
+    a[0][3] = pack_bf16x2(feat[g + 8][2 * t + 8], feat[g + 8][2 * t + 9]);
+}
+
+// the whole network on 16 rows; y[16][9] receives the 8 outputs
+template <bool STORE>
+__device__ __forceinline__ void warp_mlp(const MlpPacked& w, const float (*feat)[17],
+                                         float (*y)[9], float* z1, float* z2, float* z3,
+                                         uint16_t* h1, uint16_t* h2, uint16_t* h3) {
+    const uint32_t lane = lane_id(), g = lane >> 2, t = lane & 3;
+    uint32_t a0[1][4];
+    input_frag(feat, a0);
+    float c[8][4];
+    uint32_t a[4][4];
+    warp_layer<1, 8, kLd1>(a0, w.wt1, c);
+    act_to_frag<STORE>(c, w.b1, a, z1, h1);
+    warp_layer<4, 8, kLdH>(a, w.wt2, c);
+    act_to_frag<STORE>(c, w.b2, a, z2, h2);
+    warp_layer<4, 8, kLdH>(a, w.wt3, c);
+    act_to_frag<STORE>(c, w.b3, a, z3, h3);
+    float o[1][4];
+    warp_layer<4, 1, kLdH>(a, w.wt4, o);
+    y[g][2 * t] = o[0][0] + w.b4[2 * t];
+    y[g][2 * t + 1] = o[0][1] + w.b4[2 * t + 1];
+    y[g + 8][2 * t] = o[0][2] + w.b4[2 * t];
+    y[g + 8][2 * t + 1] = o[0][3] + w.b4[2 * t + 1];
+}
+
+// features of sorted particle i; returns m_i s kMlpOutScale
+__device__ __forceinline__ float closure_features(const TreeView& tv,
+                                                  const uint32_t* __restrict__ leaf_of,
+                                                  const float4* __restrict__ xyzm, size_t i,
+                                                  float* x) {
+    const uint32_t u = leaf_of[i];
+    if (u >= tv.lvl_base[kLevels]) {  // no leaf recorded: no features, no correction
+        for (int k = 0; k < 16; ++k) x[k] = 0.f;
+        return 0.f;
+    }
+    const float4 L = tv.lt[u];
+    const float4 g0 = tv.lg0[u];
+    const float2 g1 = tv.lg1[u];
+    const float4 c = tv.geo[u];
+    const float4 p = xyzm[i];
+    int depth = 0;
+#pragma unroll
+    for (int d = 1; d <= kMaxDepth; ++d) depth += u >= tv.lvl_base[d] ? 1 : 0;
+    const float h = c.w;
+    const float gn = sqrtf(g0.x * g0.x + g0.y * g0.y + g0.z * g0.z +
+                           2.0f * (g0.w * g0.w + g1.x * g1.x + g1.y * g1.y));
+    const float s = sqrtf(L.y * L.y + L.z * L.z + L.w * L.w) + h * gn + 1e-30f;
+    const float is = 1.0f / s;
+    const float gh = h * is;
+    const float ih = 1.0f / h;
+    x[0] = L.y * is;
+    x[1] = L.z * is;
+    x[2] = L.w * is;
+    x[3] = g0.x * gh;
+    x[4] = g0.y * gh;
+    x[5] = g0.z * gh;
+    x[6] = g0.w * gh;
+    x[7] = g1.x * gh;
+    x[8] = g1.y * gh;
+    x[9] = (p.x - c.x) * ih;
+    x[10] = (p.y - c.y) * ih;
+    x[11] = (p.z - c.z) * ih;
+    x[12] = 0.1f * (float)depth;
+    x[13] = x[14] = x[15] = 0.f;
+    return p.w * s * kMlpOutScale;
+}
+
+__device__ __forceinline__ void load_packed(MlpPacked& dst, const MlpPacked* src) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) d[i] = s[i];
+}
+
+// ---- inference: dF for every particle of the last tick -------------------
+__global__ void __launch_bounds__(128) k_closure_mlp(TreeView tv, const uint32_t* leaf_of,
+                                                     const float4* __restrict__ xyzm, size_t n,
+                                                     const MlpPacked* __restrict__ wts,
+                                                     float4* __restrict__ dF) {
+    __shared__ __align__(16) MlpPacked sw;
+    __shared__ float feat[4][16][17];
+    __shared__ float ysm[4][16][9];
+    __shared__ float scl[4][16];
+    load_packed(sw, wts);
+    __syncthreads();
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const size_t tiles = (n + 15) / 16;
+    for (size_t tile = (size_t)blockIdx.x * 4 + w; tile < tiles; tile += (size_t)gridDim.x * 4) {
+        const size_t i = tile * 16 + lane;
+        if (lane < 16) {
+            float x[16];
+            float sc = 0.f;
+            if (i < n) {
+                sc = closure_features(tv, leaf_of, xyzm, i, x);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; ++k) x[k] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) feat[w][lane][k] = x[k];
+            scl[w][lane] = sc;
+        }
+        __syncwarp();
+        warp_mlp<false>(sw, feat[w], ysm[w], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        __syncwarp();
+        if (lane < 16 && i < n) {
+            const float sc = scl[w][lane];
+            dF[i] = make_float4(sc * ysm[w][lane][0], sc * ysm[w][lane][1], sc * ysm[w][lane][2],
+                                0.f);
+        }
+        __syncwarp();
+    }
+}
+
+// the network on given inputs x[n][16] -> y[n][8] (checks of the tensor-core path)
+__global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x, size_t n,
+                                                     const MlpPacked* __restrict__ wts,
+                                                     float* __restrict__ y) {
+    __shared__ __align__(16) MlpPacked sw;
+    __shared__ float feat[4][16][17];
+    __shared__ float ysm[4][16][9];
+    load_packed(sw, wts);
+    __syncthreads();
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const size_t tiles = (n + 15) / 16;
+    for (size_t tile = (size_t)blockIdx.x * 4 + w; tile < tiles; tile += (size_t)gridDim.x * 4) {
+        const size_t i = tile * 16 + lane;
+        if (lane < 16)
+            for (int k = 0; k < 16; ++k) feat[w][lane][k] = i < n ? x[i * 16 + k] : 0.f;
+        __syncwarp();
+        warp_mlp<false>(sw, feat[w], ysm[w], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        __syncwarp();
+        if (lane < 16 && i < n)
+            for (int o = 0; o < kMlpOut; ++o) y[i * kMlpOut + o] = ysm[w][lane][o];
+        __syncwarp();
+    }
+}
+
+// features (and scale) of selected particles, for building training data
+__global__ void __launch_bounds__(256) k_closure_features(TreeView tv, const uint32_t* leaf_of,
+                                                          const float4* __restrict__ xyzm,
+                                                          size_t n, const uint32_t* idx,
+                                                          size_t k, float* __restrict__ x_out,
+                                                          float* __restrict__ scale_out) {
+    const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    const uint32_t i = idx[j];
+    float x[16];
+    float sc = 0.f;
+    if (i < n) {
+        sc = closure_features(tv, leaf_of, xyzm, i, x);
+    } else {
+        for (int q = 0; q < 16; ++q) x[q] = 0.f;
+    }
+    for (int q = 0; q < 16; ++q) x_out[j * 16 + q] = x[q];
+    scale_out[j] = sc;
+}
+
+// ---- judge ----------------------------------------------------------------
+__global__ void k_judge_sample(uint32_t* tg, int s, size_t n, uint32_t tick) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= s) return;
+    const size_t stride = n / (size_t)s;
+    const size_t off = stride > 1 ? ((size_t)tick * 7919u) % stride : 0;
+    size_t i = (size_t)k * n / (size_t)s + off;
+    tg[k] = (uint32_t)(i < n ? i : n - 1);
+}
+
+// medians of the per-sample relative errors with and without the correction;
+// the correction is used only when its median is lower
+__global__ void __launch_bounds__(1024) k_judge_decide(const uint32_t* tg, int s,
+                                                       const double* f64, const float* fx,
+                                                       const float* fy, const float* fz,
+                                                       const float4* dF, int allow,
+                                                       JudgeOut* out) {
+    __shared__ float e0[kJudgeSamples], e1[kJudgeSamples];
+    for (int k = threadIdx.x; k < kJudgeSamples; k += blockDim.x) {
+        float a = FLT_MAX, b = FLT_MAX;
+        if (k < s) {
+            const uint32_t i = tg[k];
+            const double rx = f64[3 * k], ry = f64[3 * k + 1], rz = f64[3 * k + 2];
+            const double nr = sqrt(rx * rx + ry * ry + rz * rz);
+            const double bx = (double)fx[i] - rx, by = (double)fy[i] - ry, bz = (double)fz[i] - rz;
+            const float4 d = dF[i];
+            const double cx = bx + d.x, cy = by + d.y, cz = bz + d.z;
+            const double den = nr > 1e-300 ? nr : 1e-300;
+            a = (float)(sqrt(bx * bx + by * by + bz * bz) / den);
+            b = (float)(sqrt(cx * cx + cy * cy + cz * cz) / den);
+        }
+        e0[k] = a;
+        e1[k] = b;
+    }
+    __syncthreads();
+    // bitonic sort, ascending, both arrays
+    for (int size = 2; size <= kJudgeSamples; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < kJudgeSamples; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    float x = e0[i], y = e0[j];
+                    if ((x > y) == up) {
+                        e0[i] = y;
+                        e0[j] = x;
+                    }
+                    x = e1[i];
+                    y = e1[j];
+                    if ((x > y) == up) {
+                        e1[i] = y;
+                        e1[j] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        double m0 = 0.0, m1 = 0.0;
+        if (s > 0) {
+            if (s & 1) {
+                m0 = e0[s / 2];
+                m1 = e1[s / 2];
+            } else {
+                m0 = 0.5 * ((double)e0[s / 2 - 1] + (double)e0[s / 2]);
+                m1 = 0.5 * ((double)e1[s / 2 - 1] + (double)e1[s / 2]);
+            }
+        }
+        out->median_base = m0;
+        out->median_mlp = m1;
+        out->use_mlp = (allow && s > 0 && m1 < m0) ? 1 : 0;
+        out->samples = s;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_closure_apply(float* fx, float* fy, float* fz,
+                                                       const float4* __restrict__ dF, size_t n,
+                                                       const JudgeOut* j) {
+    if (!j->use_mlp) return;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float4 d = dF[i];
+        fx[i] += d.x;
+        fy[i] += d.y;
+        fz[i] += d.z;
+    }
+}
+
+// ---- parameters -------------------------------------------------------------
+// FP32 parameter vector -> BF16 transposed weights + FP32 biases
+__global__ void k_mlp_pack(const float* __restrict__ p, MlpPacked* __restrict__ out) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    for (int e = tid; e < kMlpHid * kLd1; e += stride) {
+        const int o = e / kLd1, i = e % kLd1;
+        out->wt1[e] = float_to_bf16_bits(i < kMlpIn ? p[kOffW1 + i * kMlpHid + o] : 0.f);
+    }
+    for (int e = tid; e < kMlpHid * kLdH; e += stride) {
+        const int o = e / kLdH, i = e % kLdH;
+        out->wt2[e] = float_to_bf16_bits(i < kMlpHid ? p[kOffW2 + i * kMlpHid + o] : 0.f);
+        out->wt3[e] = float_to_bf16_bits(i < kMlpHid ? p[kOffW3 + i * kMlpHid + o] : 0.f);
+    }
+    for (int e = tid; e < kMlpOut * kLdH; e += stride) {
+        const int o = e / kLdH, i = e % kLdH;
+        out->wt4[e] = float_to_bf16_bits(i < kMlpHid ? p[kOffW4 + i * kMlpOut + o] : 0.f);
+    }
+    for (int e = tid; e < kMlpHid; e += stride) {
+        out->b1[e] = p[kOffB1 + e];
+        out->b2[e] = p[kOffB2 + e];
+        out->b3[e] = p[kOffB3 + e];
+    }
+    for (int e = tid; e < kMlpOut; e += stride) out->b4[e] = p[kOffB4 + e];
+}
+
+// ---- training ---------------------------------------------------------------
+constexpr int kTrainRows = 64;  // samples per block (4 warps x 16)
+
+struct TrainSmem {
+    MlpPacked w;
+    uint16_t h0[kTrainRows * kMlpIn];   // BF16 inputs
+    uint16_t h1[kTrainRows * kMlpHid];  // BF16 activations
+    uint16_t h2[kTrainRows * kMlpHid];
+    uint16_t h3[kTrainRows * kMlpHid];
+    float z1[kTrainRows * kMlpHid];     // FP32 pre-activations
+    float z2[kTrainRows * kMlpHid];
+    float z3[kTrainRows * kMlpHid];
+    float da[kTrainRows * kMlpHid];     // gradients, ping-pong
+    float db[kTrainRows * kMlpHid];
+    float dy[kTrainRows * kMlpOut];
+    float feat[4][16][17];
+    float y[4][16][9];
+};
+
+size_t mlp_train_smem_bytes() { return sizeof(TrainSmem); }
+
+// dW[k][n] += sum_b h[b][k] d[b][n]  and  db[n] += sum_b d[b][n]
+__device__ __forceinline__ void accum_dw(const uint16_t* h, int K, const float* d, int N,
+                                         float* gW, float* gB) {
+    for (int e = threadIdx.x; e < K * N; e += blockDim.x) {
+        const int n = e / K, k = e % K;
+        float sum = 0.f;
+        for (int b = 0; b < kTrainRows; ++b) sum = fmaf(bf16_bits_to_float(h[b * K + k]), d[b * N + n], sum);
+        atomicAdd(&gW[k * N + n], sum);
+    }
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        float sum = 0.f;
+        for (int b = 0; b < kTrainRows; ++b) sum += d[b * N + e];
+        atomicAdd(&gB[e], sum);
+    }
+}
+
+// dnext[b][k] = (sum_n d[b][n] W[k][n]) * GELU'(z[b][k]), W[k][n] = Wt[n][k]
+__device__ __forceinline__ void back_act(const float* d, int N, const uint16_t* wt, int ld,
+                                         const float* z, float* dnext) {
+    for (int e = threadIdx.x; e < kTrainRows * kMlpHid; e += blockDim.x) {
+        const int b = e / kMlpHid, k = e % kMlpHid;
+        float sum = 0.f;
+        for (int n = 0; n < N; ++n) sum = fmaf(d[b * N + n], bf16_bits_to_float(wt[n * ld + k]), sum);
+        dnext[e] = sum * gelu_grad(z[e]);
+    }
+}
+
+// Loss sum_{samples, outputs 0..2} (y - t)^2 and its gradient, scaled by
+// inv_norm, accumulated into grad (FP32 parameter layout) and loss_sum.
+__global__ void __launch_bounds__(128) k_mlp_grad(const float* __restrict__ X,
+                                                  const float* __restrict__ T,
+                                                  const uint32_t* __restrict__ perm, size_t b0,
+                                                  size_t count, const MlpPacked* __restrict__ wts,
+                                                  float inv_norm, float* __restrict__ grad,
+                                                  float* __restrict__ loss_sum) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
+    load_packed(S.w, wts);
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const size_t r_blk = (size_t)blockIdx.x * kTrainRows;
+    // inputs of this warp's 16 rows
+    if (lane < 16) {
+        const size_t r = r_blk + w * 16 + lane;
+        const bool valid = r < count;
+        const size_t src = valid ? (perm ? perm[b0 + r] : b0 + r) : 0;
+        for (int k = 0; k < kMlpIn; ++k) {
+            const float v = valid ? X[src * kMlpIn + k] : 0.f;
+            S.feat[w][lane][k] = v;
+            S.h0[(w * 16 + lane) * kMlpIn + k] = float_to_bf16_bits(v);
+        }
+    }
+    __syncthreads();
+    const int row0 = w * 16;
+    warp_mlp<true>(S.w, S.feat[w], S.y[w], S.z1 + row0 * kMlpHid, S.z2 + row0 * kMlpHid,
+                   S.z3 + row0 * kMlpHid, S.h1 + row0 * kMlpHid, S.h2 + row0 * kMlpHid,
+                   S.h3 + row0 * kMlpHid);
+    __syncwarp();
+    float lsum = 0.f;
+    if (lane < 16) {
+        const size_t r = r_blk + row0 + lane;
+        const bool valid = r < count;
+        const size_t src = valid ? (perm ? perm[b0 + r] : b0 + r) : 0;
+        for (int o = 0; o < kMlpOut; ++o) {
+            float d = 0.f;
+            if (valid && o < kMlpOutUsed) {
+                const float e = S.y[w][lane][o] - T[src * kMlpOutUsed + o];
+                lsum = fmaf(e, e, lsum);
+                d = 2.0f * e * inv_norm;
+            }
+            S.dy[(row0 + lane) * kMlpOut + o] = d;
+        }
+    }
+    lsum = warp_sum(lsum);
+    if (lane == 0 && lsum != 0.f) atomicAdd(loss_sum, lsum);
+    __syncthreads();
+    // layer 4
+    accum_dw(S.h3, kMlpHid, S.dy, kMlpOut, grad + kOffW4, grad + kOffB4);
+    back_act(S.dy, kMlpOut, S.w.wt4, kLdH, S.z3, S.da);
+    __syncthreads();
+    // layer 3
+    accum_dw(S.h2, kMlpHid, S.da, kMlpHid, grad + kOffW3, grad + kOffB3);
+    back_act(S.da, kMlpHid, S.w.wt3, kLdH, S.z2, S.db);
+    __syncthreads();
+    // layer 2
+    accum_dw(S.h1, kMlpHid, S.db, kMlpHid, grad + kOffW2, grad + kOffB2);
+    back_act(S.db, kMlpHid, S.w.wt2, kLdH, S.z1, S.da);
+    __syncthreads();
+    // layer 1
+    accum_dw(S.h0, kMlpIn, S.da, kMlpHid, grad + kOffW1, grad + kOffB1);
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master parameters
+__global__ void k_mlp_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                           const float* __restrict__ g, int n, float lr, float beta1, float beta2,
+                           float eps, float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = fmaf(beta1, m[i], (1.0f - beta1) * gi);
+    const float vi = fmaf(beta2, v[i], (1.0f - beta2) * gi * gi);
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+// ---- launchers ------------------------------------------------------------------
+void launch_closure_mlp(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm, size_t n,
+                        const MlpPacked* w, float4* dF, int sms, cudaStream_t st) {
+    const size_t tiles = (n + 15) / 16;
+    size_t grid = (tiles + 3) / 4;
+    const size_t cap = (size_t)sms * 8;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    k_closure_mlp<<<(unsigned)grid, 128, 0, st>>>(tv, leaf_of, xyzm, n, w, dF);
+}
+
+void launch_mlp_forward(const float* x, size_t n, const MlpPacked* w, float* y, cudaStream_t st) {
+    size_t grid = ((n + 15) / 16 + 3) / 4;
+    if (grid > 4096) grid = 4096;
+    if (grid < 1) grid = 1;
+    k_mlp_forward<<<(unsigned)grid, 128, 0, st>>>(x, n, w, y);
+}
+
+void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm,
+                             size_t n, const uint32_t* idx, size_t k, float* x_out,
+                             float* scale_out, cudaStream_t st) {
+    if (k == 0) return;
+    k_closure_features<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(tv, leaf_of, xyzm, n, idx, k,
+                                                                    x_out, scale_out);
+}
+
+void launch_judge(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
+                  const float* fx, const float* fy, const float* fz, const float4* dF, int allow,
+                  uint32_t tick, JudgeOut* out, int sms, cudaStream_t st) {
+    k_judge_sample<<<(s + 255) / 256, 256, 0, st>>>(tg, s, n, tick);
+    launch_direct_f64(xyzm, n, tg, (size_t)s, f64, sms, st);
+    k_judge_decide<<<1, 1024, 0, st>>>(tg, s, f64, fx, fy, fz, dF, allow, out);
+}
+
+void launch_closure_apply(float* fx, float* fy, float* fz, const float4* dF, size_t n,
+                          const JudgeOut* j, int sms, cudaStream_t st) {
+    size_t grid = (n + 255) / 256;
+    const size_t cap = (size_t)sms * 8;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    k_closure_apply<<<(unsigned)grid, 256, 0, st>>>(fx, fy, fz, dF, n, j);
+}
+
+void launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st) {
+    k_mlp_pack<<<16, 256, 0, st>>>(params, out);
+}
+
+cudaError_t prepare_mlp_grad_kernel() {
+    return cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TrainSmem));
+}
+
+void launch_mlp_grad(const float* X, const float* T, const uint32_t* perm, size_t b0,
+                     size_t count, const MlpPacked* w, float inv_norm, float* grad,
+                     float* loss_sum, cudaStream_t st) {
+    if (count == 0) return;
+    const unsigned grid = (unsigned)((count + kTrainRows - 1) / kTrainRows);
+    k_mlp_grad<<<grid, 128, sizeof(TrainSmem), st>>>(X, T, perm, b0, count, w, inv_norm, grad,
+                                                     loss_sum);
+}
+
+void launch_mlp_adam(float* p, float* m, float* v, const float* g, int n, float lr, float beta1,
+                     float beta2, float eps, float bc1, float bc2, cudaStream_t st) {
+    k_mlp_adam<<<(n + 255) / 256, 256, 0, st>>>(p, m, v, g, n, lr, beta1, beta2, eps, bc1, bc2);
+}
+
+}  // namespace psg

@@ -5,7 +5,7 @@
 //   F_i = sum_{j != i} m_i m_j d_ij / (|d_ij|^2 + eps2)^{3/2},
 // eps2 = the float literal 0.1F widened to double (accuracy.c:12, :57).
 // Sources are streamed through shared memory in tiles; each thread owns one
-// target and accumulates in FP64.
+// target and accumulates in FP64.  Also the closure's per-tick judge.
 #include "psg_common.cuh"
 #include "psg_kernels.h"
 
@@ -13,10 +13,14 @@ namespace psg {
 
 constexpr int kDirThreads = 128;
 
+// One block: 128 targets against the sources [src0, src1); the partial sums
+// are added into out (zeroed by the launcher) with FP64 atomics, so the
+// sources of a target can be split over many blocks and a sample of a few
+// thousand targets still fills the GPU.
 __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __restrict__ xyzm,
                                                             size_t n,
                                                             const uint32_t* __restrict__ targets,
-                                                            size_t n_targets,
+                                                            size_t n_targets, size_t chunk,
                                                             double* __restrict__ out) {
     __shared__ float4 tile[kDirThreads];
     const size_t k = (size_t)blockIdx.x * kDirThreads + threadIdx.x;
@@ -25,12 +29,14 @@ __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __rest
     const uint32_t ti = active ? ti_raw : 0u;
     const float4 t = active ? xyzm[ti] : make_float4(0.f, 0.f, 0.f, 0.f);
     const double eps2 = (double)0.1f;
+    const size_t src0 = (size_t)blockIdx.y * chunk;
+    const size_t src1 = src0 + chunk < n ? src0 + chunk : n;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    for (size_t j0 = 0; j0 < n; j0 += kDirThreads) {
+    for (size_t j0 = src0; j0 < src1; j0 += kDirThreads) {
         const size_t j = j0 + threadIdx.x;
-        tile[threadIdx.x] = j < n ? xyzm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tile[threadIdx.x] = j < src1 ? xyzm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
-        const int cnt = (int)((n - j0) < (size_t)kDirThreads ? (n - j0) : kDirThreads);
+        const int cnt = (int)((src1 - j0) < (size_t)kDirThreads ? (src1 - j0) : kDirThreads);
         for (int q = 0; q < cnt; ++q) {
             const float4 s = tile[q];
             const double dx = (double)s.x - (double)t.x;
@@ -45,22 +51,35 @@ __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __rest
         }
         __syncthreads();
     }
-    if (k < n_targets && !active) {
-        out[3 * k + 0] = out[3 * k + 1] = out[3 * k + 2] = __longlong_as_double(0x7FF8000000000000ll);
+    if (k < n_targets && !active && blockIdx.y == 0) {
+        const double nan = __longlong_as_double(0x7FF8000000000000ll);
+        atomicAdd(&out[3 * k + 0], nan);
+        atomicAdd(&out[3 * k + 1], nan);
+        atomicAdd(&out[3 * k + 2], nan);
     }
     if (active) {
         const double m = (double)t.w;
-        out[3 * k + 0] = m * ax;
-        out[3 * k + 1] = m * ay;
-        out[3 * k + 2] = m * az;
+        atomicAdd(&out[3 * k + 0], m * ax);
+        atomicAdd(&out[3 * k + 1], m * ay);
+        atomicAdd(&out[3 * k + 2], m * az);
     }
 }
 
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
-                       double* out, cudaStream_t st) {
+                       double* out, int sms, cudaStream_t st) {
     if (n_targets == 0) return;
-    const int grid = (int)((n_targets + kDirThreads - 1) / kDirThreads);
-    k_direct_f64<<<grid, kDirThreads, 0, st>>>(xyzm, n, targets, n_targets, out);
+    cudaMemsetAsync(out, 0, n_targets * 3 * sizeof(double), st);
+    const size_t tblocks = (n_targets + kDirThreads - 1) / kDirThreads;
+    // ~8 blocks per SM in total, each source chunk at least 1024 particles
+    size_t splits = ((size_t)sms * 8 + tblocks - 1) / tblocks;
+    const size_t max_splits = (n + 1023) / 1024;
+    if (splits > max_splits) splits = max_splits;
+    if (splits < 1) splits = 1;
+    size_t chunk = (n + splits - 1) / splits;
+    chunk = (chunk + kDirThreads - 1) / kDirThreads * kDirThreads;
+    splits = (n + chunk - 1) / chunk;
+    dim3 grid((unsigned)tblocks, (unsigned)splits);
+    k_direct_f64<<<grid, kDirThreads, 0, st>>>(xyzm, n, targets, n_targets, chunk, out);
 }
 
 }  // namespace psg

@@ -58,6 +58,9 @@ constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-en
 constexpr int kP2PCap = 128;              // staged P2P sources of a group
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
+constexpr uint32_t kDenseLeaf = 8;        // leaves this full go to k_dense_p2p
+constexpr uint32_t kDenseChunk = 32;      // target particles per dense work record
+constexpr uint32_t kDenseSwitch = 32;     // fullest leaf from which the DENSE leaf pass runs
 
 enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
@@ -73,6 +76,8 @@ struct SmemInternal {
 struct SmemLeaf {
     float4 cgeo[8];
     float4 sL[8];           // the children's local fields
+    float4 sG0[8];          // closure order 1: the children's field gradients
+    float2 sG1[8];
     uint2 cpart[8];         // the children's particle ranges
     uint2 p2p_range[kP2PCap];
     uint32_t cand_node[kCandBuf];
@@ -104,6 +109,33 @@ __device__ __forceinline__ void m2l_field(float dx, float dy, float dz, float d2
     fx = fmaf(dx, a, mp.y * ir3);
     fy = fmaf(dy, a, mp.z * ir3);
     fz = fmaf(dz, a, mp.w * ir3);
+}
+
+// m2l_field plus what the closure's order-1 local expansion needs: the
+// gradient of the monopole field at the target centre is
+// g3 * d d^T - gi * I with g3 = 3 m0 / r^5, gi = m0 / r^3 (softened r).
+__device__ __forceinline__ void m2l_field_grad(float dx, float dy, float dz, float d2, float4 mp,
+                                               float& fx, float& fy, float& fz, float& g3,
+                                               float& gi) {
+    const float soft = d2 + 0.1f;
+    const float inv = rsqrtf(soft);
+    const float inv2 = inv * inv;
+    const float ir3 = inv2 * inv;
+    const float ir5 = ir3 * inv2;
+    const float mdr = fmaf(mp.y, dx, fmaf(mp.z, dy, mp.w * dz));
+    const float a = fmaf(mp.x, ir3, -3.0f * mdr * ir5);
+    fx = fmaf(dx, a, mp.y * ir3);
+    fy = fmaf(dy, a, mp.z * ir3);
+    fz = fmaf(dz, a, mp.w * ir3);
+    g3 = 3.0f * mp.x * ir5;
+    gi = mp.x * ir3;
+}
+
+// G v for the symmetric gradient stored as (xx, yy, zz, xy) + (xz, yz)
+__device__ __forceinline__ float3 grad_apply(float4 g0, float2 g1, float vx, float vy, float vz) {
+    return make_float3(fmaf(g0.x, vx, fmaf(g0.w, vy, g1.x * vz)),
+                       fmaf(g0.w, vx, fmaf(g0.y, vy, g1.y * vz)),
+                       fmaf(g1.x, vx, fmaf(g1.y, vy, g0.z * vz)));
 }
 
 // Spill the group's staged P2P sources [0, fill) to HBM chunks of
@@ -179,7 +211,138 @@ __device__ __forceinline__ void p2p_range(const float4* __restrict__ xyzm, uint2
     }
 }
 
-template <int MODE, bool DEBUG>
+// one k_dense_p2p work record per 32 target particles of each full leaf
+// child (bits of dense_mask) of the group whose children start at node fc;
+// phead is the group's complete P2P source chain
+__device__ __noinline__ void record_dense(const SmemLeaf& sm, uint32_t dense_mask, uint32_t fc,
+                                          uint32_t phead, uint4* rec, uint32_t cap,
+                                          Status* status) {
+    const uint32_t lane = lane_id();
+    for (uint32_t m = dense_mask; m; m &= m - 1) {
+        const uint32_t q = __ffs(m) - 1;
+        const uint2 up = sm.cpart[q];
+        const uint32_t nrec = (up.y + kDenseChunk - 1) / kDenseChunk;
+        uint32_t r0 = 0;
+        if (lane == 0) r0 = atomicAdd(&status->dense_count, nrec);
+        r0 = __shfl_sync(0xFFFFFFFFu, r0, 0);
+        for (uint32_t k = lane; k < nrec; k += 32) {
+            if (r0 + k < cap) {
+                const uint32_t c0 = k * kDenseChunk;
+                rec[r0 + k] = make_uint4((fc + q) | (q << 28), phead, up.x + c0,
+                                         min(kDenseChunk, up.y - c0));
+            }
+        }
+        if (lane == 0 && r0 + nrec > cap) set_err(status, PSG_ERR_DENSE_OVERFLOW);
+    }
+}
+
+// L2P + P2P of a group's leaf children once its candidates are done: with
+// DENSE, full leaves are handed to k_dense_p2p; the others get
+// F = m (L + P2P sum) here, one target particle at a time with the lanes over
+// its sources.
+struct LeafOut {
+    const float4* xyzm;
+    const uint4* info;
+    P2PStore p2p;
+    float* fx;
+    float* fy;
+    float* fz;
+    uint32_t* leaf_of;
+    uint32_t* dbg_p2p;
+    uint4* dense_rec;
+    uint32_t dense_cap;
+    int kahan;
+};
+
+template <bool DEBUG, bool GRAD, bool DENSE>
+__device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uint32_t tgt_mask,
+                                           uint32_t fc, uint32_t pfill, uint32_t phead,
+                                           Status* status) {
+    const uint32_t lane = lane_id();
+    // ---- full leaves (depth-10 cells with many particles) go to
+    // k_dense_p2p: the group's whole source list to HBM chunks,
+    // then one work record per 32 target particles ----
+    uint32_t dense = 0;
+    if (DENSE && lane < 8 && ((tgt_mask >> lane) & 1u)) dense = sm.cpart[lane].y >= kDenseLeaf;
+    const uint32_t dense_mask = __ballot_sync(0xFFFFFFFFu, dense != 0) & 0xFFu;
+    if (DENSE && dense_mask) {
+        if (pfill) {
+            phead = spill_p2p(sm, pfill, phead, o.p2p, status);
+            pfill = 0;
+        }
+        record_dense(sm, dense_mask, fc, phead, o.dense_rec, o.dense_cap, status);
+    }
+    // ---- L2P + P2P: F = m * (L(u) + sum of u's P2P sources) ----
+    for (uint32_t e = lane; e < pfill; e += 32) {
+        const uint4 si = o.info[sm.p2p_node[e]];
+        sm.p2p_range[e] = make_uint2(si.x, si.y);
+    }
+    __syncwarp();
+    unsigned long long inter = 0;
+#pragma unroll 1
+    for (uint32_t m = tgt_mask; m; m &= m - 1) {
+        const uint32_t q = __ffs(m) - 1;
+        const uint2 up = sm.cpart[q];
+        const float4 L = sm.sL[q];
+        for (uint32_t ti = 0; (!DENSE || up.y < kDenseLeaf) && ti < up.y; ++ti) {
+            const float4 t = o.xyzm[up.x + ti];
+            float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+            for (uint32_t e = lane; e < pfill; e += 32) {
+                if ((sm.p2p_mask[e] >> q) & 1u) {
+                    const uint2 r = sm.p2p_range[e];
+                    p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
+                    if (DEBUG) inter += r.y;
+                }
+            }
+            for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
+                if (lane < o.p2p.cnt[c] &&
+                    ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
+                    const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
+                    p2p_range(o.xyzm, make_uint2(si.x, si.y), t, o.kahan, bx, by, bz,
+                              cx, cy, cz);
+                    if (DEBUG) inter += si.y;
+                }
+            }
+            const float sx = warp_sum(bx - cx);
+            const float sy = warp_sum(by - cy);
+            const float sz = warp_sum(bz - cz);
+            if (lane == 0) {
+                // final per-particle accumulation in FP64
+                const size_t gi = (size_t)up.x + ti;
+                const double mm = (double)t.w;
+                float lx = L.y, ly = L.z, lz = L.w;
+                if constexpr (GRAD) {
+                    // order-1 L2P: the field at the particle
+                    const float4 cu = sm.cgeo[q];
+                    const float3 sh = grad_apply(sm.sG0[q], sm.sG1[q], t.x - cu.x,
+                                                 t.y - cu.y, t.z - cu.z);
+                    lx += sh.x;
+                    ly += sh.y;
+                    lz += sh.z;
+                    if (o.leaf_of) o.leaf_of[gi] = fc + q;
+                }
+                o.fx[gi] = (float)(mm * ((double)lx + (double)sx));
+                o.fy[gi] = (float)(mm * ((double)ly + (double)sy));
+                o.fz[gi] = (float)(mm * ((double)lz + (double)sz));
+            }
+        }
+        if (DEBUG && lane == 0) {
+            o.dbg_p2p[fc + q] = sm.dbg_p2p[q];
+            atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS],
+                      (unsigned long long)sm.dbg_p2p[q]);
+        }
+    }
+    if (DEBUG) {
+        inter = warp_sum(inter);
+        if (lane == 0) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+    }
+    __syncwarp();
+}
+
+// DENSE (leaf pass only): the variant for trees whose fullest leaf holds at
+// least kDenseSwitch particles, which hands full leaves to k_dense_p2p.  Both
+// variants are launched; each returns at once unless the tree is its kind.
+template <int MODE, bool DEBUG, bool GRAD, bool DENSE>
 __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
     using Smem = typename SmemOf<MODE>::T;
     __shared__ Smem smem[kTravWarps];
@@ -189,6 +352,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
     const TreeView& tv = A.tv;
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
+    if (MODE == MODE_LEAF && ((status->max_leaf >= kDenseSwitch) != DENSE)) return;
     const float theta2 = __fmul_rn(A.theta, A.theta);
 
     // group index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
@@ -318,6 +482,13 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             float acc[8][3];
 #pragma unroll
             for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.f;
+            float gacc[GRAD ? 8 : 1][6];
+            if constexpr (GRAD) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) gacc[q][k] = 0.f;
+            }
             uint32_t ssize = 0, e0 = 0;
             uint32_t pfill = 0, phead = kNone;  // MODE_LEAF: staged / spilled P2P sources
             bool root_pending = root_only;
@@ -417,7 +588,20 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                                                        sg.w, theta2, dx, dy, dz, d2) && act;
                         // branch-free: every lane evaluates, only separated pairs add
                         float fx, fy, fz;
-                        m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
+                        if constexpr (GRAD) {
+                            float g3, gi;
+                            m2l_field_grad(dx, dy, dz, d2, smp, fx, fy, fz, g3, gi);
+                            g3 = sep ? g3 : 0.f;
+                            gi = sep ? gi : 0.f;
+                            gacc[q][0] += fmaf(g3 * dx, dx, -gi);
+                            gacc[q][1] += fmaf(g3 * dy, dy, -gi);
+                            gacc[q][2] += fmaf(g3 * dz, dz, -gi);
+                            gacc[q][3] += g3 * dx * dy;
+                            gacc[q][4] += g3 * dx * dz;
+                            gacc[q][5] += g3 * dy * dz;
+                        } else {
+                            m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
+                        }
                         acc[q][0] += sep ? fx : 0.f;
                         acc[q][1] += sep ? fy : 0.f;
                         acc[q][2] += sep ? fz : 0.f;
@@ -493,19 +677,53 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             }
 
             // ---- L2L: L(u) = M2L(u) + L(parent)  (polesitter.h:1248-1250) ----
+            // closure order 1 shifts the parent's field to the child's centre:
+            // L(u) = M2L(u) + L(p) + G(p) (c_u - c_p), G(u) = M2L_G(u) + G(p)
+            float4 Gp0 = make_float4(0.f, 0.f, 0.f, 0.f), cp = Gp0;
+            float2 Gp1 = make_float2(0.f, 0.f);
+            if constexpr (GRAD) {
+                cp = tv.geo[pid];
+                if (dp >= 2) {
+                    Gp0 = tv.lg0[pid];
+                    Gp1 = tv.lg1[pid];
+                }
+            }
 #pragma unroll
             for (uint32_t q = 0; q < 8; ++q) {
                 if (!((tgt_mask >> q) & 1u)) continue;
                 const float ax = warp_sum(acc[q][0]);
                 const float ay = warp_sum(acc[q][1]);
                 const float az = warp_sum(acc[q][2]);
-                const float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
-                                             __fadd_rn(az, Lp.w));
+                float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
+                                       __fadd_rn(az, Lp.w));
+                float4 G0 = Gp0;
+                float2 G1 = Gp1;
+                if constexpr (GRAD) {
+                    const float4 cu = sm.cgeo[q];
+                    const float3 sh = grad_apply(Gp0, Gp1, cu.x - cp.x, cu.y - cp.y, cu.z - cp.z);
+                    L.y += sh.x;
+                    L.z += sh.y;
+                    L.w += sh.z;
+                    G0.x += warp_sum(gacc[q][0]);
+                    G0.y += warp_sum(gacc[q][1]);
+                    G0.z += warp_sum(gacc[q][2]);
+                    G0.w += warp_sum(gacc[q][3]);
+                    G1.x += warp_sum(gacc[q][4]);
+                    G1.y += warp_sum(gacc[q][5]);
+                }
                 if (lane == 0) {
                     const uint32_t u = fc + q;
                     tv.lt[u] = L;
+                    if constexpr (GRAD) {
+                        tv.lg0[u] = G0;
+                        tv.lg1[u] = G1;
+                    }
                     if constexpr (MODE == MODE_LEAF) {
                         sm.sL[q] = L;
+                        if constexpr (GRAD) {
+                            sm.sG0[q] = G0;
+                            sm.sG1[q] = G1;
+                        }
                     } else {
                         const uint32_t sub = __popc(tgt_mask & ((1u << q) - 1u));
                         tv.ns_off[u] = (uint32_t)(ns_base + (unsigned long long)sub * cand_total);
@@ -520,79 +738,119 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             __syncwarp();
 
             if constexpr (MODE == MODE_LEAF) {
-                // ---- L2P + P2P: F = m * (L(u) + sum of u's P2P sources) ----
-                for (uint32_t e = lane; e < pfill; e += 32) {
-                    const uint4 si = tv.info[sm.p2p_node[e]];
-                    sm.p2p_range[e] = make_uint2(si.x, si.y);
-                }
-                __syncwarp();
-                unsigned long long inter = 0;
-#pragma unroll 1
-                for (uint32_t m = tgt_mask; m; m &= m - 1) {
-                    const uint32_t q = __ffs(m) - 1;
-                    const uint2 up = sm.cpart[q];
-                    const float4 L = sm.sL[q];
-                    for (uint32_t ti = 0; ti < up.y; ++ti) {
-                        const float4 t = A.xyzm[up.x + ti];
-                        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-                        for (uint32_t e = lane; e < pfill; e += 32) {
-                            if ((sm.p2p_mask[e] >> q) & 1u) {
-                                const uint2 r = sm.p2p_range[e];
-                                p2p_range(A.xyzm, r, t, A.kahan, bx, by, bz, cx, cy, cz);
-                                if (DEBUG) inter += r.y;
-                            }
-                        }
-                        for (uint32_t c = phead; c != kNone; c = A.p2p.next[c]) {
-                            if (lane < A.p2p.cnt[c] &&
-                                ((A.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
-                                const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
-                                p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz,
-                                          cx, cy, cz);
-                                if (DEBUG) inter += si.y;
-                            }
-                        }
-                        const float sx = warp_sum(bx - cx);
-                        const float sy = warp_sum(by - cy);
-                        const float sz = warp_sum(bz - cz);
-                        if (lane == 0) {
-                            // final per-particle accumulation in FP64
-                            const size_t gi = (size_t)up.x + ti;
-                            const double mm = (double)t.w;
-                            A.fx[gi] = (float)(mm * ((double)L.y + (double)sx));
-                            A.fy[gi] = (float)(mm * ((double)L.z + (double)sy));
-                            A.fz[gi] = (float)(mm * ((double)L.w + (double)sz));
-                        }
-                    }
-                    if (DEBUG && lane == 0) {
-                        tv.dbg_p2p[fc + q] = sm.dbg_p2p[q];
-                        atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS],
-                                  (unsigned long long)sm.dbg_p2p[q]);
-                    }
-                }
-                if (DEBUG) {
-                    inter = warp_sum(inter);
-                    if (lane == 0) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
-                }
-                __syncwarp();
+                leaf_epilogue<DEBUG, GRAD, DENSE>(
+                    sm,
+                    LeafOut{A.xyzm, tv.info, A.p2p, A.fx, A.fy, A.fz, A.leaf_of, tv.dbg_p2p,
+                            A.dense_rec, A.dense_cap, A.kahan},
+                    tgt_mask, fc, pfill, phead, status);
             }
         }
+    }
+}
+
+// L2P + P2P of the full leaves recorded by the leaf pass.  A warp takes one
+// record (a leaf, up to 32 of its particles, its source chain) at a time
+// from a shared counter; the lanes own the target particles and walk the
+// leaf's P2P sources together, so each source particle is one broadcast
+// load for the warp.  The sources are summed in chain order, so the result
+// does not depend on scheduling.
+template <bool DEBUG, bool GRAD>
+__global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
+    Status* status = A.status;
+    if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_DENSE_OVERFLOW)) return;
+    const TreeView& tv = A.tv;
+    const uint32_t lane = lane_id();
+    const uint32_t total = min(status->dense_count, A.dense_cap);
+    if (total == 0) return;
+    unsigned long long inter = 0;
+    for (;;) {
+        uint32_t r = 0;
+        if (lane == 0) r = atomicAdd(&status->dense_work, 1u);
+        r = __shfl_sync(0xFFFFFFFFu, r, 0);
+        if (r >= total) break;
+        const uint4 rec = A.dense_rec[r];
+        const uint32_t u = rec.x & kLinkMask, q = rec.x >> 28;
+        const bool active = lane < rec.w;
+        const uint32_t i = rec.z + (active ? lane : 0u);
+        const float4 t = A.xyzm[i];
+        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+        for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
+            const uint32_t cnt = A.p2p.cnt[c];
+            for (uint32_t k = 0; k < cnt; ++k) {
+                if (!((A.p2p.mask[(size_t)c * kP2PChunk + k] >> q) & 1u)) continue;
+                const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + k]];
+                p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz, cx, cy, cz);
+                if (DEBUG) inter += active ? si.y : 0u;
+            }
+        }
+        if (active) {
+            const float4 L = tv.lt[u];
+            float lx = L.y, ly = L.z, lz = L.w;
+            if constexpr (GRAD) {
+                const float4 cu = tv.geo[u];
+                const float3 sh = grad_apply(tv.lg0[u], tv.lg1[u], t.x - cu.x, t.y - cu.y,
+                                             t.z - cu.z);
+                lx += sh.x;
+                ly += sh.y;
+                lz += sh.z;
+                if (A.leaf_of) A.leaf_of[i] = u;
+            }
+            const double mm = (double)t.w;
+            A.fx[i] = (float)(mm * ((double)lx + (double)(bx - cx)));
+            A.fy[i] = (float)(mm * ((double)ly + (double)(by - cy)));
+            A.fz[i] = (float)(mm * ((double)lz + (double)(bz - cz)));
+        }
+    }
+    if (DEBUG) {
+        inter = warp_sum(inter);
+        if (lane == 0 && inter) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+    }
+}
+
+void launch_dense_p2p(const TravArgs& A, int grid, cudaStream_t st) {
+    if (A.order >= 1) {
+        if (A.debug) k_dense_p2p<true, true><<<grid, kTravThreads, 0, st>>>(A);
+        else k_dense_p2p<false, true><<<grid, kTravThreads, 0, st>>>(A);
+    } else {
+        if (A.debug) k_dense_p2p<true, false><<<grid, kTravThreads, 0, st>>>(A);
+        else k_dense_p2p<false, false><<<grid, kTravThreads, 0, st>>>(A);
+    }
+}
+
+template <int MODE, bool DENSE>
+static void launch_mode(const TravArgs& A, int grid, cudaStream_t st) {
+    if (A.order >= 1) {
+        if (A.debug) k_trav<MODE, true, true, DENSE><<<grid, kTravThreads, 0, st>>>(A);
+        else k_trav<MODE, false, true, DENSE><<<grid, kTravThreads, 0, st>>>(A);
+    } else {
+        if (A.debug) k_trav<MODE, true, false, DENSE><<<grid, kTravThreads, 0, st>>>(A);
+        else k_trav<MODE, false, false, DENSE><<<grid, kTravThreads, 0, st>>>(A);
     }
 }
 
 void launch_traverse_internal(const TravArgs& args, int level, int grid, cudaStream_t st) {
     TravArgs A = args;
     A.level = level;
-    if (A.debug) k_trav<MODE_INTERNAL, true><<<grid, kTravThreads, 0, st>>>(A);
-    else k_trav<MODE_INTERNAL, false><<<grid, kTravThreads, 0, st>>>(A);
+    launch_mode<MODE_INTERNAL, false>(A, grid, st);
 }
 
-void launch_traverse_leaves(const TravArgs& args, int grid, cudaStream_t st) {
-    if (args.debug) k_trav<MODE_LEAF, true><<<grid, kTravThreads, 0, st>>>(args);
-    else k_trav<MODE_LEAF, false><<<grid, kTravThreads, 0, st>>>(args);
+void launch_traverse_leaves(const TravArgs& args, const int grid[2], cudaStream_t st) {
+    launch_mode<MODE_LEAF, false>(args, grid[0], st);
+    launch_mode<MODE_LEAF, true>(args, grid[1], st);
 }
 
 int traverse_threads() { return kTravThreads; }
-const void* traverse_kernel_ptr() { return (const void*)k_trav<MODE_LEAF, false>; }
-const void* traverse_internal_kernel_ptr() { return (const void*)k_trav<MODE_INTERNAL, false>; }
+const void* traverse_kernel_ptr(int order, int dense) {
+    if (order) {
+        return dense ? (const void*)k_trav<MODE_LEAF, false, true, true>
+                     : (const void*)k_trav<MODE_LEAF, false, true, false>;
+    }
+    return dense ? (const void*)k_trav<MODE_LEAF, false, false, true>
+                 : (const void*)k_trav<MODE_LEAF, false, false, false>;
+}
+const void* traverse_internal_kernel_ptr(int order) {
+    return order ? (const void*)k_trav<MODE_INTERNAL, false, true, false>
+                 : (const void*)k_trav<MODE_INTERNAL, false, false, false>;
+}
 
 }  // namespace psg

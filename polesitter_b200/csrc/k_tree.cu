@@ -257,10 +257,12 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
     }
 }
 
-// child count = next node's first-child rank - this node's (same level)
+// child count = next node's first-child rank - this node's (same level);
+// also the particle count of the fullest leaf
 __global__ void __launch_bounds__(256) k_tree_link(TreeView tv, const Status* status) {
     const uint32_t total = tv.lvl_base[kLevels];
     const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t max_leaf = 0;
     for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
         int d = 0;
         while (d < kMaxDepth && id >= tv.lvl_base[d + 1]) ++d;
@@ -282,7 +284,10 @@ __global__ void __launch_bounds__(256) k_tree_link(TreeView tv, const Status* st
         tv.info[id] = inf;
         tv.link[id] = nch ? ((inf.z & kLinkMask) | (nch << 28)) : 0u;
         tv.lt[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (nch == 0 && inf.y > max_leaf) max_leaf = inf.y;
     }
+    max_leaf = __reduce_max_sync(0xFFFFFFFFu, max_leaf);
+    if (lane_id() == 0 && max_leaf) atomicMax(&const_cast<Status*>(status)->max_leaf, max_leaf);
 }
 
 // Upward pass, one launch per level from the deepest up: a leaf sums P2M

@@ -54,6 +54,8 @@ struct TreeView {
     uint32_t* ns_cnt;      // per node: length of its near-source list
     uint32_t* dbg_m2l;     // per node M2L pair count (debug builds of a tick)
     uint32_t* dbg_p2p;     // per node P2P leaf-pair count (debug)
+    float4* lg0;           // closure order 1: field gradient xx, yy, zz, xy
+    float2* lg1;           //                  and xz, yz (null when unused)
     uint32_t lvl_base[kLevels + 1];
     uint32_t lvl_cap[kLevels + 1];
 };
@@ -70,6 +72,9 @@ struct Status {
     uint32_t max_stack;                    // deepest DFS stack seen (debug)
     uint32_t p2p_chunks;                   // P2P chunks used this tick
     uint32_t sort_tiles[4];                // onesweep tile tickets
+    uint32_t dense_count;                  // full-leaf P2P records written
+    uint32_t dense_work;                   // ... and taken by k_dense_p2p
+    uint32_t max_leaf;                     // particles in the fullest leaf
 };
 
 // P2P sources spilled from the traversal: chunk c holds cnt[c] source-leaf

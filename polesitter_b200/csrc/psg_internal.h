@@ -27,6 +27,7 @@ extern "C" {
 #define PSG_ERR_STACK 0x4u        /* traversal stack bound violated */
 #define PSG_ERR_NODES 0x8u        /* tree level over its capacity */
 #define PSG_ERR_P2P_OVERFLOW 0x10u /* P2P chunk store too small: regrow, rerun */
+#define PSG_ERR_DENSE_OVERFLOW 0x20u /* full-leaf record list too small: regrow, rerun */
 
 /* debug statistics slots (Status.stat) */
 #define PSG_STAT_MAC 0
@@ -104,6 +105,23 @@ int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n
 #define PSG_OPT_TIMING 4         /* 1: time phases with CUDA events */
 #define PSG_OPT_USE_GRAPH 5      /* 1: replay calc_forces as a CUDA graph */
 #define PSG_OPT_KAHAN 6          /* 1: compensated FP32 sums in P2P */
+#define PSG_OPT_CLOSURE 7        /* 0 reference, 1 order-1 local, 2 + learned correction */
+#define PSG_OPT_JUDGE 8          /* 1: sampled FP64 judge in closure mode 1 too */
+
+/* the learned far-field closure (k_closure.cu) */
+#define PSG_CLOSURE_PARAMS 9928
+int psg_closure_set_weights(void* state, const float* params, size_t n_params);
+int psg_closure_last(void* state, double* median_base, double* median_mlp, int* used,
+                     int* samples);
+int psg_closure_features(void* state, const uint32_t* idx, size_t k, float* x_out,
+                         float* scale_out);
+int psg_closure_train(void* state, const float* x, const float* t, size_t n, float* params,
+                      uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* loss_out);
+int psg_closure_grad(void* state, const float* x, const float* t, size_t n, const float* params,
+                     float* grad_out, float* loss_out);
+int psg_closure_forward(void* state, const float* x, size_t n, const float* params,
+                        float* y_out);
+int psg_closure_correction(void* state, float* out, size_t n);
 
 #ifdef __cplusplus
 }

@@ -47,10 +47,11 @@ void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int gr
 // (polesitter.h:1050-1146, :1224-1254, :1258-1494)
 struct TravArgs;
 int traverse_threads();
-const void* traverse_kernel_ptr();
-const void* traverse_internal_kernel_ptr();
+const void* traverse_kernel_ptr(int order, int dense);
+const void* traverse_internal_kernel_ptr(int order);
 void launch_traverse_internal(const TravArgs& A, int level, int grid, cudaStream_t st);
-void launch_traverse_leaves(const TravArgs& A, int grid, cudaStream_t st);
+void launch_traverse_leaves(const TravArgs& A, const int grid[2], cudaStream_t st);
+void launch_dense_p2p(const TravArgs& A, int grid, cudaStream_t st);
 
 
 // k_tick.cu -- the caller's tick loop on the device (README.md:65-111)
@@ -73,9 +74,32 @@ struct TickState {
 void launch_tick_reset_ids(uint32_t* id, size_t n, int grid, cudaStream_t st);
 void launch_tick_euler(const TickState& t, size_t n, float dt, int grid, cudaStream_t st);
 
+// k_closure.cu -- the learned far-field closure (no counterpart in the reference)
+struct MlpPacked;
+struct JudgeOut;
+void launch_closure_mlp(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm, size_t n,
+                        const MlpPacked* w, float4* dF, int sms, cudaStream_t st);
+void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm,
+                             size_t n, const uint32_t* idx, size_t k, float* x_out,
+                             float* scale_out, cudaStream_t st);
+void launch_judge(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
+                  const float* fx, const float* fy, const float* fz, const float4* dF, int allow,
+                  uint32_t tick, JudgeOut* out, int sms, cudaStream_t st);
+void launch_closure_apply(float* fx, float* fy, float* fz, const float4* dF, size_t n,
+                          const JudgeOut* j, int sms, cudaStream_t st);
+void launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st);
+void launch_mlp_forward(const float* x, size_t n, const MlpPacked* w, float* y, cudaStream_t st);
+cudaError_t prepare_mlp_grad_kernel();
+size_t mlp_train_smem_bytes();
+void launch_mlp_grad(const float* X, const float* T, const uint32_t* perm, size_t b0,
+                     size_t count, const MlpPacked* w, float inv_norm, float* grad,
+                     float* loss_sum, cudaStream_t st);
+void launch_mlp_adam(float* p, float* m, float* v, const float* g, int n, float lr, float beta1,
+                     float beta2, float eps, float bc1, float bc2, cudaStream_t st);
+
 // k_direct.cu -- FP64 direct-sum forces for sampled targets (tests/accuracy.c:42-72)
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
-                       double* out /*[n_targets][3]*/, cudaStream_t st);
+                       double* out /*[n_targets][3]*/, int sms, cudaStream_t st);
 
 }  // namespace psg
 
@@ -96,5 +120,9 @@ struct TravArgs {
     int level;
     int debug;
     int kahan;          // compensated FP32 sums in P2P
+    int order;          // closure: 0 = the reference's order-0 local, 1 = order-1
+    uint32_t* leaf_of;  // closure: leaf node of each sorted particle (order 1)
+    uint4* dense_rec;   // full-leaf P2P work records: leaf | q << 28, chain, first, count
+    uint32_t dense_cap;
 };
 }  // namespace psg

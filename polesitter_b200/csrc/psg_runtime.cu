@@ -12,6 +12,7 @@
 #include <mutex>
 #include <new>
 
+#include "psg_closure.cuh"
 #include "psg_common.cuh"
 #include "psg_kernels.h"
 
@@ -43,7 +44,7 @@ static void note(const char* what, cudaError_t e) {
 
 constexpr uint32_t kMagic = 0x50534732u;  // "PSG2"
 constexpr int kPhases = 8;  // timing events
-enum Phase { PH_SORT = 0, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END, PH_BEGIN };
+enum Phase { PH_SORT = 0, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END, PH_BEGIN, PH_CLOSURE };
 
 struct Mirror {
     float *x, *y, *z, *m, *fx, *fy, *fz;
@@ -51,12 +52,32 @@ struct Mirror {
     size_t cap;
 };
 
+// the learned closure's device buffers (allocated when it is first enabled)
+struct ClosureState {
+    int mode;            // 0 off (the reference), 1 order-1 local, 2 order-1 + MLP
+    int judge;           // run the sampled FP64 judge in mode 1 too
+    float4* lg0;         // per node: field gradient xx yy zz xy
+    float2* lg1;         //           xz yz
+    uint32_t* leaf_of;   // per sorted particle: its leaf
+    float4* dF;          // per sorted particle: the MLP's correction
+    float* params;       // FP32 parameter vector (kMlpParams)
+    MlpPacked* packed;   // BF16 device copy
+    int have_weights;
+    uint32_t* judge_tg;  // judge sample (sorted indices)
+    double* judge_f64;   // FP64 direct forces of the sample
+    JudgeOut* d_judge;
+    JudgeOut* h_judge;
+    uint32_t tick;       // ticks run in closure mode (varies the judge sample)
+    JudgeOut last;       // judge result of the last tick (samples 0: none)
+    int valid;           // the last completed tick ran the order-1 traversal
+};
+
 struct State {
     uint32_t magic;
     int device;
     int sms;
-    int trav_grid;
-    int trav_int_grid;
+    int trav_grid[2][2];   // leaf-pass grid [closure order 0 / 1][sparse / dense variant]
+    int trav_int_grid[2];
     size_t max_particles;
     float theta;
     int morton_variant;
@@ -71,6 +92,8 @@ struct State {
     uint32_t* ns;
     unsigned long long ns_cap;
     P2PStore p2p;
+    uint4* dense_rec;      // full-leaf P2P work records
+    uint32_t dense_cap;
     int kahan;
     Status* d_status;
     Status* h_status;
@@ -86,6 +109,10 @@ struct State {
     float* tk_bbox;
     float* tk_v[3];
     float* tk_vmir[3];
+    ClosureState cl;
+    int order;  // traversal's local expansion order: 0 (reference) or 1
+    size_t last_n;  // particles of the last completed tick
+    int attempts;   // traversal runs of the last tick (> 1: a capacity regrow)
 };
 
 static int grid_for(const State* s, size_t n, int per_block_items) {
@@ -114,6 +141,14 @@ static int alloc_p2p(State* s, uint32_t chunks) {
     PSG_ALLOC(s->p2p.next, (size_t)chunks * 4);
     PSG_ALLOC(s->p2p.cnt, (size_t)chunks * 4);
     s->p2p.cap_chunks = chunks;
+    return PSG_OK;
+}
+
+static int alloc_dense(State* s, uint32_t cap) {
+    if (s->dense_rec) cudaFree(s->dense_rec);
+    s->dense_rec = nullptr;
+    PSG_ALLOC(s->dense_rec, (size_t)cap * sizeof(uint4));
+    s->dense_cap = cap;
     return PSG_OK;
 }
 
@@ -159,11 +194,14 @@ static void free_state(State* s) {
                   s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
                   s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->tv.link,
                   s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.mask, s->p2p.next, s->p2p.cnt,
-                  s->d_status, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
-                  s->tk_vmir[0], s->tk_vmir[1], s->tk_vmir[2]};
+                  s->d_status, s->dense_rec, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
+                  s->tk_vmir[0], s->tk_vmir[1], s->tk_vmir[2], s->cl.lg0, s->cl.lg1,
+                  s->cl.leaf_of, s->cl.dF, s->cl.params, s->cl.packed, s->cl.judge_tg,
+                  s->cl.judge_f64, s->cl.d_judge};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->cl.h_judge) cudaFreeHost(s->cl.h_judge);
     free_mirror(s->mir);
     for (int i = 0; i < kPhases; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
@@ -226,14 +264,40 @@ static int init_state(State* s, size_t maxp, float theta) {
     if (r != PSG_OK) return r;
     r = alloc_p2p(s, (uint32_t)(n < 4096 ? 4096 : n / 4));
     if (r != PSG_OK) return r;
-    int bps = 0;
-    PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, traverse_kernel_ptr(),
-                                                            traverse_threads(), 0));
-    s->trav_grid = s->sms * (bps > 0 ? bps : 1);
-    PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, traverse_internal_kernel_ptr(),
-                                                            traverse_threads(), 0));
-    s->trav_int_grid = s->sms * (bps > 0 ? bps : 1);
+    // a full leaf holds >= 8 particles, so n / 8 records always suffice
+    r = alloc_dense(s, (uint32_t)(n / 8 + 1024));
+    if (r != PSG_OK) return r;
+    for (int o = 0; o < 2; ++o) {
+        int bps = 0;
+        for (int dn = 0; dn < 2; ++dn) {
+            PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &bps, traverse_kernel_ptr(o, dn), traverse_threads(), 0));
+            s->trav_grid[o][dn] = s->sms * (bps > 0 ? bps : 1);
+        }
+        PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &bps, traverse_internal_kernel_ptr(o), traverse_threads(), 0));
+        s->trav_int_grid[o] = s->sms * (bps > 0 ? bps : 1);
+    }
     s->magic = kMagic;
+    return PSG_OK;
+}
+
+static int closure_alloc(State* s) {
+    ClosureState& c = s->cl;
+    if (c.lg0) return PSG_OK;
+    const size_t nodes = s->tv.lvl_base[kLevels];
+    const size_t n = s->max_particles ? s->max_particles : 1;
+    PSG_ALLOC(c.lg0, nodes * sizeof(float4));
+    PSG_ALLOC(c.lg1, nodes * sizeof(float2));
+    PSG_ALLOC(c.leaf_of, n * 4);
+    PSG_ALLOC(c.dF, n * sizeof(float4));
+    PSG_ALLOC(c.params, kMlpParams * sizeof(float));
+    PSG_ALLOC(c.packed, sizeof(MlpPacked));
+    PSG_ALLOC(c.judge_tg, kJudgeSamples * 4);
+    PSG_ALLOC(c.judge_f64, kJudgeSamples * 3 * sizeof(double));
+    PSG_ALLOC(c.d_judge, sizeof(JudgeOut));
+    PSG_CHECK(cudaMallocHost((void**)&c.h_judge, sizeof(JudgeOut)));
+    std::memset(c.h_judge, 0, sizeof(JudgeOut));
     return PSG_OK;
 }
 
@@ -246,10 +310,12 @@ static void record(State* s, int ph) {
 static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, float* fz,
                          uint32_t* err_out) {
     for (int attempt = 0; attempt < 6; ++attempt) {
+        s->attempts = attempt + 1;
         PSG_CHECK(cudaMemsetAsync(&s->d_status->work[0], 0, sizeof(s->d_status->work), s->stream));
         PSG_CHECK(cudaMemsetAsync(&s->d_status->ns_used[0], 0, sizeof(s->d_status->ns_used),
                                   s->stream));
         PSG_CHECK(cudaMemsetAsync(&s->d_status->p2p_chunks, 0, 4, s->stream));
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->dense_count, 0, 8, s->stream));
         TravArgs A;
         A.tv = s->tv;
         A.p2p = s->p2p;
@@ -264,17 +330,25 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
         A.fx = fx;
         A.fy = fy;
         A.fz = fz;
+        const int o = s->order >= 1 ? 1 : 0;
+        A.order = o;
+        A.leaf_of = o ? s->cl.leaf_of : nullptr;
+        A.tv.lg0 = o ? s->cl.lg0 : nullptr;
+        A.tv.lg1 = o ? s->cl.lg1 : nullptr;
+        A.dense_rec = s->dense_rec;
+        A.dense_cap = s->dense_cap;
         for (int k = 2; k <= kMaxDepth; ++k)
-            launch_traverse_internal(A, k, s->trav_int_grid, s->stream);
+            launch_traverse_internal(A, k, s->trav_int_grid[o], s->stream);
         record(s, PH_TRAV);
-        launch_traverse_leaves(A, s->trav_grid, s->stream);
+        launch_traverse_leaves(A, s->trav_grid[o], s->stream);
+        launch_dense_p2p(A, s->sms * 8, s->stream);
         record(s, PH_END);
         PSG_CHECK(cudaGetLastError());
         PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
                                   cudaMemcpyDeviceToHost, s->stream));
         PSG_CHECK(cudaStreamSynchronize(s->stream));
         const uint32_t err = s->h_status->err;
-        if (!(err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW))) {
+        if (!(err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW | PSG_ERR_DENSE_OVERFLOW))) {
             *err_out = err;
             return PSG_OK;
         }
@@ -283,6 +357,13 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
             need = need + need / 4 + 1024;
             if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
             int r = alloc_ns(s, need);
+            if (r != PSG_OK) return r;
+        }
+        if (err & PSG_ERR_DENSE_OVERFLOW) {
+            unsigned long long need = s->h_status->dense_count;
+            need = need + need / 4 + 1024;
+            if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
+            int r = alloc_dense(s, (uint32_t)need);
             if (r != PSG_OK) return r;
         }
         if (err & PSG_ERR_P2P_OVERFLOW) {
@@ -402,22 +483,56 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
         std::snprintf(g_err, sizeof(g_err), "morton codes not sorted/30-bit (0x%x)", err);
         return PSG_EINVAL;
     }
+    s->cl.last.samples = 0;
+    s->cl.valid = s->order >= 1 && n > 1;
+    if (s->order >= 1 && n > 1) {
+        // learned closure: MLP correction, sampled FP64 judge, fallback
+        ClosureState& c = s->cl;
+        const bool mlp = c.mode == 2 && c.have_weights;
+        if (mlp || c.judge) {
+            TreeView tv = s->tv;
+            tv.lg0 = c.lg0;
+            tv.lg1 = c.lg1;
+            if (mlp) {
+                launch_closure_mlp(tv, c.leaf_of, s->xyzm, n, c.packed, c.dF, s->sms, st);
+            } else {
+                PSG_CHECK(cudaMemsetAsync(c.dF, 0, n * sizeof(float4), st));
+            }
+            const int smp = n < (size_t)kJudgeSamples ? (int)n : kJudgeSamples;
+            launch_judge(s->xyzm, n, c.judge_tg, smp, c.judge_f64, d.fx, d.fy, d.fz, c.dF,
+                         mlp ? 1 : 0, c.tick, c.d_judge, s->sms, st);
+            if (mlp) launch_closure_apply(d.fx, d.fy, d.fz, c.dF, n, c.d_judge, s->sms, st);
+            PSG_CHECK(cudaGetLastError());
+            PSG_CHECK(cudaMemcpyAsync(c.h_judge, c.d_judge, sizeof(JudgeOut),
+                                      cudaMemcpyDeviceToHost, st));
+            PSG_CHECK(cudaStreamSynchronize(st));
+            c.last = *c.h_judge;
+            ++c.tick;
+        }
+    }
+    record(s, PH_CLOSURE);
     uint32_t nodes = 0;
     for (int k = 0; k <= kMaxDepth; ++k) {
         s->lvl_count[k] = s->h_status->lvl_count[k];
         nodes += s->lvl_count[k];
     }
     s->last_nodes = nodes;
+    s->last_n = n;
     for (int i = 0; i < 8; ++i) s->stats[i] = s->h_status->stat[i];
     s->stats[8] = nodes;
     s->stats[9] = s->h_status->max_stack;
     for (int i = 8; i < 16; ++i) s->stats[i + 8] = s->h_status->stat[i];
     s->stats[10] = s->h_status->p2p_chunks;
+    s->stats[11] = (unsigned long long)s->attempts;
+    s->stats[12] = s->h_status->max_leaf;
+    s->stats[13] = s->h_status->dense_count;
     if (s->timing) {
+        cudaEventSynchronize(s->ev[PH_CLOSURE]);
         const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END};
         for (int i = 0; i + 1 < 7; ++i)
             cudaEventElapsedTime(&s->ms[i], s->ev[order[i]], s->ev[order[i + 1]]);
-        cudaEventElapsedTime(&s->ms[6], s->ev[PH_BEGIN], s->ev[PH_END]);
+        cudaEventElapsedTime(&s->ms[6], s->ev[PH_BEGIN], s->ev[PH_CLOSURE]);
+        cudaEventElapsedTime(&s->ms[7], s->ev[PH_END], s->ev[PH_CLOSURE]);
     }
     return PSG_OK;
 }
@@ -624,6 +739,19 @@ int psg_set_option(void* mem, int key, double value) {
             return PSG_OK;
         case PSG_OPT_TIMING: s->timing = value != 0.0; return PSG_OK;
         case PSG_OPT_KAHAN: s->kahan = value != 0.0; return PSG_OK;
+        case PSG_OPT_CLOSURE: {
+            const int mode = (int)value;
+            if (mode < 0 || mode > 2 || (double)mode != value) return PSG_EINVAL;
+            if (mode >= 1) {
+                PSG_CHECK(cudaSetDevice(s->device));
+                const int r = psg::closure_alloc(s);
+                if (r != PSG_OK) return r;
+            }
+            s->cl.mode = mode;
+            s->order = mode >= 1 ? 1 : 0;
+            return PSG_OK;
+        }
+        case PSG_OPT_JUDGE: s->cl.judge = value != 0.0; return PSG_OK;
         default: return PSG_EINVAL;
     }
 }
@@ -724,12 +852,230 @@ int psg_direct_f64(void* mem, const psg_arrays_t* a, const uint32_t* targets, si
         PSG_CHECK(cudaMemcpyAsync(dt, targets, n_t * 4, cudaMemcpyHostToDevice, st));
     }
     if (ho) PSG_ALLOC(dout, n_t * 3 * sizeof(double));
-    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, st);
+    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, s->sms, st);
     PSG_CHECK(cudaGetLastError());
     if (ho) PSG_CHECK(cudaMemcpyAsync(out, dout, n_t * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     PSG_CHECK(cudaStreamSynchronize(st));
     if (ht) cudaFree(dt);
     if (ho) cudaFree(dout);
+    return PSG_OK;
+}
+
+// ---- learned closure ----------------------------------------------------------
+
+int psg_closure_set_weights(void* mem, const float* params, size_t n_params) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !params) return PSG_EINVAL;
+    if (n_params != (size_t)psg::kMlpParams) {
+        std::snprintf(psg::g_err, sizeof(psg::g_err), "closure weights: %zu parameters, want %d",
+                      n_params, psg::kMlpParams);
+        return PSG_EINVAL;
+    }
+    PSG_CHECK(cudaSetDevice(s->device));
+    int r = psg::closure_alloc(s);
+    if (r != PSG_OK) return r;
+    PSG_CHECK(cudaMemcpyAsync(s->cl.params, params, n_params * 4, cudaMemcpyHostToDevice,
+                              s->stream));
+    psg::launch_mlp_pack(s->cl.params, s->cl.packed, s->stream);
+    PSG_CHECK(cudaGetLastError());
+    PSG_CHECK(cudaStreamSynchronize(s->stream));
+    s->cl.have_weights = 1;
+    return PSG_OK;
+}
+
+int psg_closure_last(void* mem, double* median_base, double* median_mlp, int* used,
+                     int* samples) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
+    if (median_base) *median_base = s->cl.last.median_base;
+    if (median_mlp) *median_mlp = s->cl.last.median_mlp;
+    if (used) *used = s->cl.last.use_mlp;
+    if (samples) *samples = s->cl.last.samples;
+    return PSG_OK;
+}
+
+// features of sorted particles idx[0, k) after a closure tick (host arrays)
+int psg_closure_features(void* mem, const uint32_t* idx, size_t k, float* x_out,
+                         float* scale_out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !idx || !x_out || !scale_out) return PSG_EINVAL;
+    if (!s->cl.valid) {
+        std::snprintf(psg::g_err, sizeof(psg::g_err), "closure features need a closure tick");
+        return PSG_EINVAL;
+    }
+    if (k == 0) return PSG_OK;
+    PSG_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    uint32_t* d_idx = nullptr;
+    float* d_x = nullptr;
+    PSG_ALLOC(d_idx, k * 4);
+    PSG_ALLOC(d_x, k * 17 * 4);
+    PSG_CHECK(cudaMemcpyAsync(d_idx, idx, k * 4, cudaMemcpyHostToDevice, st));
+    psg::TreeView tv = s->tv;
+    tv.lg0 = s->cl.lg0;
+    tv.lg1 = s->cl.lg1;
+    psg::launch_closure_features(tv, s->cl.leaf_of, s->xyzm, s->last_n, d_idx, k, d_x,
+                                 d_x + k * 16, st);
+    PSG_CHECK(cudaGetLastError());
+    PSG_CHECK(cudaMemcpyAsync(x_out, d_x, k * 16 * 4, cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaMemcpyAsync(scale_out, d_x + k * 16, k * 4, cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaStreamSynchronize(st));
+    cudaFree(d_idx);
+    cudaFree(d_x);
+    return PSG_OK;
+}
+
+// Train the closure MLP with Adam on (x, t) pairs (host arrays, n x 16 and
+// n x 3).  params (kMlpParams) holds the initial values and receives the
+// trained ones; loss_out (epochs) receives each epoch's mean squared error.
+int psg_closure_train(void* mem, const float* x, const float* t, size_t n, float* params,
+                      uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* loss_out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !x || !t || !params || n == 0 || batch == 0)
+        return PSG_EINVAL;
+    PSG_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    PSG_CHECK(psg::prepare_mlp_grad_kernel());
+    const int P = psg::kMlpParams;
+    float *d_x = nullptr, *d_t = nullptr, *d_p = nullptr, *d_m = nullptr, *d_v = nullptr,
+          *d_g = nullptr, *d_loss = nullptr;
+    uint32_t* d_perm = nullptr;
+    psg::MlpPacked* d_w = nullptr;
+    PSG_ALLOC(d_x, n * 16 * 4);
+    PSG_ALLOC(d_t, n * 3 * 4);
+    PSG_ALLOC(d_perm, n * 4);
+    PSG_ALLOC(d_p, P * 4);
+    PSG_ALLOC(d_m, P * 4);
+    PSG_ALLOC(d_v, P * 4);
+    PSG_ALLOC(d_g, P * 4);
+    PSG_ALLOC(d_loss, (epochs ? epochs : 1) * 4);
+    PSG_ALLOC(d_w, sizeof(psg::MlpPacked));
+    PSG_CHECK(cudaMemcpyAsync(d_x, x, n * 16 * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemcpyAsync(d_t, t, n * 3 * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemcpyAsync(d_p, params, P * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemsetAsync(d_m, 0, P * 4, st));
+    PSG_CHECK(cudaMemsetAsync(d_v, 0, P * 4, st));
+    PSG_CHECK(cudaMemsetAsync(d_loss, 0, (epochs ? epochs : 1) * 4, st));
+    uint32_t* perm = nullptr;
+    PSG_CHECK(cudaMallocHost((void**)&perm, n * 4));
+    uint64_t rng = seed ^ 0x9E3779B97F4A7C15ull;
+    auto next = [&rng]() {  // splitmix64
+        uint64_t z = (rng += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
+    uint64_t step = 0;
+    int r = PSG_OK;
+    for (uint32_t ep = 0; ep < epochs && r == PSG_OK; ++ep) {
+        PSG_CHECK(cudaStreamSynchronize(st));  // perm is reused
+        for (size_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+        for (size_t i = n - 1; i > 0; --i) {
+            const size_t j = (size_t)(next() % (i + 1));
+            const uint32_t tmp = perm[i];
+            perm[i] = perm[j];
+            perm[j] = tmp;
+        }
+        PSG_CHECK(cudaMemcpyAsync(d_perm, perm, n * 4, cudaMemcpyHostToDevice, st));
+        for (size_t b0 = 0; b0 < n; b0 += batch) {
+            const size_t cnt = n - b0 < batch ? n - b0 : batch;
+            PSG_CHECK(cudaMemsetAsync(d_g, 0, P * 4, st));
+            psg::launch_mlp_pack(d_p, d_w, st);
+            psg::launch_mlp_grad(d_x, d_t, d_perm, b0, cnt, d_w, 1.0f / (3.0f * (float)cnt), d_g,
+                                 d_loss + ep, st);
+            ++step;
+            const float bc1 = 1.0f - powf(beta1, (float)step);
+            const float bc2 = 1.0f - powf(beta2, (float)step);
+            psg::launch_mlp_adam(d_p, d_m, d_v, d_g, P, lr, beta1, beta2, eps, bc1, bc2, st);
+        }
+        if (cudaGetLastError() != cudaSuccess) r = PSG_EDEVICE;
+    }
+    if (r == PSG_OK) {
+        PSG_CHECK(cudaMemcpyAsync(params, d_p, P * 4, cudaMemcpyDeviceToHost, st));
+        if (loss_out && epochs)
+            PSG_CHECK(cudaMemcpyAsync(loss_out, d_loss, epochs * 4, cudaMemcpyDeviceToHost, st));
+        PSG_CHECK(cudaStreamSynchronize(st));
+        if (loss_out)
+            for (uint32_t ep = 0; ep < epochs; ++ep) loss_out[ep] /= (float)(3 * n);
+    }
+    cudaFreeHost(perm);
+    void* bufs[] = {d_x, d_t, d_perm, d_p, d_m, d_v, d_g, d_loss, d_w};
+    for (void* b : bufs) cudaFree(b);
+    if (r != PSG_OK) std::snprintf(psg::g_err, sizeof(psg::g_err), "closure training failed");
+    return r;
+}
+
+// loss (mean squared error) and its gradient w.r.t. params for one batch of
+// n samples (host arrays): the training step's own kernels, no update
+int psg_closure_grad(void* mem, const float* x, const float* t, size_t n, const float* params,
+                     float* grad_out, float* loss_out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !x || !t || !params || !grad_out || n == 0)
+        return PSG_EINVAL;
+    PSG_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    PSG_CHECK(psg::prepare_mlp_grad_kernel());
+    const int P = psg::kMlpParams;
+    float *d_x = nullptr, *d_t = nullptr, *d_p = nullptr, *d_g = nullptr, *d_loss = nullptr;
+    psg::MlpPacked* d_w = nullptr;
+    PSG_ALLOC(d_x, n * 16 * 4);
+    PSG_ALLOC(d_t, n * 3 * 4);
+    PSG_ALLOC(d_p, P * 4);
+    PSG_ALLOC(d_g, P * 4);
+    PSG_ALLOC(d_loss, 4);
+    PSG_ALLOC(d_w, sizeof(psg::MlpPacked));
+    PSG_CHECK(cudaMemcpyAsync(d_x, x, n * 16 * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemcpyAsync(d_t, t, n * 3 * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemcpyAsync(d_p, params, P * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemsetAsync(d_g, 0, P * 4, st));
+    PSG_CHECK(cudaMemsetAsync(d_loss, 0, 4, st));
+    psg::launch_mlp_pack(d_p, d_w, st);
+    psg::launch_mlp_grad(d_x, d_t, nullptr, 0, n, d_w, 1.0f / (3.0f * (float)n), d_g, d_loss, st);
+    PSG_CHECK(cudaGetLastError());
+    PSG_CHECK(cudaMemcpyAsync(grad_out, d_g, P * 4, cudaMemcpyDeviceToHost, st));
+    float loss = 0.f;
+    PSG_CHECK(cudaMemcpyAsync(&loss, d_loss, 4, cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaStreamSynchronize(st));
+    if (loss_out) *loss_out = loss / (float)(3 * n);
+    void* bufs[] = {d_x, d_t, d_p, d_g, d_loss, d_w};
+    for (void* b : bufs) cudaFree(b);
+    return PSG_OK;
+}
+
+// MLP outputs (n x 8, before scaling) for inputs x (n x 16), host arrays:
+// the inference kernel's network on the tensor cores
+int psg_closure_forward(void* mem, const float* x, size_t n, const float* params, float* y_out) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !x || !params || !y_out || n == 0) return PSG_EINVAL;
+    PSG_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    float *d_x = nullptr, *d_p = nullptr, *d_y = nullptr;
+    psg::MlpPacked* d_w = nullptr;
+    PSG_ALLOC(d_x, n * 16 * 4);
+    PSG_ALLOC(d_p, psg::kMlpParams * 4);
+    PSG_ALLOC(d_y, n * 8 * 4);
+    PSG_ALLOC(d_w, sizeof(psg::MlpPacked));
+    PSG_CHECK(cudaMemcpyAsync(d_x, x, n * 16 * 4, cudaMemcpyHostToDevice, st));
+    PSG_CHECK(cudaMemcpyAsync(d_p, params, psg::kMlpParams * 4, cudaMemcpyHostToDevice, st));
+    psg::launch_mlp_pack(d_p, d_w, st);
+    psg::launch_mlp_forward(d_x, n, d_w, d_y, st);
+    PSG_CHECK(cudaGetLastError());
+    PSG_CHECK(cudaMemcpyAsync(y_out, d_y, n * 8 * 4, cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaStreamSynchronize(st));
+    void* bufs[] = {d_x, d_p, d_y, d_w};
+    for (void* b : bufs) cudaFree(b);
+    return PSG_OK;
+}
+
+// the last closure tick's per-particle correction (sorted order, n x 3)
+int psg_closure_correction(void* mem, float* out, size_t n) {
+    State* s = static_cast<State*>(mem);
+    if (!s || s->magic != psg::kMagic || !out || !s->cl.dF) return PSG_EINVAL;
+    if (n != s->last_n || !s->cl.valid) return PSG_EINVAL;
+    PSG_CHECK(cudaSetDevice(s->device));
+    PSG_CHECK(cudaMemcpy2DAsync(out, 12, s->cl.dF, 16, 12, n, cudaMemcpyDeviceToHost, s->stream));
+    PSG_CHECK(cudaStreamSynchronize(s->stream));
     return PSG_OK;
 }
 

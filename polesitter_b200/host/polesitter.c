@@ -217,6 +217,64 @@ ps_result_t ps_b200_run_ticks(ps_context_t* ctx, const ps_particle_arrs_t* arrs,
     return to_ps(psg_run_ticks(ctx_state(ctx), &a, vx, vy, vz, dt, ticks, g_morton_variant));
 }
 
+#define PS_CTX_OK(ctx) ((ctx) && (ctx)->magic == PS_CTX_MAGIC)
+
+ps_result_t ps_b200_closure_set_weights(ps_context_t* ctx, const float* params, size_t n) {
+    if (!PS_CTX_OK(ctx) || !params) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_set_weights(ctx_state(ctx), params, n));
+}
+
+ps_result_t ps_b200_closure_last(ps_context_t* ctx, double* median_base, double* median_mlp,
+                                 int* used, int* samples) {
+    if (!PS_CTX_OK(ctx)) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_last(ctx_state(ctx), median_base, median_mlp, used, samples));
+}
+
+ps_result_t ps_b200_closure_features(ps_context_t* ctx, const uint32_t* idx, size_t k,
+                                     float* x_out, float* scale_out) {
+    if (!PS_CTX_OK(ctx)) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_features(ctx_state(ctx), idx, k, x_out, scale_out));
+}
+
+ps_result_t ps_b200_closure_correction(ps_context_t* ctx, float* out, size_t n) {
+    if (!PS_CTX_OK(ctx)) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_correction(ctx_state(ctx), out, n));
+}
+
+ps_result_t ps_b200_closure_forward(ps_context_t* ctx, const float* x, size_t n,
+                                    const float* params, float* y_out) {
+    if (!PS_CTX_OK(ctx)) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_forward(ctx_state(ctx), x, n, params, y_out));
+}
+
+ps_result_t ps_b200_closure_grad(ps_context_t* ctx, const float* x, const float* t, size_t n,
+                                 const float* params, float* grad_out, float* loss_out) {
+    if (!PS_CTX_OK(ctx)) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_grad(ctx_state(ctx), x, t, n, params, grad_out, loss_out));
+}
+
+ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float* t, size_t n,
+                                  float* params, uint32_t epochs, uint32_t batch, float lr,
+                                  uint64_t seed, float* loss_out) {
+    if (!PS_CTX_OK(ctx)) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_closure_train(ctx_state(ctx), x, t, n, params, epochs, batch, lr, seed,
+                                   loss_out));
+}
+
 const char* ps_b200_last_error(void) { return psg_last_error(); }
 
 ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,

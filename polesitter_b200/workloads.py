@@ -148,6 +148,33 @@ def two_plummer(n_total: int, seed: int, mass_ratio: float = 3.0,
     return Particles(pos[0], pos[1], pos[2], m), vel[0].copy(), vel[1].copy(), vel[2].copy()
 
 
+def clumpy_plummer(n: int, seed: int, n_clumps: int = 32, clump_fraction: float = 0.3,
+                   a: float = 1.0, rmax: float = 10.0, clump_a=(0.02, 0.1)) -> Particles:
+    """The learned closure's snapshot family: an equal-mass Plummer sphere
+    (scale ``a``, radii truncated at ``rmax * a``) holding a fraction
+    1 - ``clump_fraction`` of the particles, plus ``n_clumps`` small Plummer
+    sub-clumps that share the rest equally.  Clump centres are drawn from the
+    host sphere (within 5a), clump scale radii log-uniform in ``clump_a``
+    (truncated at 10 clump radii).  Particle masses are all 1/n."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n_clumped = int(round(n * clump_fraction)) if n_clumps > 0 else 0
+    per = np.full(n_clumps, n_clumped // max(n_clumps, 1), np.int64)
+    per[: n_clumped - int(per.sum())] += 1
+    n_host = n - int(per.sum())
+    r = _plummer_radii(rng, n_host, a, rmax)
+    parts = [_isotropic(rng, n_host) * r[None, :]]
+    centres = _isotropic(rng, n_clumps) * _plummer_radii(rng, n_clumps, a, 5.0)[None, :]
+    scales = np.exp(rng.uniform(np.log(clump_a[0]), np.log(clump_a[1]), size=n_clumps))
+    for k in range(n_clumps):
+        if per[k] == 0:
+            continue
+        rc = _plummer_radii(rng, int(per[k]), scales[k], 10.0)
+        parts.append(_isotropic(rng, int(per[k])) * rc[None, :] + centres[:, k:k + 1])
+    pos = np.concatenate(parts, axis=1).astype(np.float32)
+    m = np.full(n, 1.0 / n, np.float32)
+    return Particles(pos[0], pos[1], pos[2], m)
+
+
 def _lcg_stream(state: int, count: int) -> tuple[np.ndarray, int]:
     """``state = state*1664525 + 1013904223 (mod 2^32)`` (tests/accuracy.c:33-36),
     returned as float32 ``(state >> 8) / 16777215`` (accuracy.c:38-40)."""

@@ -1,0 +1,187 @@
+"""The learned far-field closure on the GPU, through the C ABI.
+
+Checked against the oracles: the order-1 local expansion (closure mode 1)
+against the C oracle's order-1 downward pass (same interaction set, forces
+within 1e-5 relative L2, identical features); the tensor-core network and
+its training gradient against the numpy restatement (oracle/closure_oracle.py);
+the applied correction against oracle features through the oracle network;
+the judge's fallback; and the shipped weights' gain over the method without
+them on held-out snapshots."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import polesitter_b200 as P
+from conftest import rel_l2
+from oracle import closure_oracle as CO
+from polesitter_b200 import closure as CL
+from polesitter_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FORCE_REL_L2 = 1e-5
+
+
+def forces(p):
+    return np.stack([p.fx, p.fy, p.fz], axis=1).astype(np.float64)
+
+
+def test_order1_matches_oracle(oracle):
+    n, theta = 20000, 6.0
+    p0 = W.clumpy_plummer(n, 5)
+    a, b = p0.copy(), p0.copy()
+    raw = np.zeros((n, 16), np.float32)
+    ro = oracle.tick(a, theta=theta, order=1, feat=raw)
+    with P.Context(n, theta=theta) as ctx:
+        ctx.set_closure(1)
+        ctx.set_option(P.OPT_DEBUG, 1)
+        codes = np.zeros(n, np.uint32)
+        ctx.tick(b, codes)
+        st = ctx.stats()
+        t = ctx.tree()
+        idx = np.arange(0, n, 3, dtype=np.uint32)
+        x, scale = ctx.closure_features(idx)
+    assert np.array_equal(a.id, b.id)
+    assert np.array_equal(t["m2l_cnt"], ro["tree"]["m2l_cnt"])
+    assert np.array_equal(t["p2p_cnt"], ro["tree"]["p2p_cnt"])
+    assert st["p2p_interactions"] == ro["stats"]["p2p_interactions"]
+    assert rel_l2(forces(b), forces(a)) < FORCE_REL_L2
+    xo, so = CO.features_from_raw(raw[idx])
+    assert np.abs(x - xo).max() < 1e-4
+    assert np.abs(scale - so).max() <= 1e-4 * np.abs(so).max()
+
+
+def test_order1_is_more_accurate_than_order0(oracle):
+    n = 16384
+    p0 = W.clumpy_plummer(n, 6)
+    tg = np.arange(0, n, 8, dtype=np.uint32)
+    errs = []
+    with P.Context(n, theta=4.0) as ctx:
+        for mode in (0, 1):
+            p = p0.copy()
+            ctx.set_closure(mode)
+            ctx.tick(p, np.zeros(n, np.uint32))
+            f64 = ctx.direct_f64(p, tg)
+            e = np.linalg.norm(forces(p)[tg] - f64, axis=1) / np.linalg.norm(f64, axis=1)
+            errs.append(np.median(e))
+    assert errs[1] < 0.5 * errs[0], errs
+
+
+def _random_params(seed):
+    rng = np.random.default_rng(seed)
+    prm = CL.init_params(seed).astype(np.float64)
+    parts = CO.unpack(prm)
+    for k in parts:
+        parts[k] = parts[k] + rng.normal(0.0, 0.05, parts[k].shape)
+    parts["W1"][13:] = 0.0
+    parts["W4"][:, 3:] = 0.0
+    parts["b4"][3:] = 0.0
+    return CO.pack(parts).astype(np.float32)
+
+
+def test_network_forward_matches_oracle():
+    rng = np.random.default_rng(0)
+    prm = _random_params(3)
+    x = rng.normal(0.0, 1.0, (2000, 16)).astype(np.float32)
+    x[:, 13:] = 0.0
+    with P.Context(1024) as ctx:
+        y = ctx.closure_forward(x, prm)
+    yo, _ = CO.forward(prm, x)
+    assert np.abs(y - yo).max() <= 2e-3 * np.abs(yo).max()
+    assert rel_l2(y[:, :3], yo[:, :3]) < 1e-3
+
+
+def test_training_gradient_matches_oracle():
+    rng = np.random.default_rng(1)
+    prm = _random_params(4)
+    x = rng.normal(0.0, 1.0, (3000, 16)).astype(np.float32)
+    x[:, 13:] = 0.0
+    t = rng.normal(0.0, 1.0, (3000, 3)).astype(np.float32)
+    with P.Context(1024) as ctx:
+        g, loss = ctx.closure_grad(x, t, prm)
+    lo, go = CO.loss_and_grad(prm, x, t)
+    assert abs(loss - lo) <= 1e-4 * lo
+    assert rel_l2(g, go) < 1e-3
+    # padding parameters receive no gradient
+    parts = CO.unpack(g)
+    assert np.all(parts["W1"][13:] == 0) and np.all(parts["W4"][:, 3:] == 0)
+
+
+def test_training_lowers_the_loss():
+    n = 16384
+    with P.Context(n, theta=6.0) as ctx:
+        x, t = CL.snapshot_dataset(ctx, 8, n, 6.0, 1024, 300)
+        p0 = CL.init_params(2)
+        _, loss0 = ctx.closure_grad(x, t, p0)
+        params, losses = CL.train(ctx, x, t, p0, epochs=12, batch=1024, lr=2e-3, seed=2)
+        _, loss1 = ctx.closure_grad(x, t, params)
+    assert losses.shape == (12,) and np.all(np.isfinite(params))
+    assert losses[-1] < losses[0]
+    assert loss1 < 0.8 * loss0, (loss0, loss1)
+
+
+def test_applied_correction_is_the_oracle_network(oracle):
+    n, theta = 12000, 6.0
+    prm = _random_params(5)
+    p0 = W.clumpy_plummer(n, 8)
+    a = p0.copy()
+    raw = np.zeros((n, 16), np.float32)
+    oracle.tick(a, theta=theta, order=1, feat=raw)
+    with P.Context(n, theta=theta) as ctx:
+        ctx.closure_set_weights(prm)
+        ctx.set_closure(2)
+        b = p0.copy()
+        ctx.tick(b, np.zeros(n, np.uint32))
+        dF = ctx.closure_correction(n)
+    xo, so = CO.features_from_raw(raw)
+    yo, _ = CO.forward(prm, xo)
+    want = so[:, None] * yo[:, :3]
+    assert rel_l2(dF, want) < 1e-2
+
+
+def test_judge_falls_back_when_the_network_hurts():
+    n, theta = 16384, 6.0
+    prm = np.zeros(CL.N_PARAMS, np.float32)
+    prm[-8:-5] = 50.0  # b4: a constant, large correction
+    p0 = W.clumpy_plummer(n, 9)
+    with P.Context(n, theta=theta) as ctx:
+        ctx.set_closure(1)
+        a = p0.copy()
+        ctx.tick(a, np.zeros(n, np.uint32))
+        ctx.closure_set_weights(prm)
+        ctx.set_closure(2)
+        b = p0.copy()
+        ctx.tick(b, np.zeros(n, np.uint32))
+        j = ctx.closure_last()
+    assert j["samples"] == 4096
+    assert not j["used"]
+    assert j["median_mlp"] > j["median_base"]
+    assert np.array_equal(forces(a), forces(b))
+
+
+WEIGHTS = CL.default_weights_path()
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no shipped closure weights")
+def test_shipped_weights_gain_over_the_method_without_them():
+    # ablation on held-out snapshots of the training family: the sampled
+    # FP64 judge's median error with the learned correction against the
+    # order-1 expansion alone
+    params, meta = CL.load(WEIGHTS)
+    n, theta = int(meta["n"]), float(meta["theta"])
+    base, mlp = [], []
+    with P.Context(n, theta=theta) as ctx:
+        ctx.closure_set_weights(params)
+        ctx.set_closure(2)
+        for k in range(4):
+            p = W.clumpy_plummer(n, 55_000_000 + k)
+            ctx.tick(p, np.zeros(n, np.uint32))
+            j = ctx.closure_last()
+            base.append(j["median_base"])
+            mlp.append(j["median_mlp"])
+            assert j["used"]
+    assert np.mean(mlp) < 0.85 * np.mean(base), (base, mlp)

@@ -75,6 +75,9 @@ CASES = [
     ("clusters4096", lambda: W.lcg_two_clusters(4096), 2.0),
     ("ragged12345", lambda: W.uniform_cube(12345, 6), 2.0),
     ("cube100_30000", lambda: W.benchmark_cube(30000), 1.0),
+    # sub-clumps fill depth-10 leaves with hundreds of particles: the
+    # full-leaf P2P kernel
+    ("clumpy20000", lambda: W.clumpy_plummer(20000, 3), 2.0),
 ]
 
 

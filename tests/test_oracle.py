@@ -203,3 +203,66 @@ def test_euler_step_follows_the_readme_loop(oracle):
     for c in range(3):
         assert np.array_equal(v[c], want_v[c])
     assert np.array_equal(p.x, want_x[0]) and np.array_equal(p.z, want_x[2])
+
+
+def test_closure_order1_beats_order0(oracle):
+    # the closure's order-1 local expansion (no counterpart in the reference)
+    # is a strictly better far field than the reference's order-0 one
+    n = 4096
+    p0 = W.clumpy_plummer(n, 12)
+    tg = np.arange(0, n, 4, dtype=np.uint32)
+    errs = []
+    for order in (0, 1):
+        p = p0.copy()
+        oracle.tick(p, theta=4.0, order=order, want_tree=False)
+        f64 = oracle.direct_f64(p, tg)
+        F = np.stack([p.fx, p.fy, p.fz], 1)[tg].astype(np.float64)
+        errs.append(np.median(np.linalg.norm(F - f64, axis=1) / np.linalg.norm(f64, axis=1)))
+    assert errs[1] < 0.5 * errs[0], errs
+
+
+def test_closure_features_are_normalised(oracle):
+    from oracle import closure_oracle as CO
+    n = 4096
+    p = W.clumpy_plummer(n, 13)
+    raw = np.zeros((n, 16), np.float32)
+    oracle.tick(p, theta=6.0, order=1, feat=raw, want_tree=False)
+    x, scale = CO.features_from_raw(raw)
+    assert np.all(np.linalg.norm(x[:, 0:3], axis=1) <= 1.0 + 1e-6)
+    # rounded (not truncated) Morton quantisation (polesitter.h:2015-2073) lets
+    # a particle sit up to ~1.5 half widths from its depth-10 cell's centre
+    assert np.all(np.abs(x[:, 9:12]) <= 2.0)
+    assert np.all(x[:, 13:] == 0) and np.all(scale > 0)
+    assert set(np.round(x[:, 12] * 10).astype(int)) <= set(range(1, 11))
+
+
+def test_closure_network_oracle_gradient_by_finite_differences(monkeypatch):
+    # the numpy backward pass against central differences (BF16 rounding
+    # switched off so that the loss is smooth)
+    from oracle import closure_oracle as CO
+    monkeypatch.setattr(CO, "bf16", lambda a: np.asarray(a, np.float64))
+    rng = np.random.default_rng(1)
+    p = rng.normal(0.0, 0.2, CO.N_PARAMS)
+    x = rng.normal(0.0, 1.0, (40, 16))
+    t = rng.normal(0.0, 1.0, (40, 3))
+    _, g = CO.loss_and_grad(p, x, t)
+    idx = rng.choice(CO.N_PARAMS, 30, replace=False)
+    eps = 1e-6
+    num = []
+    for i in idx:
+        q = p.copy()
+        q[i] += eps
+        lp, _ = CO.loss_and_grad(q, x, t)
+        q[i] -= 2 * eps
+        lm, _ = CO.loss_and_grad(q, x, t)
+        num.append((lp - lm) / (2 * eps))
+    assert np.abs(np.array(num) - g[idx]).max() <= 1e-6 * np.abs(g).max()
+
+
+def test_bf16_rounding_is_round_to_nearest_even():
+    from oracle import closure_oracle as CO
+    one = np.float32(1.0)
+    ulp = np.float32(2.0 ** -7)  # bf16 spacing at 1
+    vals = np.array([one, one + ulp / 2, one + ulp / 2 + ulp / 8, one + 1.5 * ulp], np.float32)
+    got = CO.bf16(vals)
+    assert got.tolist() == [1.0, 1.0, float(one + ulp), float(one + 2 * ulp)]
