@@ -39,7 +39,8 @@ ps_result_t ps_b200_get_stats(ps_context_t* ctx, uint64_t* out, size_t n);
 /* per-phase device times of the last tick in ms (PS_B200_OPT_TIMING):
  * [0] sort, [1] gather + write-back, [2] tree build, [3] upward pass,
  * [4] interaction pass of internal nodes (MAC/M2L/L2L, all levels),
- * [5] leaf pass (MAC/M2L/L2L + P2P + L2P), [6] whole tick */
+ * [5] leaf pass (MAC/M2L/L2L + P2P + L2P), [6] whole tick, [7] learned
+ * closure (correction, judge decision), [8] P2P + L2P of full leaves */
 ps_result_t ps_b200_last_timing(ps_context_t* ctx, float* ms, size_t n);
 
 /* The last tick's tree in canonical form: level-major, each level in Morton

@@ -284,15 +284,17 @@ class Context:
                 "nodes": int(out[8]), "max_stack": int(out[9]), "p2p_chunks": int(out[10]),
                 "traversal_runs": int(out[11]), "max_leaf": int(out[12]),
                 "dense_records": int(out[13]),
-                "lanes": int(out[16]), "leaf_groups": int(out[17]), "dfs_steps": int(out[18])}
+                "lanes": int(out[16]), "leaf_groups": int(out[17]), "dfs_steps": int(out[18]),
+                "slowest_group_cycles": int(out[19]) >> 28,
+                "slowest_group_node": int(out[19]) & 0xFFFFFFF}
 
     def timing(self) -> dict:
         import numpy as np
-        out = np.zeros(8, np.float32)
-        _check("ps_b200_last_timing", lib().ps_b200_last_timing(self.ptr, out.ctypes.data, 8))
+        out = np.zeros(9, np.float32)
+        _check("ps_b200_last_timing", lib().ps_b200_last_timing(self.ptr, out.ctypes.data, 9))
         return {"sort": float(out[0]), "gather": float(out[1]), "tree": float(out[2]),
                 "upward": float(out[3]), "internal": float(out[4]), "leaves": float(out[5]),
-                "tick": float(out[6]), "closure": float(out[7])}
+                "tick": float(out[6]), "closure": float(out[7]), "full_leaves": float(out[8])}
 
     def tree(self) -> dict:
         import numpy as np

@@ -538,11 +538,15 @@ void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const 
                                                                     x_out, scale_out);
 }
 
-void launch_judge(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
-                  const float* fx, const float* fy, const float* fz, const float4* dF, int allow,
-                  uint32_t tick, JudgeOut* out, int sms, cudaStream_t st) {
+void launch_judge_direct(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
+                         uint32_t tick, int blocks, cudaStream_t st) {
     k_judge_sample<<<(s + 255) / 256, 256, 0, st>>>(tg, s, n, tick);
-    launch_direct_f64(xyzm, n, tg, (size_t)s, f64, sms, st);
+    launch_direct_f64(xyzm, n, tg, (size_t)s, f64, blocks, st);
+}
+
+void launch_judge_decide(const uint32_t* tg, int s, const double* f64, const float* fx,
+                         const float* fy, const float* fz, const float4* dF, int allow,
+                         JudgeOut* out, cudaStream_t st) {
     k_judge_decide<<<1, 1024, 0, st>>>(tg, s, f64, fx, fy, fz, dF, allow, out);
 }
 

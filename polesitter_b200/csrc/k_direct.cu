@@ -66,12 +66,12 @@ __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __rest
 }
 
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
-                       double* out, int sms, cudaStream_t st) {
+                       double* out, int blocks, cudaStream_t st) {
     if (n_targets == 0) return;
     cudaMemsetAsync(out, 0, n_targets * 3 * sizeof(double), st);
     const size_t tblocks = (n_targets + kDirThreads - 1) / kDirThreads;
-    // ~8 blocks per SM in total, each source chunk at least 1024 particles
-    size_t splits = ((size_t)sms * 8 + tblocks - 1) / tblocks;
+    // about `blocks` blocks in total, each source chunk at least 1024 particles
+    size_t splits = ((size_t)blocks + tblocks - 1) / tblocks;
     const size_t max_splits = (n + 1023) / 1024;
     if (splits > max_splits) splits = max_splits;
     if (splits < 1) splits = 1;

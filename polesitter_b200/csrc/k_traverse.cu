@@ -58,9 +58,10 @@ constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-en
 constexpr int kP2PCap = 128;              // staged P2P sources of a group
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
-constexpr uint32_t kDenseLeaf = 8;        // leaves this full go to k_dense_p2p
+constexpr uint32_t kDenseGroup = 8;       // DENSE: groups with this many leaf particles go to k_dense_p2p
 constexpr uint32_t kDenseChunk = 32;      // target particles per dense work record
 constexpr uint32_t kDenseSwitch = 32;     // fullest leaf from which the DENSE leaf pass runs
+constexpr uint32_t kBigSource = 16;       // DENSE: sources this full are summed by all lanes
 
 enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
@@ -89,6 +90,7 @@ struct SmemLeaf {
     uint8_t cand_mask[kCandBuf];
     uint8_t stk_mask[kStackCap];
     uint8_t p2p_mask[kP2PCap];
+    uint8_t big[kP2PCap];   // staged sources with more than kBigSource particles
 };
 
 template <int MODE>
@@ -211,35 +213,39 @@ __device__ __forceinline__ void p2p_range(const float4* __restrict__ xyzm, uint2
     }
 }
 
-// one k_dense_p2p work record per 32 target particles of each full leaf
-// child (bits of dense_mask) of the group whose children start at node fc;
-// phead is the group's complete P2P source chain
-__device__ __noinline__ void record_dense(const SmemLeaf& sm, uint32_t dense_mask, uint32_t fc,
+// k_dense_p2p work records for the leaf children in mask of the group whose
+// children start at node fc: each run of consecutive children (their
+// particles are contiguous) is cut into records of up to kDenseChunk
+// particles; phead is the group's complete P2P source chain.
+// Record: fc, phead, first particle, count | run's child mask << 8.
+__device__ __noinline__ void record_dense(const SmemLeaf& sm, uint32_t mask, uint32_t fc,
                                           uint32_t phead, uint4* rec, uint32_t cap,
                                           Status* status) {
     const uint32_t lane = lane_id();
-    for (uint32_t m = dense_mask; m; m &= m - 1) {
-        const uint32_t q = __ffs(m) - 1;
-        const uint2 up = sm.cpart[q];
-        const uint32_t nrec = (up.y + kDenseChunk - 1) / kDenseChunk;
+    while (mask) {
+        const uint32_t q0 = __ffs(mask) - 1;
+        uint32_t q1 = q0;
+        while (q1 + 1 < 8 && ((mask >> (q1 + 1)) & 1u)) ++q1;
+        const uint32_t run = ((2u << q1) - 1u) & ~((1u << q0) - 1u);
+        mask &= ~run;
+        const uint32_t first = sm.cpart[q0].x;
+        uint32_t count = 0;
+        for (uint32_t q = q0; q <= q1; ++q) count += sm.cpart[q].y;
+        const uint32_t nrec = (count + kDenseChunk - 1) / kDenseChunk;
         uint32_t r0 = 0;
         if (lane == 0) r0 = atomicAdd(&status->dense_count, nrec);
         r0 = __shfl_sync(0xFFFFFFFFu, r0, 0);
         for (uint32_t k = lane; k < nrec; k += 32) {
             if (r0 + k < cap) {
                 const uint32_t c0 = k * kDenseChunk;
-                rec[r0 + k] = make_uint4((fc + q) | (q << 28), phead, up.x + c0,
-                                         min(kDenseChunk, up.y - c0));
+                rec[r0 + k] = make_uint4(fc, phead, first + c0,
+                                         min(kDenseChunk, count - c0) | (run << 8));
             }
         }
         if (lane == 0 && r0 + nrec > cap) set_err(status, PSG_ERR_DENSE_OVERFLOW);
     }
 }
 
-// L2P + P2P of a group's leaf children once its candidates are done: with
-// DENSE, full leaves are handed to k_dense_p2p; the others get
-// F = m (L + P2P sum) here, one target particle at a time with the lanes over
-// its sources.
 struct LeafOut {
     const float4* xyzm;
     const uint4* info;
@@ -254,6 +260,10 @@ struct LeafOut {
     int kahan;
 };
 
+// L2P + P2P of a group's leaf children once its candidates are done: with
+// DENSE, a group holding kDenseGroup or more leaf particles is handed to
+// k_dense_p2p; the others get F = m (L + P2P sum) here, one target particle
+// at a time with the lanes over its sources.
 template <bool DEBUG, bool GRAD, bool DENSE>
 __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uint32_t tgt_mask,
                                            uint32_t fc, uint32_t pfill, uint32_t phead,
@@ -262,9 +272,12 @@ __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uin
     // ---- full leaves (depth-10 cells with many particles) go to
     // k_dense_p2p: the group's whole source list to HBM chunks,
     // then one work record per 32 target particles ----
-    uint32_t dense = 0;
-    if (DENSE && lane < 8 && ((tgt_mask >> lane) & 1u)) dense = sm.cpart[lane].y >= kDenseLeaf;
-    const uint32_t dense_mask = __ballot_sync(0xFFFFFFFFu, dense != 0) & 0xFFu;
+    uint32_t dense_mask = 0;
+    if constexpr (DENSE) {
+        uint32_t cnt = 0;
+        if (lane < 8 && ((tgt_mask >> lane) & 1u)) cnt = sm.cpart[lane].y;
+        if (warp_sum(cnt) >= kDenseGroup) dense_mask = tgt_mask;
+    }
     if (DENSE && dense_mask) {
         if (pfill) {
             phead = spill_p2p(sm, pfill, phead, o.p2p, status);
@@ -273,9 +286,28 @@ __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uin
         record_dense(sm, dense_mask, fc, phead, o.dense_rec, o.dense_cap, status);
     }
     // ---- L2P + P2P: F = m * (L(u) + sum of u's P2P sources) ----
-    for (uint32_t e = lane; e < pfill; e += 32) {
-        const uint4 si = o.info[sm.p2p_node[e]];
-        sm.p2p_range[e] = make_uint2(si.x, si.y);
+    // A lane takes whole source leaves; with DENSE, a source leaf holding more
+    // than kBigSource particles is shared by all lanes instead, so no lane
+    // walks a full leaf alone while the others wait.
+    uint32_t nbig = 0;
+    if constexpr (DENSE) {
+        for (uint32_t e0 = 0; e0 < pfill; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            bool big = false;
+            if (e < pfill) {
+                const uint4 si = o.info[sm.p2p_node[e]];
+                sm.p2p_range[e] = make_uint2(si.x, si.y);
+                big = si.y > kBigSource;
+            }
+            const uint32_t bm = __ballot_sync(0xFFFFFFFFu, big);
+            if (big) sm.big[nbig + __popc(bm & lanemask_lt())] = (uint8_t)e;
+            nbig += __popc(bm);
+        }
+    } else {
+        for (uint32_t e = lane; e < pfill; e += 32) {
+            const uint4 si = o.info[sm.p2p_node[e]];
+            sm.p2p_range[e] = make_uint2(si.x, si.y);
+        }
     }
     __syncwarp();
     unsigned long long inter = 0;
@@ -284,23 +316,66 @@ __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uin
         const uint32_t q = __ffs(m) - 1;
         const uint2 up = sm.cpart[q];
         const float4 L = sm.sL[q];
-        for (uint32_t ti = 0; (!DENSE || up.y < kDenseLeaf) && ti < up.y; ++ti) {
+        for (uint32_t ti = 0; (!DENSE || !((dense_mask >> q) & 1u)) && ti < up.y; ++ti) {
             const float4 t = o.xyzm[up.x + ti];
             float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
             for (uint32_t e = lane; e < pfill; e += 32) {
                 if ((sm.p2p_mask[e] >> q) & 1u) {
                     const uint2 r = sm.p2p_range[e];
-                    p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
-                    if (DEBUG) inter += r.y;
+                    if (!DENSE || r.y <= kBigSource) {
+                        p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
+                        if (DEBUG) inter += r.y;
+                    }
                 }
             }
-            for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
-                if (lane < o.p2p.cnt[c] &&
-                    ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
-                    const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
-                    p2p_range(o.xyzm, make_uint2(si.x, si.y), t, o.kahan, bx, by, bz,
-                              cx, cy, cz);
-                    if (DEBUG) inter += si.y;
+            if constexpr (DENSE) {
+                for (uint32_t b = 0; b < nbig; ++b) {
+                    const uint32_t e = sm.big[b];
+                    if (!((sm.p2p_mask[e] >> q) & 1u)) continue;
+                    const uint2 r = sm.p2p_range[e];
+                    for (uint32_t j = lane; j < r.y; j += 32) {
+                        p2p_range(o.xyzm, make_uint2(r.x + j, 1u), t, o.kahan, bx, by, bz, cx, cy,
+                                  cz);
+                        if (DEBUG) inter += 1;
+                    }
+                }
+            }
+            if constexpr (DENSE) {
+                for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
+                    const bool has = lane < o.p2p.cnt[c] &&
+                                     ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u);
+                    uint2 r = make_uint2(0u, 0u);
+                    if (has) {
+                        const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
+                        r = make_uint2(si.x, si.y);
+                    }
+                    const bool big = DENSE && has && r.y > kBigSource;
+                    if (has && !big) {
+                        p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
+                        if (DEBUG) inter += r.y;
+                    }
+                    if constexpr (DENSE) {
+                        for (uint32_t bm = __ballot_sync(0xFFFFFFFFu, big); bm; bm &= bm - 1) {
+                            const int l = __ffs(bm) - 1;
+                            const uint32_t bx0 = __shfl_sync(0xFFFFFFFFu, r.x, l);
+                            const uint32_t bn = __shfl_sync(0xFFFFFFFFu, r.y, l);
+                            for (uint32_t jj = lane; jj < bn; jj += 32) {
+                                p2p_range(o.xyzm, make_uint2(bx0 + jj, 1u), t, o.kahan, bx, by, bz,
+                                          cx, cy, cz);
+                                if (DEBUG) inter += 1;
+                            }
+                        }
+                    }
+                }
+            } else {
+                for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
+                    if (lane < o.p2p.cnt[c] &&
+                        ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
+                        const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
+                        p2p_range(o.xyzm, make_uint2(si.x, si.y), t, o.kahan, bx, by, bz,
+                                  cx, cy, cz);
+                        if (DEBUG) inter += si.y;
+                    }
                 }
             }
             const float sx = warp_sum(bx - cx);
@@ -407,6 +482,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 }
                 pid = tv.lvl_base[dp] + (g - off);
             }
+            const long long t_group = DEBUG ? clock64() : 0;
             const uint32_t plink = tv.link[pid];
             const uint32_t nc = plink >> 28;
             if (nc == 0) continue;
@@ -743,6 +819,11 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     LeafOut{A.xyzm, tv.info, A.p2p, A.fx, A.fy, A.fz, A.leaf_of, tv.dbg_p2p,
                             A.dense_rec, A.dense_cap, A.kahan},
                     tgt_mask, fc, pfill, phead, status);
+                if (DEBUG && lane == 0) {
+                    const unsigned long long cyc = (unsigned long long)(clock64() - t_group);
+                    atomicMax(&status->stat[PSG_STAT_SLOWEST_GROUP],
+                              (min(cyc, (1ull << 36) - 1) << 28) | pid);
+                }
             }
         }
     }
@@ -769,9 +850,16 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         r = __shfl_sync(0xFFFFFFFFu, r, 0);
         if (r >= total) break;
         const uint4 rec = A.dense_rec[r];
-        const uint32_t u = rec.x & kLinkMask, q = rec.x >> 28;
-        const bool active = lane < rec.w;
+        const uint32_t fc = rec.x, run = rec.w >> 8;
+        const bool active = lane < (rec.w & 0xFFu);
         const uint32_t i = rec.z + (active ? lane : 0u);
+        // this lane's leaf: the child of the run whose particles hold i
+        uint32_t q = __ffs(run) - 1;
+        for (uint32_t m = run; m; m &= m - 1) {
+            const uint32_t qq = __ffs(m) - 1;
+            if (tv.info[fc + qq].x <= i) q = qq;
+        }
+        const uint32_t u = fc + q;
         const float4 t = A.xyzm[i];
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
         for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
@@ -804,6 +892,266 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
     if (DEBUG) {
         inter = warp_sum(inter);
         if (lane == 0 && inter) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+    }
+}
+
+// L2L + L2P + P2P of the shallow leaves (depth <= heavy_depth; the leaf
+// pass starts below them), one block each.  A shallow leaf is a large cell, so its walk -- the reference's
+// (t leaf, s) recursion over the whole candidate set -- reaches a large part
+// of the tree; the block runs it level-synchronously: the frontier of
+// candidates at one level is tested by all threads (separated: M2L, leaf:
+// P2P, else: its children go to the next frontier, placed by a block scan).
+// Frontier order and the final reduction are fixed, so the result does not
+// depend on scheduling.  Shallow leaves (depth < 10) hold one particle.
+constexpr int kHeavyThreads = 512;
+constexpr int kHeavyWarps = kHeavyThreads / 32;
+
+// exclusive block scan of v; returns the block total
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t& excl, uint32_t* s_w) {
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint32_t inc = warp_incl_scan(v);
+    if (lane == 31) s_w[w] = inc;
+    __syncthreads();
+    uint32_t base = 0, total = 0;
+    for (int k = 0; k < kHeavyWarps; ++k) {
+        const uint32_t x = s_w[k];
+        if (k < (int)w) base += x;
+        total += x;
+    }
+    __syncthreads();
+    excl = base + inc - v;
+    return total;
+}
+
+template <bool DEBUG, bool GRAD>
+__global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
+    __shared__ uint32_t s_w[kHeavyWarps];
+    __shared__ uint32_t s_rec;
+    __shared__ float s_red[kHeavyWarps][12];
+    __shared__ unsigned long long s_cnt[kHeavyWarps][3];
+    Status* status = A.status;
+    if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_HEAVY_OVERFLOW)) return;
+    const TreeView& tv = A.tv;
+    // work items: the leaf children of the nodes at depths 0 .. heavy_depth-1
+    uint32_t cum[kMaxDepth + 1];
+    uint32_t total = 0;
+    for (int d = 0; d < A.heavy_depth && d < kMaxDepth; ++d) {
+        cum[d] = total;
+        total += status->lvl_count[d];
+    }
+    if (total == 0) return;
+    const uint32_t tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
+    const float theta2 = __fmul_rn(A.theta, A.theta);
+    uint32_t* fa = A.heavy_frontier + (size_t)blockIdx.x * 2 * A.heavy_fcap;
+    uint32_t* fb = fa + A.heavy_fcap;
+    uint32_t leaves = 0, pid = 0, dp = 0, fc = 0;  // current group's leaf children
+    for (;;) {
+        if (leaves == 0) {
+            // next group with leaf children
+            if (tid == 0) s_rec = atomicAdd(&status->heavy_work, 1u);
+            __syncthreads();
+            const uint32_t g = s_rec;
+            __syncthreads();
+            if (g >= total) break;
+            dp = 0;
+            for (int d = 1; d < A.heavy_depth && d < kMaxDepth; ++d)
+                if (g >= cum[d]) dp = d;
+            pid = tv.lvl_base[dp] + (g - cum[dp]);
+            const uint32_t plink = tv.link[pid];
+            fc = plink & kLinkMask;
+            for (uint32_t q = 0; q < (plink >> 28); ++q)
+                if ((tv.link[fc + q] >> 28) == 0) leaves |= 1u << q;
+            if (leaves == 0) continue;
+        }
+        const uint32_t u = fc + __ffs(leaves) - 1;
+        leaves &= leaves - 1;
+        const float4 ug = tv.geo[u];
+        const uint4 ui = tv.info[u];
+        const float4 t = A.xyzm[ui.x];
+        // initial candidates: cand(p)
+        uint32_t F = 0;
+        if (dp <= 1) {
+            if (tid == 0) fa[0] = 0;  // the root
+            F = 1;
+        } else {
+            const uint32_t* nsl = A.ns + tv.ns_off[pid];
+            const uint32_t nsn = tv.ns_cnt[pid];
+            for (uint32_t e0 = 0; e0 < nsn; e0 += kHeavyThreads) {
+                const uint32_t e = e0 + tid;
+                uint32_t s0 = 0, link = 0, c = 0;
+                if (e < nsn) {
+                    s0 = nsl[e];
+                    link = tv.link[s0];
+                    c = (link >> 28) ? (link >> 28) : 1u;
+                }
+                uint32_t ex;
+                const uint32_t tot = block_scan(c, ex, s_w);
+                if (F + tot > A.heavy_fcap) {
+                    if (tid == 0) set_err(status, PSG_ERR_HEAVY_OVERFLOW);
+                    return;
+                }
+                for (uint32_t i = 0; i < c; ++i)
+                    fa[F + ex + i] = (link >> 28) ? (link & kLinkMask) + i : s0;
+                F += tot;
+            }
+        }
+        __syncthreads();
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+        unsigned long long n_m2l = 0, n_p2p = 0, n_inter = 0;
+        while (F > 0) {
+            uint32_t Fn = 0;
+            for (uint32_t i0 = 0; i0 < F; i0 += kHeavyThreads) {
+                const uint32_t i = i0 + tid;
+                uint32_t c = 0, link = 0;
+                if (i < F) {
+                    const uint32_t sn = fa[i];
+                    const float4 sg = tv.geo[sn];
+                    float dx, dy, dz, d2;
+                    if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w, theta2, dx,
+                                      dy, dz, d2)) {
+                        const float4 mp = tv.mp[sn];
+                        float fx, fy, fz;
+                        if constexpr (GRAD) {
+                            float g3, gi;
+                            m2l_field_grad(dx, dy, dz, d2, mp, fx, fy, fz, g3, gi);
+                            g[0] += fmaf(g3 * dx, dx, -gi);
+                            g[1] += fmaf(g3 * dy, dy, -gi);
+                            g[2] += fmaf(g3 * dz, dz, -gi);
+                            g[3] += g3 * dx * dy;
+                            g[4] += g3 * dx * dz;
+                            g[5] += g3 * dy * dz;
+                        } else {
+                            m2l_field(dx, dy, dz, d2, mp, fx, fy, fz);
+                        }
+                        ax += fx;
+                        ay += fy;
+                        az += fz;
+                        ++n_m2l;
+                    } else {
+                        link = tv.link[sn];
+                        c = link >> 28;
+                        if (c == 0) {  // leaf x leaf: P2P
+                            const uint4 si = tv.info[sn];
+                            p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz, cx,
+                                      cy, cz);
+                            ++n_p2p;
+                            n_inter += si.y;
+                        }
+                    }
+                }
+                uint32_t ex;
+                const uint32_t tot = block_scan(c, ex, s_w);
+                if (Fn + tot > A.heavy_fcap) {
+                    if (tid == 0) set_err(status, PSG_ERR_HEAVY_OVERFLOW);
+                    return;
+                }
+                for (uint32_t k = 0; k < c; ++k) fb[Fn + ex + k] = (link & kLinkMask) + k;
+                Fn += tot;
+            }
+            __syncthreads();
+            uint32_t* tmp = fa;
+            fa = fb;
+            fb = tmp;
+            F = Fn;
+        }
+        // fixed-order block reduction
+        float v[12] = {ax, ay, az, g[0], g[1], g[2], g[3], g[4], g[5], bx - cx, by - cy, bz - cz};
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const float x = warp_sum(v[k]);
+            if (lane == 0) s_red[w][k] = x;
+        }
+        if (DEBUG) {
+            const unsigned long long c0 = warp_sum(n_m2l), c1 = warp_sum(n_p2p),
+                                     c2 = warp_sum(n_inter);
+            if (lane == 0) {
+                s_cnt[w][0] = c0;
+                s_cnt[w][1] = c1;
+                s_cnt[w][2] = c2;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float sum[12];
+            for (int k = 0; k < 12; ++k) {
+                sum[k] = 0.f;
+                for (int q = 0; q < kHeavyWarps; ++q) sum[k] += s_red[q][k];
+            }
+            // L2L from the parent, then L2P at the particle
+            const float4 Lp = tv.lt[pid];
+            float4 L = make_float4(0.f, __fadd_rn(sum[0], Lp.y), __fadd_rn(sum[1], Lp.z),
+                                   __fadd_rn(sum[2], Lp.w));
+            float lx = L.y, ly = L.z, lz = L.w;
+            if constexpr (GRAD) {
+                float4 G0 = make_float4(sum[3], sum[4], sum[5], sum[6]);
+                float2 G1 = make_float2(sum[7], sum[8]);
+                if (dp >= 2) {
+                    const float4 cp = tv.geo[pid];
+                    const float4 Gp0 = tv.lg0[pid];
+                    const float2 Gp1 = tv.lg1[pid];
+                    const float3 sh = grad_apply(Gp0, Gp1, ug.x - cp.x, ug.y - cp.y, ug.z - cp.z);
+                    L.y += sh.x;
+                    L.z += sh.y;
+                    L.w += sh.z;
+                    G0.x += Gp0.x;
+                    G0.y += Gp0.y;
+                    G0.z += Gp0.z;
+                    G0.w += Gp0.w;
+                    G1.x += Gp1.x;
+                    G1.y += Gp1.y;
+                }
+                tv.lg0[u] = G0;
+                tv.lg1[u] = G1;
+                const float3 at = grad_apply(G0, G1, t.x - ug.x, t.y - ug.y, t.z - ug.z);
+                lx = L.y + at.x;
+                ly = L.z + at.y;
+                lz = L.w + at.z;
+                if (A.leaf_of) A.leaf_of[ui.x] = u;
+            }
+            tv.lt[u] = L;
+            const double mm = (double)t.w;
+            A.fx[ui.x] = (float)(mm * ((double)lx + (double)sum[9]));
+            A.fy[ui.x] = (float)(mm * ((double)ly + (double)sum[10]));
+            A.fz[ui.x] = (float)(mm * ((double)lz + (double)sum[11]));
+            if (DEBUG) {
+                unsigned long long c0 = 0, c1 = 0, c2 = 0;
+                for (int q = 0; q < kHeavyWarps; ++q) {
+                    c0 += s_cnt[q][0];
+                    c1 += s_cnt[q][1];
+                    c2 += s_cnt[q][2];
+                }
+                tv.dbg_m2l[u] = (uint32_t)c0;
+                tv.dbg_p2p[u] = (uint32_t)c1;
+                atomicAdd(&status->stat[PSG_STAT_M2L], c0);
+                atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS], c1);
+                atomicAdd(&status->stat[PSG_STAT_P2P_INTER], c2);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// the leaf pass's work counter starts past the groups of depths 0 ..
+// heavy_depth-1, whose leaf children k_heavy_leaf takes
+__global__ void k_leaf_start(Status* status, int heavy_depth) {
+    uint32_t skip = 0;
+    for (int d = 0; d < heavy_depth && d < kMaxDepth; ++d) skip += status->lvl_count[d];
+    status->work[0] = skip;
+}
+
+void launch_leaf_start(Status* status, int heavy_depth, cudaStream_t st) {
+    k_leaf_start<<<1, 1, 0, st>>>(status, heavy_depth);
+}
+
+void launch_heavy_leaf(const TravArgs& A, int grid, cudaStream_t st) {
+    if (A.order >= 1) {
+        if (A.debug) k_heavy_leaf<true, true><<<grid, kHeavyThreads, 0, st>>>(A);
+        else k_heavy_leaf<false, true><<<grid, kHeavyThreads, 0, st>>>(A);
+    } else {
+        if (A.debug) k_heavy_leaf<true, false><<<grid, kHeavyThreads, 0, st>>>(A);
+        else k_heavy_leaf<false, false><<<grid, kHeavyThreads, 0, st>>>(A);
     }
 }
 

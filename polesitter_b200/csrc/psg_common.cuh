@@ -75,6 +75,8 @@ struct Status {
     uint32_t dense_count;                  // full-leaf P2P records written
     uint32_t dense_work;                   // ... and taken by k_dense_p2p
     uint32_t max_leaf;                     // particles in the fullest leaf
+    uint32_t heavy_work;                   // groups taken by k_heavy_leaf
+    uint32_t pad_heavy;
 };
 
 // P2P sources spilled from the traversal: chunk c holds cnt[c] source-leaf

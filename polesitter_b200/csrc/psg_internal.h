@@ -28,6 +28,7 @@ extern "C" {
 #define PSG_ERR_NODES 0x8u        /* tree level over its capacity */
 #define PSG_ERR_P2P_OVERFLOW 0x10u /* P2P chunk store too small: regrow, rerun */
 #define PSG_ERR_DENSE_OVERFLOW 0x20u /* full-leaf record list too small: regrow, rerun */
+#define PSG_ERR_HEAVY_OVERFLOW 0x40u /* shallow-leaf records or frontier too small */
 
 /* debug statistics slots (Status.stat) */
 #define PSG_STAT_MAC 0
@@ -41,6 +42,7 @@ extern "C" {
 #define PSG_STAT_LANES 8        /* occupied candidate lanes over all chunks */
 #define PSG_STAT_GROUPS 9       /* groups processed (leaf mode) */
 #define PSG_STAT_DFS_STEPS 10
+#define PSG_STAT_SLOWEST_GROUP 11 /* leaf pass: (clock cycles << 28) | node of the slowest group */
 
 /* Morton quantisation variants of polesitter.h:2013-2157 */
 #define PSG_MORTON_AVX2 0
@@ -107,6 +109,7 @@ int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n
 #define PSG_OPT_KAHAN 6          /* 1: compensated FP32 sums in P2P */
 #define PSG_OPT_CLOSURE 7        /* 0 reference, 1 order-1 local, 2 + learned correction */
 #define PSG_OPT_JUDGE 8          /* 1: sampled FP64 judge in closure mode 1 too */
+#define PSG_OPT_HEAVY_DEPTH 9    /* leaves this shallow walk block-parallel (-1: from theta) */
 
 /* the learned far-field closure (k_closure.cu) */
 #define PSG_CLOSURE_PARAMS 9928

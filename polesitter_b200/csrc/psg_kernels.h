@@ -52,6 +52,8 @@ const void* traverse_internal_kernel_ptr(int order);
 void launch_traverse_internal(const TravArgs& A, int level, int grid, cudaStream_t st);
 void launch_traverse_leaves(const TravArgs& A, const int grid[2], cudaStream_t st);
 void launch_dense_p2p(const TravArgs& A, int grid, cudaStream_t st);
+void launch_heavy_leaf(const TravArgs& A, int grid, cudaStream_t st);
+void launch_leaf_start(Status* status, int heavy_depth, cudaStream_t st);
 
 
 // k_tick.cu -- the caller's tick loop on the device (README.md:65-111)
@@ -82,9 +84,13 @@ void launch_closure_mlp(const TreeView& tv, const uint32_t* leaf_of, const float
 void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm,
                              size_t n, const uint32_t* idx, size_t k, float* x_out,
                              float* scale_out, cudaStream_t st);
-void launch_judge(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
-                  const float* fx, const float* fy, const float* fz, const float4* dF, int allow,
-                  uint32_t tick, JudgeOut* out, int sms, cudaStream_t st);
+// the judge's FP64 direct sum on a sample (runs beside the tree build and
+// traversal on its own stream) and its decision (after the traversal)
+void launch_judge_direct(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
+                         uint32_t tick, int blocks, cudaStream_t st);
+void launch_judge_decide(const uint32_t* tg, int s, const double* f64, const float* fx,
+                         const float* fy, const float* fz, const float4* dF, int allow,
+                         JudgeOut* out, cudaStream_t st);
 void launch_closure_apply(float* fx, float* fy, float* fz, const float4* dF, size_t n,
                           const JudgeOut* j, int sms, cudaStream_t st);
 void launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st);
@@ -99,7 +105,7 @@ void launch_mlp_adam(float* p, float* m, float* v, const float* g, int n, float 
 
 // k_direct.cu -- FP64 direct-sum forces for sampled targets (tests/accuracy.c:42-72)
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
-                       double* out /*[n_targets][3]*/, int sms, cudaStream_t st);
+                       double* out /*[n_targets][3]*/, int blocks, cudaStream_t st);
 
 }  // namespace psg
 
@@ -124,5 +130,8 @@ struct TravArgs {
     uint32_t* leaf_of;  // closure: leaf node of each sorted particle (order 1)
     uint4* dense_rec;   // full-leaf P2P work records: leaf | q << 28, chain, first, count
     uint32_t dense_cap;
+    int heavy_depth;    // leaf children of nodes above this depth go to k_heavy_leaf
+    uint32_t* heavy_frontier;  // per block: 2 x heavy_fcap candidate slots
+    uint32_t heavy_fcap;
 };
 }  // namespace psg

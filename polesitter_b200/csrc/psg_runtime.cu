@@ -43,8 +43,9 @@ static void note(const char* what, cudaError_t e) {
     } while (0)
 
 constexpr uint32_t kMagic = 0x50534732u;  // "PSG2"
-constexpr int kPhases = 8;  // timing events
-enum Phase { PH_SORT = 0, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END, PH_BEGIN, PH_CLOSURE };
+constexpr int kPhases = 9;  // timing events
+enum Phase { PH_SORT = 0, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END, PH_BEGIN, PH_CLOSURE,
+             PH_DENSE };
 
 struct Mirror {
     float *x, *y, *z, *m, *fx, *fy, *fz;
@@ -70,6 +71,8 @@ struct ClosureState {
     uint32_t tick;       // ticks run in closure mode (varies the judge sample)
     JudgeOut last;       // judge result of the last tick (samples 0: none)
     int valid;           // the last completed tick ran the order-1 traversal
+    cudaStream_t side;   // the judge's direct sum, beside the tree and traversal
+    cudaEvent_t ev_sorted, ev_judge;
 };
 
 struct State {
@@ -94,6 +97,10 @@ struct State {
     P2PStore p2p;
     uint4* dense_rec;      // full-leaf P2P work records
     uint32_t dense_cap;
+    uint32_t* heavy_frontier;
+    uint32_t heavy_fcap;
+    int heavy_slots;       // blocks of k_heavy_leaf
+    int heavy_depth;       // option; < 0: derived from theta
     int kahan;
     Status* d_status;
     Status* h_status;
@@ -194,7 +201,7 @@ static void free_state(State* s) {
                   s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
                   s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->tv.link,
                   s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.mask, s->p2p.next, s->p2p.cnt,
-                  s->d_status, s->dense_rec, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
+                  s->d_status, s->dense_rec, s->heavy_frontier, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
                   s->tk_vmir[0], s->tk_vmir[1], s->tk_vmir[2], s->cl.lg0, s->cl.lg1,
                   s->cl.leaf_of, s->cl.dF, s->cl.params, s->cl.packed, s->cl.judge_tg,
                   s->cl.judge_f64, s->cl.d_judge};
@@ -202,6 +209,10 @@ static void free_state(State* s) {
         if (p) cudaFree(p);
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->cl.h_judge) cudaFreeHost(s->cl.h_judge);
+    if (s->cl.side) cudaStreamSynchronize(s->cl.side);
+    if (s->cl.ev_sorted) cudaEventDestroy(s->cl.ev_sorted);
+    if (s->cl.ev_judge) cudaEventDestroy(s->cl.ev_judge);
+    if (s->cl.side) cudaStreamDestroy(s->cl.side);
     free_mirror(s->mir);
     for (int i = 0; i < kPhases; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
@@ -264,9 +275,14 @@ static int init_state(State* s, size_t maxp, float theta) {
     if (r != PSG_OK) return r;
     r = alloc_p2p(s, (uint32_t)(n < 4096 ? 4096 : n / 4));
     if (r != PSG_OK) return r;
-    // a full leaf holds >= 8 particles, so n / 8 records always suffice
-    r = alloc_dense(s, (uint32_t)(n / 8 + 1024));
+    r = alloc_dense(s, (uint32_t)(n / 4 + 1024));
     if (r != PSG_OK) return r;
+    // shallow leaves: a frontier holds at most one level's nodes plus the
+    // parent's near list
+    s->heavy_slots = 32;
+    s->heavy_fcap = (uint32_t)(2 * n + 1024);
+    PSG_ALLOC(s->heavy_frontier, (size_t)s->heavy_slots * 2 * s->heavy_fcap * 4);
+    s->heavy_depth = -1;
     for (int o = 0; o < 2; ++o) {
         int bps = 0;
         for (int dn = 0; dn < 2; ++dn) {
@@ -298,7 +314,21 @@ static int closure_alloc(State* s) {
     PSG_ALLOC(c.d_judge, sizeof(JudgeOut));
     PSG_CHECK(cudaMallocHost((void**)&c.h_judge, sizeof(JudgeOut)));
     std::memset(c.h_judge, 0, sizeof(JudgeOut));
+    PSG_CHECK(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    PSG_CHECK(cudaEventCreateWithFlags(&c.ev_sorted, cudaEventDisableTiming));
+    PSG_CHECK(cudaEventCreateWithFlags(&c.ev_judge, cudaEventDisableTiming));
     return PSG_OK;
+}
+
+// Leaves at most this deep are walked block-parallel by k_heavy_leaf: a leaf
+// at depth d (half width H / 2^d of the root's H) stays unseparated from the
+// sources within about theta H / 2^(d-1), a large part of the tree once
+// 2^d <= 4 theta.
+static int heavy_depth_for(const State* s) {
+    if (s->heavy_depth >= 0) return s->heavy_depth > 5 ? 5 : s->heavy_depth;
+    int d = 0;
+    while (d < 5 && (float)(2 << d) <= 4.0f * s->theta) ++d;
+    return d < 2 ? 2 : d;
 }
 
 static void record(State* s, int ph) {
@@ -316,6 +346,7 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
                                   s->stream));
         PSG_CHECK(cudaMemsetAsync(&s->d_status->p2p_chunks, 0, 4, s->stream));
         PSG_CHECK(cudaMemsetAsync(&s->d_status->dense_count, 0, 8, s->stream));
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->heavy_work, 0, 4, s->stream));
         TravArgs A;
         A.tv = s->tv;
         A.p2p = s->p2p;
@@ -337,10 +368,17 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
         A.tv.lg1 = o ? s->cl.lg1 : nullptr;
         A.dense_rec = s->dense_rec;
         A.dense_cap = s->dense_cap;
+        A.heavy_depth = heavy_depth_for(s);
+        A.heavy_frontier = s->heavy_frontier;
+        A.heavy_fcap = s->heavy_fcap;
         for (int k = 2; k <= kMaxDepth; ++k)
             launch_traverse_internal(A, k, s->trav_int_grid[o], s->stream);
         record(s, PH_TRAV);
+        // the leaf pass starts at the groups of depth heavy_depth
+        launch_leaf_start(s->d_status, A.heavy_depth, s->stream);
         launch_traverse_leaves(A, s->trav_grid[o], s->stream);
+        launch_heavy_leaf(A, s->heavy_slots, s->stream);
+        record(s, PH_DENSE);
         launch_dense_p2p(A, s->sms * 8, s->stream);
         record(s, PH_END);
         PSG_CHECK(cudaGetLastError());
@@ -354,7 +392,7 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
         }
         if (err & PSG_ERR_NS_OVERFLOW) {
             unsigned long long need = s->h_status->ns_used[0];
-            need = need + need / 4 + 1024;
+            need = 2 * need + 1024;
             if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
             int r = alloc_ns(s, need);
             if (r != PSG_OK) return r;
@@ -368,7 +406,7 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
         }
         if (err & PSG_ERR_P2P_OVERFLOW) {
             unsigned long long need = s->h_status->p2p_chunks;
-            need = need + need / 4 + 1024;
+            need = 2 * need + 1024;
             if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
             int r = alloc_p2p(s, (uint32_t)need);
             if (r != PSG_OK) return r;
@@ -448,6 +486,19 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
     launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
     record(s, PH_GATHER);
+    // closure judge: its FP64 direct sum needs only the sorted particles, so
+    // it runs on a side stream under the tree build and traversal, on a
+    // quarter of the GPU's block slots
+    ClosureState& cj = s->cl;
+    const bool judge = s->order >= 1 && n > 1 && ((cj.mode == 2 && cj.have_weights) || cj.judge);
+    const int smp = n < (size_t)kJudgeSamples ? (int)n : kJudgeSamples;
+    if (judge) {
+        PSG_CHECK(cudaEventRecord(cj.ev_sorted, st));
+        PSG_CHECK(cudaStreamWaitEvent(cj.side, cj.ev_sorted, 0));
+        launch_judge_direct(s->xyzm, n, cj.judge_tg, smp, cj.judge_f64, cj.tick, s->sms * 2,
+                            cj.side);
+        PSG_CHECK(cudaEventRecord(cj.ev_judge, cj.side));
+    }
     const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
     if (s->debug) {
         PSG_CHECK(cudaMemsetAsync(s->tv.dbg_m2l, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
@@ -466,6 +517,7 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
         PSG_CHECK(cudaMemsetAsync(d.fy, 0, 4, st));
         PSG_CHECK(cudaMemsetAsync(d.fz, 0, 4, st));
         record(s, PH_TRAV);
+        record(s, PH_DENSE);
         record(s, PH_END);
         PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
                                   cudaMemcpyDeviceToHost, st));
@@ -473,23 +525,26 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
         err = s->h_status->err;
     } else {
         int r = run_traversal(s, s->xyzm, d.fx, d.fy, d.fz, &err);
-        if (r != PSG_OK) return r;
+        if (r != PSG_OK) {
+            if (judge) cudaStreamSynchronize(cj.side);  // leave no judge work running
+            return r;
+        }
     }
-    if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK)) {
-        std::snprintf(g_err, sizeof(g_err), "device status error 0x%x", err);
-        return PSG_EDEVICE;
-    }
-    if (err & PSG_ERR_NODES) {
-        std::snprintf(g_err, sizeof(g_err), "morton codes not sorted/30-bit (0x%x)", err);
-        return PSG_EINVAL;
+    if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_HEAVY_OVERFLOW)) {
+        if (judge) cudaStreamSynchronize(cj.side);
+        const bool nodes = (err & PSG_ERR_NODES) &&
+                           !(err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_HEAVY_OVERFLOW));
+        std::snprintf(g_err, sizeof(g_err), nodes ? "morton codes not sorted/30-bit (0x%x)"
+                                                  : "device status error 0x%x", err);
+        return nodes ? PSG_EINVAL : PSG_EDEVICE;
     }
     s->cl.last.samples = 0;
     s->cl.valid = s->order >= 1 && n > 1;
-    if (s->order >= 1 && n > 1) {
-        // learned closure: MLP correction, sampled FP64 judge, fallback
+    if (judge) {
+        // learned closure: MLP correction, the judge's decision, fallback
         ClosureState& c = s->cl;
         const bool mlp = c.mode == 2 && c.have_weights;
-        if (mlp || c.judge) {
+        {
             TreeView tv = s->tv;
             tv.lg0 = c.lg0;
             tv.lg1 = c.lg1;
@@ -498,9 +553,9 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
             } else {
                 PSG_CHECK(cudaMemsetAsync(c.dF, 0, n * sizeof(float4), st));
             }
-            const int smp = n < (size_t)kJudgeSamples ? (int)n : kJudgeSamples;
-            launch_judge(s->xyzm, n, c.judge_tg, smp, c.judge_f64, d.fx, d.fy, d.fz, c.dF,
-                         mlp ? 1 : 0, c.tick, c.d_judge, s->sms, st);
+            PSG_CHECK(cudaStreamWaitEvent(st, c.ev_judge, 0));
+            launch_judge_decide(c.judge_tg, smp, c.judge_f64, d.fx, d.fy, d.fz, c.dF,
+                                mlp ? 1 : 0, c.d_judge, st);
             if (mlp) launch_closure_apply(d.fx, d.fy, d.fz, c.dF, n, c.d_judge, s->sms, st);
             PSG_CHECK(cudaGetLastError());
             PSG_CHECK(cudaMemcpyAsync(c.h_judge, c.d_judge, sizeof(JudgeOut),
@@ -528,11 +583,12 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     s->stats[13] = s->h_status->dense_count;
     if (s->timing) {
         cudaEventSynchronize(s->ev[PH_CLOSURE]);
-        const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_END};
+        const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_DENSE};
         for (int i = 0; i + 1 < 7; ++i)
             cudaEventElapsedTime(&s->ms[i], s->ev[order[i]], s->ev[order[i + 1]]);
         cudaEventElapsedTime(&s->ms[6], s->ev[PH_BEGIN], s->ev[PH_CLOSURE]);
         cudaEventElapsedTime(&s->ms[7], s->ev[PH_END], s->ev[PH_CLOSURE]);
+        cudaEventElapsedTime(&s->ms[8], s->ev[PH_DENSE], s->ev[PH_END]);
     }
     return PSG_OK;
 }
@@ -752,6 +808,10 @@ int psg_set_option(void* mem, int key, double value) {
             return PSG_OK;
         }
         case PSG_OPT_JUDGE: s->cl.judge = value != 0.0; return PSG_OK;
+        case PSG_OPT_HEAVY_DEPTH:
+            if (value > 5) return PSG_EINVAL;
+            s->heavy_depth = value < 0 ? -1 : (int)value;
+            return PSG_OK;
         default: return PSG_EINVAL;
     }
 }
@@ -852,7 +912,7 @@ int psg_direct_f64(void* mem, const psg_arrays_t* a, const uint32_t* targets, si
         PSG_CHECK(cudaMemcpyAsync(dt, targets, n_t * 4, cudaMemcpyHostToDevice, st));
     }
     if (ho) PSG_ALLOC(dout, n_t * 3 * sizeof(double));
-    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, s->sms, st);
+    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, s->sms * 8, st);
     PSG_CHECK(cudaGetLastError());
     if (ho) PSG_CHECK(cudaMemcpyAsync(out, dout, n_t * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     PSG_CHECK(cudaStreamSynchronize(st));
