@@ -285,6 +285,7 @@ class Context:
                 "traversal_runs": int(out[11]), "max_leaf": int(out[12]),
                 "dense_records": int(out[13]),
                 "lanes": int(out[16]), "leaf_groups": int(out[17]), "dfs_steps": int(out[18]),
+                "full_leaf_interactions": int(out[20]),
                 "slowest_group_cycles": int(out[19]) >> 28,
                 "slowest_group_node": int(out[19]) & 0xFFFFFFF}
 

@@ -891,7 +891,10 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
     }
     if (DEBUG) {
         inter = warp_sum(inter);
-        if (lane == 0 && inter) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+        if (lane == 0 && inter) {
+            atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+            atomicAdd(&status->stat[PSG_STAT_DENSE_INTER], inter);
+        }
     }
 }
 

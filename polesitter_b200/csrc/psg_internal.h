@@ -43,6 +43,7 @@ extern "C" {
 #define PSG_STAT_GROUPS 9       /* groups processed (leaf mode) */
 #define PSG_STAT_DFS_STEPS 10
 #define PSG_STAT_SLOWEST_GROUP 11 /* leaf pass: (clock cycles << 28) | node of the slowest group */
+#define PSG_STAT_DENSE_INTER 12   /* particle pairs summed by the full-leaf kernel */
 
 /* Morton quantisation variants of polesitter.h:2013-2157 */
 #define PSG_MORTON_AVX2 0
