@@ -95,6 +95,9 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-curve", action="store_true")
+    ap.add_argument("--minimal", action="store_true",
+                    help="only the timed ticks (for profiling runs): no plain curve, no plain "
+                         "C2 line, one e2e step, no CPU baseline")
     return ap.parse_args()
 
 
@@ -423,7 +426,7 @@ def run_b200(args):
         line["equal_error"] = plain_curve(ctx, P, d, pristine, codes, flush, n, value,
                                           accuracy["judge"]["max_of_tick_medians"])
     ctx.destroy()
-    if closure and rank == 0:
+    if closure and rank == 0 and not args.minimal:
         line["plain_c2"] = plain_c2(P, torch, dev, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference_ticks(p0, ticks=1 if closure else 3, warmup=1,
@@ -507,6 +510,9 @@ def plain_c2(P, torch, dev, flush):
 
 def main():
     args = parse_args()
+    if args.minimal:
+        args.no_plain_curve = args.no_cpu_baseline = True
+        args.e2e_steps = 1
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -100,6 +100,8 @@ struct State {
     uint32_t* heavy_frontier;
     uint32_t heavy_fcap;
     int heavy_slots;       // blocks of k_heavy_leaf
+    cudaStream_t aux;      // k_heavy_leaf, beside the leaf pass
+    cudaEvent_t ev_levels, ev_heavy;
     int heavy_depth;       // option; < 0: derived from theta
     int kahan;
     Status* d_status;
@@ -156,6 +158,15 @@ static int alloc_dense(State* s, uint32_t cap) {
     s->dense_rec = nullptr;
     PSG_ALLOC(s->dense_rec, (size_t)cap * sizeof(uint4));
     s->dense_cap = cap;
+    return PSG_OK;
+}
+
+// frontier buffers of k_heavy_leaf: 2 x cap candidates per block
+static int alloc_heavy(State* s, uint32_t cap) {
+    if (s->heavy_frontier) cudaFree(s->heavy_frontier);
+    s->heavy_frontier = nullptr;
+    PSG_ALLOC(s->heavy_frontier, (size_t)s->heavy_slots * 2 * cap * 4);
+    s->heavy_fcap = cap;
     return PSG_OK;
 }
 
@@ -216,6 +227,12 @@ static void free_state(State* s) {
     free_mirror(s->mir);
     for (int i = 0; i < kPhases; ++i)
         if (s->ev[i]) cudaEventDestroy(s->ev[i]);
+    if (s->aux) {
+        cudaStreamSynchronize(s->aux);
+        cudaStreamDestroy(s->aux);
+    }
+    if (s->ev_levels) cudaEventDestroy(s->ev_levels);
+    if (s->ev_heavy) cudaEventDestroy(s->ev_heavy);
     if (s->stream) cudaStreamDestroy(s->stream);
     s->magic = 0;
 }
@@ -279,10 +296,13 @@ static int init_state(State* s, size_t maxp, float theta) {
     if (r != PSG_OK) return r;
     // shallow leaves: a frontier holds at most one level's nodes plus the
     // parent's near list
-    s->heavy_slots = 32;
-    s->heavy_fcap = (uint32_t)(2 * n + 1024);
-    PSG_ALLOC(s->heavy_frontier, (size_t)s->heavy_slots * 2 * s->heavy_fcap * 4);
+    s->heavy_slots = 64;
+    r = alloc_heavy(s, (uint32_t)(n / 4 + 4096));
+    if (r != PSG_OK) return r;
     s->heavy_depth = -1;
+    PSG_CHECK(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+    PSG_CHECK(cudaEventCreateWithFlags(&s->ev_levels, cudaEventDisableTiming));
+    PSG_CHECK(cudaEventCreateWithFlags(&s->ev_heavy, cudaEventDisableTiming));
     for (int o = 0; o < 2; ++o) {
         int bps = 0;
         for (int dn = 0; dn < 2; ++dn) {
@@ -374,19 +394,25 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
         for (int k = 2; k <= kMaxDepth; ++k)
             launch_traverse_internal(A, k, s->trav_int_grid[o], s->stream);
         record(s, PH_TRAV);
-        // the leaf pass starts at the groups of depth heavy_depth
+        // shallow leaves on the aux stream, beside the leaf pass; the leaf
+        // pass starts at the groups of depth heavy_depth
+        PSG_CHECK(cudaEventRecord(s->ev_levels, s->stream));
+        PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
+        launch_heavy_leaf(A, s->heavy_slots, s->aux);
+        PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
         launch_leaf_start(s->d_status, A.heavy_depth, s->stream);
         launch_traverse_leaves(A, s->trav_grid[o], s->stream);
-        launch_heavy_leaf(A, s->heavy_slots, s->stream);
         record(s, PH_DENSE);
         launch_dense_p2p(A, s->sms * 8, s->stream);
+        PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
         record(s, PH_END);
         PSG_CHECK(cudaGetLastError());
         PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
                                   cudaMemcpyDeviceToHost, s->stream));
         PSG_CHECK(cudaStreamSynchronize(s->stream));
         const uint32_t err = s->h_status->err;
-        if (!(err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW | PSG_ERR_DENSE_OVERFLOW))) {
+        if (!(err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW | PSG_ERR_DENSE_OVERFLOW |
+                     PSG_ERR_HEAVY_OVERFLOW))) {
             *err_out = err;
             return PSG_OK;
         }
@@ -395,6 +421,12 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
             need = 2 * need + 1024;
             if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
             int r = alloc_ns(s, need);
+            if (r != PSG_OK) return r;
+        }
+        if (err & PSG_ERR_HEAVY_OVERFLOW) {
+            unsigned long long cap = 2ull * s->heavy_fcap;
+            const unsigned long long most = 2ull * s->max_particles + 1024;
+            int r = alloc_heavy(s, (uint32_t)(cap < most ? cap : most));
             if (r != PSG_OK) return r;
         }
         if (err & PSG_ERR_DENSE_OVERFLOW) {
