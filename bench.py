@@ -76,8 +76,15 @@ WORKLOADS = {
 # judge (sample, FP64 direct sum, decision), the MLP and the apply kernel
 KERNELS_PER_TICK = {"plain": 39, "closure": 44}
 # DRAM bytes (read + write) of one leaf-pass launch, from the ncu captures
-# summarised under profiles/
-LEAF_PASS_DRAM_BYTES = {"plain": 254.3e6, "closure": None}
+# summarised under profiles/: the plain one at this size; the closure one
+# captured at N=131072 and scaled by the M2L pair count (x 8.43) to N=1M
+LEAF_PASS_DRAM_BYTES = {"plain": 255.3e6, "closure": 1.64e9}
+TRAFFIC_NOTE = {
+    "plain": "dram read+write bytes per launch, ncu capture of this workload "
+             "(profiles/traversal_leaf_plummer1m.md)",
+    "closure": "dram read+write bytes per launch, ncu capture of the same kernel at N=131072 "
+               "(194.1 MB) scaled by the M2L pair count to N=1M "
+               "(profiles/traversal_leaf_closure_clumpy131k.md)"}
 FLOP_M2L = 35         # per M2L pair: polesitter.h:1065-1092
 FLOP_M2L_ORDER1 = 59  # ... plus the monopole field gradient (closure order 1)
 FLOP_P2P = 20         # per particle pair: polesitter.h:1424-1444
@@ -397,8 +404,7 @@ def run_b200(args):
                                f"{peaks.get('sm_max_mhz', 1965.0)} MHz (sm_max_mhz, {peak_src}); "
                                "no measured FP32 peak exists",
                 "traffic": LEAF_PASS_DRAM_BYTES[args.workload],
-                "traffic_note": "dram read+write bytes per launch from the ncu summaries under "
-                                "profiles/ (null: not captured at this size)",
+                "traffic_note": TRAFFIC_NOTE[args.workload],
                 "algorithmic_flop": flops_leaf,
                 "counts": {"m2l_pairs_leaf_targets": m2l_leaf,
                            "p2p_particle_pairs": p2p_inter - p2p_full,
