@@ -153,6 +153,42 @@ ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float
                                   float* params, uint32_t epochs, uint32_t batch, float lr,
                                   uint64_t seed, float* loss_out);
 
+/* ---- batched ensemble (no counterpart in the reference) ----------------
+ *
+ * Many independent systems advanced together: each keeps its own context,
+ * and one tick of all of them is two CUDA graphs captured once and replayed
+ * (forces: a branch per system -- ids reset, prepare, sort, tree, upward,
+ * traversal; step: each system's velocity permutation + semi-implicit Euler,
+ * as in ps_b200_run_ticks).  The systems' particles are one concatenated set
+ * of DEVICE arrays: system k holds counts[k] particles from the sum of the
+ * counts before it, its ids are local (0 .. counts[k]-1) and, like its
+ * positions, come back sorted within its range.  Results equal running each
+ * system through ps_b200_run_ticks with its own theta. */
+typedef struct ps_b200_ensemble ps_b200_ensemble_t;
+
+/* theta per system (NULL: 2.0 for all) */
+ps_result_t ps_b200_ensemble_create(ps_b200_ensemble_t** out, const size_t* counts,
+                                    size_t n_systems, const float* theta);
+
+/* The autotuner, on copies of the given state (arrs and the codes array are
+ * not changed): per size class (systems with equal floor(log2 N)), the
+ * smallest theta of {1, 1.5, 2, 3, 4, 6, 8} whose median relative force
+ * error against an FP64 direct sum (1024 sampled particles of the class's
+ * first system) is at most target_median_error; then the traversal grids'
+ * scale among {1, 1/2, 1/4} of one system's persistent grids, by the time of
+ * one forces replay of the whole ensemble.  theta_out (n_systems) and
+ * grid_scale_out receive the choice (either may be NULL). */
+ps_result_t ps_b200_ensemble_autotune(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
+                                      uint32_t* morton_codes, float target_median_error,
+                                      float* theta_out, double* grid_scale_out);
+
+/* `ticks` ensemble ticks; vx, vy, vz are concatenated device arrays too */
+ps_result_t ps_b200_ensemble_run(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
+                                 uint32_t* morton_codes, float* vx, float* vy, float* vz,
+                                 float dt, uint32_t ticks);
+ps_result_t ps_b200_ensemble_theta(ps_b200_ensemble_t* ens, float* theta_out, size_t n);
+ps_result_t ps_b200_ensemble_destroy(ps_b200_ensemble_t* ens);
+
 /* message of the last CUDA-side failure on this thread */
 const char* ps_b200_last_error(void);
 

@@ -35,7 +35,8 @@ EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
             "ps_b200_prepare_particles_noalloc", "ps_b200_run_ticks",
             "ps_b200_closure_set_weights", "ps_b200_closure_last", "ps_b200_closure_features",
             "ps_b200_closure_correction", "ps_b200_closure_forward", "ps_b200_closure_grad",
-            "ps_b200_closure_train")
+            "ps_b200_closure_train", "ps_b200_ensemble_create", "ps_b200_ensemble_autotune",
+            "ps_b200_ensemble_run", "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy")
 
 
 class ParticleArrs(C.Structure):
@@ -111,7 +112,17 @@ def lib() -> C.CDLL:
                                         C.c_uint64, vp]
     for name in ("ps_b200_closure_set_weights", "ps_b200_closure_last", "ps_b200_closure_features",
                  "ps_b200_closure_correction", "ps_b200_closure_forward", "ps_b200_closure_grad",
-                 "ps_b200_closure_train"):
+                 "ps_b200_closure_train", "ps_b200_ensemble_create", "ps_b200_ensemble_autotune",
+            "ps_b200_ensemble_run", "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy"):
+        getattr(L, name).restype = C.c_int
+    L.ps_b200_ensemble_create.argtypes = [C.POINTER(vp), vp, sz, vp]
+    L.ps_b200_ensemble_autotune.argtypes = [vp, C.POINTER(ParticleArrs), vp, f32, vp, vp]
+    L.ps_b200_ensemble_run.argtypes = [vp, C.POINTER(ParticleArrs), vp, vp, vp, vp, f32,
+                                       C.c_uint32]
+    L.ps_b200_ensemble_theta.argtypes = [vp, vp, sz]
+    L.ps_b200_ensemble_destroy.argtypes = [vp]
+    for name in ("ps_b200_ensemble_create", "ps_b200_ensemble_autotune", "ps_b200_ensemble_run",
+                 "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy"):
         getattr(L, name).restype = C.c_int
     L.ps_b200_run_ticks.restype = C.c_int
     L.ps_b200_run_ticks.argtypes = [vp, C.POINTER(ParticleArrs), vp, vp, vp, vp, f32, C.c_uint32]
@@ -340,3 +351,51 @@ class Context:
                 lib().ps_destroy(self.ptr)
         except Exception:
             pass
+
+
+class Ensemble:
+    """Many independent systems advanced together (ps_b200_ensemble_*): one
+    context per system, each tick two replayed CUDA graphs.  Arrays are
+    concatenated device arrays (torch CUDA tensors), system k at offsets
+    sum(counts[:k])."""
+
+    def __init__(self, counts, theta=None):
+        import numpy as np
+        self.counts = np.ascontiguousarray(counts, np.uint64)
+        th = None if theta is None else np.ascontiguousarray(theta, np.float32)
+        self.ptr = C.c_void_p()
+        _check("ps_b200_ensemble_create", lib().ps_b200_ensemble_create(
+            C.byref(self.ptr), self.counts.ctypes.data, len(self.counts),
+            None if th is None else th.ctypes.data))
+
+    def autotune(self, p, codes, target: float):
+        import numpy as np
+        th = np.zeros(len(self.counts), np.float32)
+        gs = C.c_double()
+        arrs = arrs_of(p)
+        _check("ps_b200_ensemble_autotune", lib().ps_b200_ensemble_autotune(
+            self.ptr, C.byref(arrs), _addr(codes), target, th.ctypes.data, C.byref(gs)))
+        return th, gs.value
+
+    def run(self, p, codes, vx, vy, vz, dt: float, ticks: int):
+        arrs = arrs_of(p)
+        _check("ps_b200_ensemble_run", lib().ps_b200_ensemble_run(
+            self.ptr, C.byref(arrs), _addr(codes), _addr(vx), _addr(vy), _addr(vz), dt, ticks))
+
+    def theta(self):
+        import numpy as np
+        th = np.zeros(len(self.counts), np.float32)
+        _check("ps_b200_ensemble_theta", lib().ps_b200_ensemble_theta(
+            self.ptr, th.ctypes.data, len(th)))
+        return th
+
+    def destroy(self):
+        if self.ptr:
+            _check("ps_b200_ensemble_destroy", lib().ps_b200_ensemble_destroy(self.ptr))
+            self.ptr = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()

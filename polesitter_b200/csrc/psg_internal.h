@@ -94,6 +94,14 @@ int psg_direct_f64(void* state, const psg_arrays_t* a, const uint32_t* targets, 
 /* the caller's tick loop on the device (k_tick.cu) */
 int psg_run_ticks(void* state, const psg_arrays_t* a, float* vx, float* vy, float* vz, float dt,
                   uint32_t ticks, int morton_variant);
+/* batched ensemble of independent systems (CUDA graphs; psg_runtime.cu) */
+int psg_ensemble_create(void** out, const size_t* counts, size_t n_systems, const float* theta);
+int psg_ensemble_destroy(void* ens);
+int psg_ensemble_run(void* ens, const psg_arrays_t* a, float* vx, float* vy, float* vz, float dt,
+                     uint32_t ticks);
+int psg_ensemble_autotune(void* ens, const psg_arrays_t* a, float target, float* theta_out,
+                          double* grid_scale_out);
+int psg_ensemble_systems(void* ens, float* theta_out, size_t n);
 const char* psg_last_error(void);
 void psg_set_error(const char* msg);
 

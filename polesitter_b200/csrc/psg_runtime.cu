@@ -9,8 +9,11 @@
 // ps_destroy; it replaces the reference's arena + radix temporaries.
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "psg_closure.cuh"
 #include "psg_common.cuh"
@@ -103,6 +106,7 @@ struct State {
     cudaStream_t aux;      // k_heavy_leaf, beside the leaf pass
     cudaEvent_t ev_levels, ev_heavy;
     int heavy_depth;       // option; < 0: derived from theta
+    double grid_scale;     // traversal grids x this (ensemble autotuner); 0: 1
     int kahan;
     Status* d_status;
     Status* h_status;
@@ -355,57 +359,104 @@ static void record(State* s, int ph) {
     if (s->timing) cudaEventRecord(s->ev[ph], s->stream);
 }
 
+// one traversal run (internal levels, leaf pass, shallow leaves, full
+// leaves) enqueued on s->stream; no host synchronisation
+static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy, float* fz) {
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->work[0], 0, sizeof(s->d_status->work), s->stream));
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->ns_used[0], 0, sizeof(s->d_status->ns_used),
+                              s->stream));
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->p2p_chunks, 0, 4, s->stream));
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->dense_count, 0, 8, s->stream));
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->heavy_work, 0, 4, s->stream));
+    TravArgs A;
+    A.tv = s->tv;
+    A.p2p = s->p2p;
+    A.ns = s->ns;
+    A.ns_cap = s->ns_cap;
+    A.status = s->d_status;
+    A.theta = s->theta;
+    A.level = 0;
+    A.debug = s->debug;
+    A.kahan = s->kahan;
+    A.xyzm = xyzm;
+    A.fx = fx;
+    A.fy = fy;
+    A.fz = fz;
+    const int o = s->order >= 1 ? 1 : 0;
+    A.order = o;
+    A.leaf_of = o ? s->cl.leaf_of : nullptr;
+    A.tv.lg0 = o ? s->cl.lg0 : nullptr;
+    A.tv.lg1 = o ? s->cl.lg1 : nullptr;
+    A.dense_rec = s->dense_rec;
+    A.dense_cap = s->dense_cap;
+    A.heavy_depth = heavy_depth_for(s);
+    A.heavy_frontier = s->heavy_frontier;
+    A.heavy_fcap = s->heavy_fcap;
+    const double gs = s->grid_scale > 0.0 ? s->grid_scale : 1.0;
+    auto scaled = [&](int g) {
+        const int v = (int)(g * gs);
+        return v < 1 ? 1 : v;
+    };
+    for (int k = 2; k <= kMaxDepth; ++k)
+        launch_traverse_internal(A, k, scaled(s->trav_int_grid[o]), s->stream);
+    record(s, PH_TRAV);
+    // shallow leaves on the aux stream, beside the leaf pass; the leaf
+    // pass starts at the groups of depth heavy_depth
+    PSG_CHECK(cudaEventRecord(s->ev_levels, s->stream));
+    PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
+    launch_heavy_leaf(A, scaled(s->heavy_slots), s->aux);
+    PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
+    launch_leaf_start(s->d_status, A.heavy_depth, s->stream);
+    const int lg[2] = {scaled(s->trav_grid[o][0]), scaled(s->trav_grid[o][1])};
+    launch_traverse_leaves(A, lg, s->stream);
+    record(s, PH_DENSE);
+    launch_dense_p2p(A, scaled(s->sms * 8), s->stream);
+    PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
+    record(s, PH_END);
+    return PSG_OK;
+}
+
+// grows every store whose capacity bit is set in err (x2 of what the run
+// asked for), after a traversal run read back its status
+static int regrow(State* s, uint32_t err) {
+    if (err & PSG_ERR_NS_OVERFLOW) {
+        unsigned long long need = s->h_status->ns_used[0];
+        need = 2 * need + 1024;
+        if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
+        int r = alloc_ns(s, need);
+        if (r != PSG_OK) return r;
+    }
+    if (err & PSG_ERR_HEAVY_OVERFLOW) {
+        unsigned long long cap = 2ull * s->heavy_fcap;
+        const unsigned long long most = 2ull * s->max_particles + 1024;
+        int r = alloc_heavy(s, (uint32_t)(cap < most ? cap : most));
+        if (r != PSG_OK) return r;
+    }
+    if (err & PSG_ERR_DENSE_OVERFLOW) {
+        unsigned long long need = s->h_status->dense_count;
+        need = need + need / 4 + 1024;
+        if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
+        int r = alloc_dense(s, (uint32_t)need);
+        if (r != PSG_OK) return r;
+    }
+    if (err & PSG_ERR_P2P_OVERFLOW) {
+        unsigned long long need = s->h_status->p2p_chunks;
+        need = 2 * need + 1024;
+        if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
+        int r = alloc_p2p(s, (uint32_t)need);
+        if (r != PSG_OK) return r;
+    }
+    return PSG_OK;
+}
+
 // traversal of all levels + P2P/L2P; regrows the near-list regions or the
 // P2P chunk store and reruns when a capacity flag comes back
 static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, float* fz,
                          uint32_t* err_out) {
     for (int attempt = 0; attempt < 6; ++attempt) {
         s->attempts = attempt + 1;
-        PSG_CHECK(cudaMemsetAsync(&s->d_status->work[0], 0, sizeof(s->d_status->work), s->stream));
-        PSG_CHECK(cudaMemsetAsync(&s->d_status->ns_used[0], 0, sizeof(s->d_status->ns_used),
-                                  s->stream));
-        PSG_CHECK(cudaMemsetAsync(&s->d_status->p2p_chunks, 0, 4, s->stream));
-        PSG_CHECK(cudaMemsetAsync(&s->d_status->dense_count, 0, 8, s->stream));
-        PSG_CHECK(cudaMemsetAsync(&s->d_status->heavy_work, 0, 4, s->stream));
-        TravArgs A;
-        A.tv = s->tv;
-        A.p2p = s->p2p;
-        A.ns = s->ns;
-        A.ns_cap = s->ns_cap;
-        A.status = s->d_status;
-        A.theta = s->theta;
-        A.level = 0;
-        A.debug = s->debug;
-        A.kahan = s->kahan;
-        A.xyzm = xyzm;
-        A.fx = fx;
-        A.fy = fy;
-        A.fz = fz;
-        const int o = s->order >= 1 ? 1 : 0;
-        A.order = o;
-        A.leaf_of = o ? s->cl.leaf_of : nullptr;
-        A.tv.lg0 = o ? s->cl.lg0 : nullptr;
-        A.tv.lg1 = o ? s->cl.lg1 : nullptr;
-        A.dense_rec = s->dense_rec;
-        A.dense_cap = s->dense_cap;
-        A.heavy_depth = heavy_depth_for(s);
-        A.heavy_frontier = s->heavy_frontier;
-        A.heavy_fcap = s->heavy_fcap;
-        for (int k = 2; k <= kMaxDepth; ++k)
-            launch_traverse_internal(A, k, s->trav_int_grid[o], s->stream);
-        record(s, PH_TRAV);
-        // shallow leaves on the aux stream, beside the leaf pass; the leaf
-        // pass starts at the groups of depth heavy_depth
-        PSG_CHECK(cudaEventRecord(s->ev_levels, s->stream));
-        PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
-        launch_heavy_leaf(A, s->heavy_slots, s->aux);
-        PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
-        launch_leaf_start(s->d_status, A.heavy_depth, s->stream);
-        launch_traverse_leaves(A, s->trav_grid[o], s->stream);
-        record(s, PH_DENSE);
-        launch_dense_p2p(A, s->sms * 8, s->stream);
-        PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
-        record(s, PH_END);
+        int r0 = enqueue_traversal(s, xyzm, fx, fy, fz);
+        if (r0 != PSG_OK) return r0;
         PSG_CHECK(cudaGetLastError());
         PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status),
                                   cudaMemcpyDeviceToHost, s->stream));
@@ -416,33 +467,8 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
             *err_out = err;
             return PSG_OK;
         }
-        if (err & PSG_ERR_NS_OVERFLOW) {
-            unsigned long long need = s->h_status->ns_used[0];
-            need = 2 * need + 1024;
-            if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
-            int r = alloc_ns(s, need);
-            if (r != PSG_OK) return r;
-        }
-        if (err & PSG_ERR_HEAVY_OVERFLOW) {
-            unsigned long long cap = 2ull * s->heavy_fcap;
-            const unsigned long long most = 2ull * s->max_particles + 1024;
-            int r = alloc_heavy(s, (uint32_t)(cap < most ? cap : most));
-            if (r != PSG_OK) return r;
-        }
-        if (err & PSG_ERR_DENSE_OVERFLOW) {
-            unsigned long long need = s->h_status->dense_count;
-            need = need + need / 4 + 1024;
-            if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
-            int r = alloc_dense(s, (uint32_t)need);
-            if (r != PSG_OK) return r;
-        }
-        if (err & PSG_ERR_P2P_OVERFLOW) {
-            unsigned long long need = s->h_status->p2p_chunks;
-            need = 2 * need + 1024;
-            if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
-            int r = alloc_p2p(s, (uint32_t)need);
-            if (r != PSG_OK) return r;
-        }
+        int rg = regrow(s, err);
+        if (rg != PSG_OK) return rg;
         PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, s->stream));
         PSG_CHECK(cudaMemsetAsync(&s->d_status->stat[0], 0, sizeof(s->d_status->stat), s->stream));
         if (s->timing) cudaEventRecord(s->ev[PH_UP], s->stream);
@@ -773,9 +799,420 @@ static int prepare(const psg_arrays_t* a, float* out_min, float* out_max, float*
     return PSG_OK;
 }
 
+// ---- batched ensemble: many independent systems per tick in CUDA graphs ----
+//
+// Every system keeps its own context (tree, stores, streams).  One tick of
+// all systems is two CUDA graphs captured once and replayed: the forces
+// graph forks one branch per system (ids reset, prepare with the root taken
+// on the device, sort, tree, upward, traversal, status copy) and joins them;
+// the step graph does each system's velocity permutation + Euler.  Between
+// the two the host reads every system's status once: a store that ran out is
+// regrown and that system's traversal rerun directly, and both graphs are
+// captured again with the new buffers.
+
+constexpr uint32_t kEnsMagic = 0x50534745u;  // "PSGE"
+
+struct Ensemble {
+    uint32_t magic = 0;
+    int device = 0;
+    size_t nsys = 0, total = 0;
+    std::vector<size_t> count, offset;
+    std::vector<State*> sys;
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t root = nullptr;
+    cudaGraphExec_t g_force = nullptr, g_step = nullptr;
+    bool dirty = true;
+    DevArrays cap{};          // arrays the graphs were captured with
+    float* cap_v[3] = {nullptr, nullptr, nullptr};
+    float cap_dt = 0.f;
+    float* vtmp = nullptr;    // 3 x total velocity scratch
+    double grid_scale = 1.0;
+    int variant = PSG_MORTON_AVX2;
+};
+
+static int ensure_tick_scratch(State* s) {
+    if (s->tk_bbox) return PSG_OK;
+    s->tk_grid = s->sms * 4;
+    PSG_ALLOC(s->tk_partial, s->tk_grid * sizeof(float2));
+    PSG_ALLOC(s->tk_bbox, 4 * sizeof(float));
+    for (int c = 0; c < 3; ++c) PSG_ALLOC(s->tk_v[c], s->max_particles * 4);
+    for (int c = 0; c < 3; ++c) PSG_ALLOC(s->tk_vmir[c], s->max_particles * 4);
+    return PSG_OK;
+}
+
+static DevArrays slice(const DevArrays& a, size_t off) {
+    DevArrays d = a;
+    d.x += off; d.y += off; d.z += off; d.m += off;
+    d.fx += off; d.fy += off; d.fz += off; d.id += off; d.codes += off;
+    return d;
+}
+
+// one system's forces for a tick, enqueued on s->stream without any host
+// synchronisation (capturable)
+static int enqueue_system_forces(State* s, const DevArrays& d, size_t n, int variant) {
+    cudaStream_t st = s->stream;
+    const int g = grid_for(s, n, 1024);
+    int gp = (int)((n + 1023) / 1024);
+    if (gp > s->tk_grid) gp = s->tk_grid;
+    launch_tick_reset_ids(d.id, n, g, st);
+    launch_prepare(d.x, d.y, d.z, n, s->tk_partial, gp, d.codes, s->tk_bbox, variant, st);
+    PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
+    launch_sort(s->sort, d.codes, n, g, s->d_status, st);
+    launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
+    launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
+    const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
+    launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, 0.f, 0.f, 0.f, 0.f, gt, st,
+                s->tk_bbox);
+    launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
+    if (n > 1) {
+        int r = enqueue_traversal(s, s->xyzm, d.fx, d.fy, d.fz);
+        if (r != PSG_OK) return r;
+    } else {
+        PSG_CHECK(cudaMemsetAsync(d.fx, 0, 4, st));
+        PSG_CHECK(cudaMemsetAsync(d.fy, 0, 4, st));
+        PSG_CHECK(cudaMemsetAsync(d.fz, 0, 4, st));
+    }
+    PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status), cudaMemcpyDeviceToHost,
+                              st));
+    return PSG_OK;
+}
+
+// one system's velocity permutation through ids + semi-implicit Euler
+static int enqueue_system_step(State* s, const DevArrays& d, float* const v[3], float* vt,
+                               size_t n, float dt) {
+    cudaStream_t st = s->stream;
+    TickState ts;
+    ts.id = d.id;
+    ts.vx_in = v[0]; ts.vy_in = v[1]; ts.vz_in = v[2];
+    ts.vx_out = vt; ts.vy_out = vt + n; ts.vz_out = vt + 2 * n;
+    ts.x = d.x; ts.y = d.y; ts.z = d.z; ts.m = d.m;
+    ts.fx = d.fx; ts.fy = d.fy; ts.fz = d.fz;
+    launch_tick_euler(ts, n, dt, grid_for(s, n, 1024), st);
+    for (int c = 0; c < 3; ++c)
+        PSG_CHECK(cudaMemcpyAsync(v[c], vt + c * n, n * 4, cudaMemcpyDeviceToDevice, st));
+    return PSG_OK;
+}
+
+static void drop_graphs(Ensemble* e) {
+    if (e->g_force) cudaGraphExecDestroy(e->g_force);
+    if (e->g_step) cudaGraphExecDestroy(e->g_step);
+    e->g_force = e->g_step = nullptr;
+    e->dirty = true;
+}
+
+// capture one graph: a branch per system, forked from and joined into root
+static int capture(Ensemble* e, bool forces, const DevArrays& a, float* const v[3], float dt,
+                   cudaGraphExec_t* out) {
+    PSG_CHECK(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
+    int r = PSG_OK;
+    if (cudaEventRecord(e->fork, e->root) != cudaSuccess) r = PSG_EDEVICE;
+    for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
+        State* s = e->sys[k];
+        if (cudaStreamWaitEvent(s->stream, e->fork, 0) != cudaSuccess) {
+            r = PSG_EDEVICE;
+            break;
+        }
+        const DevArrays d = slice(a, e->offset[k]);
+        if (forces) {
+            r = enqueue_system_forces(s, d, e->count[k], e->variant);
+        } else {
+            float* vk[3] = {v[0] + e->offset[k], v[1] + e->offset[k], v[2] + e->offset[k]};
+            r = enqueue_system_step(s, d, vk, e->vtmp + 3 * e->offset[k], e->count[k], dt);
+        }
+        if (r != PSG_OK) break;
+        if (cudaEventRecord(e->join[k], s->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(e->root, e->join[k], 0) != cudaSuccess)
+            r = PSG_EDEVICE;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->root, &graph);
+    if (r == PSG_OK && ce != cudaSuccess) {
+        note("cudaStreamEndCapture", ce);
+        r = PSG_EDEVICE;
+    }
+    if (r == PSG_OK) {
+        const cudaError_t ie = cudaGraphInstantiate(out, graph, 0ull);
+        if (ie != cudaSuccess) {
+            note("cudaGraphInstantiate", ie);
+            r = PSG_EDEVICE;
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    return r;
+}
+
+static int ensure_graphs(Ensemble* e, const DevArrays& a, float* const v[3], float dt) {
+    const bool same = !e->dirty && std::memcmp(&e->cap, &a, sizeof(DevArrays)) == 0 &&
+                      e->cap_v[0] == v[0] && e->cap_v[1] == v[1] && e->cap_v[2] == v[2] &&
+                      e->cap_dt == dt;
+    if (same) return PSG_OK;
+    drop_graphs(e);
+    for (State* s : e->sys) s->grid_scale = e->grid_scale;
+    int r = capture(e, true, a, v, dt, &e->g_force);
+    if (r == PSG_OK) r = capture(e, false, a, v, dt, &e->g_step);
+    if (r != PSG_OK) {
+        drop_graphs(e);
+        return r;
+    }
+    e->cap = a;
+    for (int c = 0; c < 3; ++c) e->cap_v[c] = v[c];
+    e->cap_dt = dt;
+    e->dirty = false;
+    return PSG_OK;
+}
+
+// after a forces replay: fatal status -> error; capacity bits -> regrow and
+// rerun that system's traversal, and capture again before the next tick
+static int check_systems(Ensemble* e, const DevArrays& a) {
+    for (size_t k = 0; k < e->nsys; ++k) {
+        State* s = e->sys[k];
+        const uint32_t err = s->h_status->err;
+        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES)) {
+            std::snprintf(g_err, sizeof(g_err), "ensemble system %zu: device status 0x%x", k, err);
+            return (err & PSG_ERR_NODES) ? PSG_EINVAL : PSG_EDEVICE;
+        }
+        if (err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW | PSG_ERR_DENSE_OVERFLOW |
+                   PSG_ERR_HEAVY_OVERFLOW)) {
+            int r = regrow(s, err);
+            if (r != PSG_OK) return r;
+            PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, s->stream));
+            const DevArrays d = slice(a, e->offset[k]);
+            uint32_t err2 = 0;
+            r = run_traversal(s, s->xyzm, d.fx, d.fy, d.fz, &err2);
+            if (r != PSG_OK) return r;
+            e->dirty = true;
+        }
+    }
+    return PSG_OK;
+}
+
+static int ens_map(Ensemble* e, const psg_arrays_t* a, DevArrays& d) {
+    if (a->n != e->total) {
+        std::snprintf(g_err, sizeof(g_err), "ensemble: %zu particles given, %zu expected", a->n,
+                      e->total);
+        return PSG_EINVAL;
+    }
+    d.x = a->x; d.y = a->y; d.z = a->z; d.m = a->mass;
+    d.fx = a->fx; d.fy = a->fy; d.fz = a->fz; d.id = a->id; d.codes = a->codes;
+    void* ps[9] = {d.x, d.y, d.z, d.m, d.fx, d.fy, d.fz, d.id, d.codes};
+    for (void* p : ps) {
+        if (!on_device(p)) {
+            std::snprintf(g_err, sizeof(g_err), "ensemble arrays must be device memory");
+            return PSG_EINVAL;
+        }
+    }
+    d.any_host = false;
+    return PSG_OK;
+}
+
+static void free_ensemble(Ensemble* e) {
+    if (e->root) cudaStreamSynchronize(e->root);
+    drop_graphs(e);
+    for (State* s : e->sys) {
+        if (s) {
+            free_state(s);
+            delete s;
+        }
+    }
+    for (cudaEvent_t ev : e->join)
+        if (ev) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->root) cudaStreamDestroy(e->root);
+    if (e->vtmp) cudaFree(e->vtmp);
+    e->magic = 0;
+}
+
+static int ens_create(Ensemble* e, const size_t* counts, size_t nsys, const float* theta) {
+    PSG_CHECK(cudaGetDevice(&e->device));
+    e->nsys = nsys;
+    e->count.assign(counts, counts + nsys);
+    e->offset.resize(nsys);
+    size_t off = 0;
+    for (size_t k = 0; k < nsys; ++k) {
+        e->offset[k] = off;
+        off += counts[k];
+    }
+    e->total = off;
+    PSG_CHECK(cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking));
+    PSG_CHECK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    e->join.assign(nsys, nullptr);
+    e->sys.assign(nsys, nullptr);
+    for (size_t k = 0; k < nsys; ++k) {
+        PSG_CHECK(cudaEventCreateWithFlags(&e->join[k], cudaEventDisableTiming));
+        State* s = new (std::nothrow) State;
+        if (!s) return PSG_EALLOC;
+        e->sys[k] = s;
+        const float th = theta && theta[k] > 0.f ? theta[k] : 2.0f;
+        int r = init_state(s, counts[k], th);
+        if (r != PSG_OK) return r;
+        r = ensure_tick_scratch(s);
+        if (r != PSG_OK) return r;
+    }
+    PSG_ALLOC(e->vtmp, 3 * (e->total ? e->total : 1) * sizeof(float));
+    e->magic = kEnsMagic;
+    return PSG_OK;
+}
+
+static int ens_run(Ensemble* e, const psg_arrays_t* a, float* const v[3], float dt,
+                   uint32_t ticks) {
+    DevArrays d;
+    int r = ens_map(e, a, d);
+    if (r != PSG_OK) return r;
+    for (int c = 0; c < 3; ++c) {
+        if (!on_device(v[c])) {
+            std::snprintf(g_err, sizeof(g_err), "ensemble velocities must be device memory");
+            return PSG_EINVAL;
+        }
+    }
+    PSG_CHECK(cudaSetDevice(e->device));
+    for (uint32_t t = 0; t < ticks; ++t) {
+        r = ensure_graphs(e, d, v, dt);
+        if (r != PSG_OK) return r;
+        PSG_CHECK(cudaGraphLaunch(e->g_force, e->root));
+        PSG_CHECK(cudaStreamSynchronize(e->root));
+        r = check_systems(e, d);
+        if (r != PSG_OK) return r;
+        PSG_CHECK(cudaGraphLaunch(e->g_step, e->root));
+    }
+    PSG_CHECK(cudaStreamSynchronize(e->root));
+    return PSG_OK;
+}
+
+// Autotuner.  theta: per size class (the systems with the same floor(log2 N)),
+// the smallest theta of a ladder whose median relative force error against
+// an FP64 direct sum on up to 1024 particles of the class's first system is
+// at most `target`.  Launch shape: the traversal grids' scale, among
+// {1, 1/2, 1/4} of the single-system persistent grids, by the time of one
+// forces replay of the whole ensemble.  Works on copies; the caller's arrays
+// are left as they are.
+static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float* theta_out,
+                        double* scale_out) {
+    DevArrays d;
+    int r = ens_map(e, a, d);
+    if (r != PSG_OK) return r;
+    PSG_CHECK(cudaSetDevice(e->device));
+    const size_t T = e->total;
+    float* buf = nullptr;  // scratch copy: x y z m fx fy fz (7 T floats), id, codes
+    PSG_ALLOC(buf, (size_t)9 * T * 4 + 16);
+    DevArrays c;
+    c.x = buf; c.y = buf + T; c.z = buf + 2 * T; c.m = buf + 3 * T;
+    c.fx = buf + 4 * T; c.fy = buf + 5 * T; c.fz = buf + 6 * T;
+    c.id = (uint32_t*)(buf + 7 * T); c.codes = (uint32_t*)(buf + 8 * T);
+    c.any_host = false;
+    auto restore = [&]() -> int {
+        PSG_CHECK(cudaMemcpyAsync(c.x, d.x, T * 4, cudaMemcpyDeviceToDevice, e->root));
+        PSG_CHECK(cudaMemcpyAsync(c.y, d.y, T * 4, cudaMemcpyDeviceToDevice, e->root));
+        PSG_CHECK(cudaMemcpyAsync(c.z, d.z, T * 4, cudaMemcpyDeviceToDevice, e->root));
+        PSG_CHECK(cudaMemcpyAsync(c.m, d.m, T * 4, cudaMemcpyDeviceToDevice, e->root));
+        PSG_CHECK(cudaStreamSynchronize(e->root));
+        return PSG_OK;
+    };
+    static const float ladder[] = {1.0f, 1.5f, 2.0f, 3.0f, 4.0f, 6.0f, 8.0f};
+    const int nl = (int)(sizeof(ladder) / sizeof(ladder[0]));
+    std::vector<int> cls(e->nsys);
+    for (size_t k = 0; k < e->nsys; ++k) cls[k] = (int)std::floor(std::log2((double)e->count[k] + 1));
+    std::vector<float> chosen(e->nsys, 0.f);
+    uint32_t* d_tg = nullptr;
+    double* d_f64 = nullptr;
+    const size_t kSample = 1024;
+    PSG_ALLOC(d_tg, kSample * 4);
+    PSG_ALLOC(d_f64, kSample * 3 * sizeof(double));
+    std::vector<uint32_t> tg(kSample);
+    std::vector<double> f64(kSample * 3);
+    std::vector<float> fx(kSample), fy(kSample), fz(kSample);
+    for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
+        if (chosen[k] > 0.f) continue;
+        State* s = e->sys[k];
+        const size_t n = e->count[k];
+        const DevArrays ck = slice(c, e->offset[k]);
+        float pick = ladder[nl - 1];
+        for (int li = 0; li < nl && r == PSG_OK; ++li) {
+            if ((r = restore()) != PSG_OK) break;
+            s->theta = ladder[li];
+            launch_tick_reset_ids(ck.id, n, grid_for(s, n, 1024), s->stream);
+            int gp = (int)((n + 1023) / 1024);
+            if (gp > s->tk_grid) gp = s->tk_grid;
+            launch_prepare(ck.x, ck.y, ck.z, n, s->tk_partial, gp, ck.codes, s->tk_bbox,
+                           e->variant, s->stream);
+            r = tick_core(s, ck, n, 0.f, 0.f, 0.f, 0.f, s->tk_bbox);
+            if (r != PSG_OK) break;
+            const size_t ns = n < kSample ? n : kSample;
+            for (size_t i = 0; i < ns; ++i) tg[i] = (uint32_t)(i * n / ns);
+            PSG_CHECK(cudaMemcpyAsync(d_tg, tg.data(), ns * 4, cudaMemcpyHostToDevice, s->stream));
+            launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, s->sms * 8, s->stream);
+            PSG_CHECK(cudaMemcpyAsync(f64.data(), d_f64, ns * 3 * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s->stream));
+            std::vector<float> hf[3] = {std::vector<float>(n), std::vector<float>(n),
+                                        std::vector<float>(n)};
+            PSG_CHECK(cudaMemcpyAsync(hf[0].data(), ck.fx, n * 4, cudaMemcpyDeviceToHost, s->stream));
+            PSG_CHECK(cudaMemcpyAsync(hf[1].data(), ck.fy, n * 4, cudaMemcpyDeviceToHost, s->stream));
+            PSG_CHECK(cudaMemcpyAsync(hf[2].data(), ck.fz, n * 4, cudaMemcpyDeviceToHost, s->stream));
+            PSG_CHECK(cudaStreamSynchronize(s->stream));
+            std::vector<double> rel(ns);
+            for (size_t i = 0; i < ns; ++i) {
+                const double gx = f64[3 * i], gy = f64[3 * i + 1], gz = f64[3 * i + 2];
+                const double ex = hf[0][tg[i]] - gx, ey = hf[1][tg[i]] - gy, ez = hf[2][tg[i]] - gz;
+                const double nr = std::sqrt(gx * gx + gy * gy + gz * gz);
+                rel[i] = nr > 0 ? std::sqrt(ex * ex + ey * ey + ez * ez) / nr : 0.0;
+            }
+            std::nth_element(rel.begin(), rel.begin() + ns / 2, rel.end());
+            if (rel[ns / 2] <= (double)target) {
+                pick = ladder[li];
+                break;
+            }
+        }
+        for (size_t j = 0; j < e->nsys; ++j)
+            if (cls[j] == cls[k]) chosen[j] = pick;
+    }
+    cudaFree(d_tg);
+    cudaFree(d_f64);
+    if (r == PSG_OK) {
+        for (size_t k = 0; k < e->nsys; ++k) e->sys[k]->theta = chosen[k];
+        // launch shape: one forces replay of the copies per grid scale
+        static const double scales[] = {1.0, 0.5, 0.25};
+        float* vdummy[3] = {c.fx, c.fy, c.fz};
+        double best = 1e300;
+        double best_scale = 1.0;
+        cudaEvent_t t0, t1;
+        PSG_CHECK(cudaEventCreate(&t0));
+        PSG_CHECK(cudaEventCreate(&t1));
+        for (double sc : scales) {
+            e->grid_scale = sc;
+            e->dirty = true;
+            for (int rep = 0; rep < 2 && r == PSG_OK; ++rep) {  // the first replay grows stores
+                if ((r = restore()) != PSG_OK) break;
+                if ((r = ensure_graphs(e, c, vdummy, 0.f)) != PSG_OK) break;
+                PSG_CHECK(cudaEventRecord(t0, e->root));
+                PSG_CHECK(cudaGraphLaunch(e->g_force, e->root));
+                PSG_CHECK(cudaEventRecord(t1, e->root));
+                PSG_CHECK(cudaStreamSynchronize(e->root));
+                if ((r = check_systems(e, c)) != PSG_OK) break;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, t0, t1);
+                if (rep == 1 && ms < best) {
+                    best = ms;
+                    best_scale = sc;
+                }
+            }
+            if (r != PSG_OK) break;
+        }
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        e->grid_scale = best_scale;
+        drop_graphs(e);
+        if (scale_out) *scale_out = best_scale;
+        if (theta_out)
+            for (size_t k = 0; k < e->nsys; ++k) theta_out[k] = chosen[k];
+    }
+    cudaFree(buf);
+    return r;
+}
+
 }  // namespace psg
 
 using psg::State;
+
 
 extern "C" {
 
@@ -950,6 +1387,55 @@ int psg_direct_f64(void* mem, const psg_arrays_t* a, const uint32_t* targets, si
     PSG_CHECK(cudaStreamSynchronize(st));
     if (ht) cudaFree(dt);
     if (ho) cudaFree(dout);
+    return PSG_OK;
+}
+
+// ---- batched ensemble ------------------------------------------------------------
+
+int psg_ensemble_create(void** out, const size_t* counts, size_t n_systems, const float* theta) {
+    if (!out || !counts || n_systems == 0) return PSG_EINVAL;
+    for (size_t k = 0; k < n_systems; ++k)
+        if (counts[k] == 0 || counts[k] > 60000000u) return PSG_EINVAL;
+    psg::Ensemble* e = new (std::nothrow) psg::Ensemble;
+    if (!e) return PSG_EALLOC;
+    int r = psg::ens_create(e, counts, n_systems, theta);
+    if (r != PSG_OK) {
+        psg::free_ensemble(e);
+        delete e;
+        return r;
+    }
+    *out = e;
+    return PSG_OK;
+}
+
+int psg_ensemble_destroy(void* h) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic) return PSG_EINVAL;
+    cudaSetDevice(e->device);
+    psg::free_ensemble(e);
+    delete e;
+    return PSG_OK;
+}
+
+int psg_ensemble_run(void* h, const psg_arrays_t* a, float* vx, float* vy, float* vz, float dt,
+                     uint32_t ticks) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || !a || !vx || !vy || !vz) return PSG_EINVAL;
+    float* const v[3] = {vx, vy, vz};
+    return psg::ens_run(e, a, v, dt, ticks);
+}
+
+int psg_ensemble_autotune(void* h, const psg_arrays_t* a, float target, float* theta_out,
+                          double* grid_scale_out) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || !a || !(target > 0.f)) return PSG_EINVAL;
+    return psg::ens_autotune(e, a, target, theta_out, grid_scale_out);
+}
+
+int psg_ensemble_systems(void* h, float* theta_out, size_t n) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || !theta_out || n != e->nsys) return PSG_EINVAL;
+    for (size_t k = 0; k < n; ++k) theta_out[k] = e->sys[k]->theta;
     return PSG_OK;
 }
 

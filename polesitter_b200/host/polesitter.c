@@ -275,6 +275,68 @@ ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float
                                    loss_out));
 }
 
+static void ens_arrays(psg_arrays_t* a, const ps_particle_arrs_t* arrs, uint32_t* codes) {
+    a->x = arrs->x;
+    a->y = arrs->y;
+    a->z = arrs->z;
+    a->mass = arrs->mass;
+    a->fx = arrs->fx;
+    a->fy = arrs->fy;
+    a->fz = arrs->fz;
+    a->id = arrs->id;
+    a->codes = codes;
+    a->n = arrs->cnt;
+}
+
+ps_result_t ps_b200_ensemble_create(ps_b200_ensemble_t** out, const size_t* counts,
+                                    size_t n_systems, const float* theta) {
+    if (!out) {
+        return PS_EINVAL;
+    }
+    void* h = NULL;
+    int r = psg_ensemble_create(&h, counts, n_systems, theta);
+    if (r == PSG_OK) {
+        *out = (ps_b200_ensemble_t*)h;
+    }
+    return to_ps(r);
+}
+
+ps_result_t ps_b200_ensemble_autotune(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
+                                      uint32_t* morton_codes, float target_median_error,
+                                      float* theta_out, double* grid_scale_out) {
+    if (!ens || !arrs || !morton_codes) {
+        return PS_EINVAL;
+    }
+    psg_arrays_t a;
+    ens_arrays(&a, arrs, morton_codes);
+    return to_ps(psg_ensemble_autotune(ens, &a, target_median_error, theta_out, grid_scale_out));
+}
+
+ps_result_t ps_b200_ensemble_run(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
+                                 uint32_t* morton_codes, float* vx, float* vy, float* vz,
+                                 float dt, uint32_t ticks) {
+    if (!ens || !arrs || !morton_codes) {
+        return PS_EINVAL;
+    }
+    psg_arrays_t a;
+    ens_arrays(&a, arrs, morton_codes);
+    return to_ps(psg_ensemble_run(ens, &a, vx, vy, vz, dt, ticks));
+}
+
+ps_result_t ps_b200_ensemble_theta(ps_b200_ensemble_t* ens, float* theta_out, size_t n) {
+    if (!ens) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_systems(ens, theta_out, n));
+}
+
+ps_result_t ps_b200_ensemble_destroy(ps_b200_ensemble_t* ens) {
+    if (!ens) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_destroy(ens));
+}
+
 const char* ps_b200_last_error(void) { return psg_last_error(); }
 
 ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,

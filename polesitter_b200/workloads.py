@@ -175,6 +175,39 @@ def clumpy_plummer(n: int, seed: int, n_clumps: int = 32, clump_fraction: float 
     return Particles(pos[0], pos[1], pos[2], m)
 
 
+def ensemble(n_systems: int, seed: int, n_min: int = 1024, n_max: int = 262144):
+    """The batched-ensemble workload: ``n_systems`` independent systems with
+    N drawn log-uniform in [n_min, n_max]; even-numbered ones uniform cubes
+    ([-1, 1]^3, masses U[0.5, 1.5] / N, at rest), odd-numbered ones Plummer
+    spheres with a in [0.5, 2] (masses 1/N, isotropic Plummer velocities).
+    Returns (counts, Particles of all systems concatenated, vx, vy, vz)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    counts = np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=n_systems)).astype(np.int64)
+    xs, vs, ms = [], [], []
+    for k, n in enumerate(counts):
+        sub = int(rng.integers(0, 2**31))
+        if k % 2 == 0:
+            p = uniform_cube(int(n), sub)
+            pos = np.stack([p.x, p.y, p.z])
+            m = (p.mass / np.float32(n)).astype(np.float32)
+            vel = np.zeros((3, n), np.float64)
+        else:
+            r2 = np.random.Generator(np.random.PCG64(sub))
+            a = r2.uniform(0.5, 2.0)
+            r = _plummer_radii(r2, int(n), a, 10.0)
+            pos = _isotropic(r2, int(n)) * r[None, :]
+            vel = plummer_velocities(r2, r, a, 1.0)
+            m = np.full(int(n), 1.0 / n, np.float32)
+        xs.append(pos.astype(np.float32))
+        vs.append(vel.astype(np.float32))
+        ms.append(m)
+    pos = np.concatenate(xs, axis=1)
+    vel = np.concatenate(vs, axis=1)
+    p = Particles(pos[0], pos[1], pos[2], np.concatenate(ms))
+    p.id[:] = np.concatenate([np.arange(n, dtype=np.uint32) for n in counts])
+    return counts, p, vel[0].copy(), vel[1].copy(), vel[2].copy()
+
+
 def _lcg_stream(state: int, count: int) -> tuple[np.ndarray, int]:
     """``state = state*1664525 + 1013904223 (mod 2^32)`` (tests/accuracy.c:33-36),
     returned as float32 ``(state >> 8) / 16777215`` (accuracy.c:38-40)."""
