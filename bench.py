@@ -31,6 +31,10 @@ Reported (one JSON line on rank 0):
              FP32-bound, from its CUDA-event time and algorithmic flop count
   cpu_baseline  the reference's own threaded CPU tick (oracle/_ref) on the
              same workload, timed on this host's cores
+  plain_c2, tick_loop, ensemble  (closure workload, unless --minimal) the
+             plain Plummer theta=2 tick; 100 device-resident Euler ticks of
+             two colliding 4M-particle Plummer spheres; 256 independent
+             systems in replayed CUDA graphs with the autotuner
 With --gpus N > 1 every rank runs an independent replica (the path has no
 exchange step on one system): weak scaling, value = N x ticks / max time.
 
@@ -434,6 +438,8 @@ def run_b200(args):
     ctx.destroy()
     if closure and rank == 0 and not args.minimal:
         line["plain_c2"] = plain_c2(P, torch, dev, flush)
+        line["tick_loop"] = tick_loop(P, torch, dev)
+        line["ensemble"] = ensemble_run(P, torch, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference_ticks(p0, ticks=1 if closure else 3, warmup=1,
                                                    theta=theta)
@@ -512,6 +518,94 @@ def plain_c2(P, torch, dev, flush):
                 ts.append(time.perf_counter() - t0)
     return {"workload": WORKLOADS["plain"], "ticks_per_s": len(ts) / sum(ts), "steps": len(ts),
             "warmup": 3}
+
+
+def tick_loop(P, torch, dev):
+    """The device-resident tick loop on two colliding Plummer spheres
+    (N=4,194,304, mass ratio 3:1, 20a apart, 0.3 relative velocity, theta=2):
+    100 ticks of semi-implicit Euler, dt=1e-3 (ps_b200_run_ticks)."""
+    from polesitter_b200 import workloads as W
+    n, ticks = 1 << 22, 100
+    p, vx, vy, vz = W.two_plummer(n, 1)
+    a = Arrays()
+    for k in ("x", "y", "z", "mass", "fx", "fy", "fz"):
+        setattr(a, k, torch.from_numpy(getattr(p, k).copy()).to(dev))
+    a.id = torch.from_numpy(p.id.view(np.int32).copy()).to(dev)
+    v = [torch.from_numpy(x.astype(np.float32)).to(dev) for x in (vx, vy, vz)]
+    codes = torch.zeros(n, dtype=torch.int32, device=dev)
+    with P.Context(n, theta=2.0) as ctx:
+        ctx.run_ticks(a, codes, *v, 1e-3, 2)  # warm-up: grows the stores
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.run_ticks(a, codes, *v, 1e-3, ticks)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    return {"workload": "two colliding Plummer spheres, N=4,194,304 (3:1), theta=2, "
+                        "100 ticks of semi-implicit Euler dt=1e-3 on the device "
+                        "(ps_b200_run_ticks)",
+            "ticks_per_s": ticks / dt, "particle_ticks_per_s": n * ticks / dt}
+
+
+def ensemble_run(P, torch, dev):
+    """The batched ensemble: 256 independent systems, N log-uniform in
+    [1024, 262144], half uniform cubes and half Plummer spheres (a in
+    [0.5, 2]); theta per size class and the traversal grid scale from the
+    autotuner (target median force error 3e-2); 50 ticks of semi-implicit
+    Euler, dt=1e-3, each tick two replayed CUDA graphs.  Beside it, the same
+    systems advanced one after the other through ps_b200_run_ticks."""
+    from polesitter_b200 import workloads as W
+    nsys, ticks, target = 256, 50, 3e-2
+    counts, p, vx, vy, vz = W.ensemble(nsys, 2026)
+
+    def arrays():
+        a = Arrays()
+        for k in ("x", "y", "z", "mass", "fx", "fy", "fz"):
+            setattr(a, k, torch.from_numpy(getattr(p, k).copy()).to(dev))
+        a.id = torch.from_numpy(p.id.view(np.int32).copy()).to(dev)
+        return a, [torch.from_numpy(x.copy()).to(dev) for x in (vx, vy, vz)]
+
+    a, v = arrays()
+    codes = torch.zeros(p.n, dtype=torch.int32, device=dev)
+    with P.Ensemble(counts) as ens:
+        theta, scale = ens.autotune(a, codes, target)
+        ens.run(a, codes, *v, 1e-3, 2)  # warm-up: captures the graphs, grows stores
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens.run(a, codes, *v, 1e-3, ticks)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    # the same systems one after the other, without graphs
+    b, w = arrays()
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    ctxs = [P.Context(int(counts[k]), theta=float(theta[k])) for k in range(nsys)]
+
+    def one_pass():
+        for k in range(nsys):
+            lo, hi = int(offs[k]), int(offs[k + 1])
+            s = Arrays()
+            for key in ("x", "y", "z", "mass", "fx", "fy", "fz", "id"):
+                setattr(s, key, getattr(b, key)[lo:hi])
+            ctxs[k].run_ticks(s, codes[lo:hi], *(x[lo:hi] for x in w), 1e-3, 1)
+
+    one_pass()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        one_pass()
+    torch.cuda.synchronize()
+    seq = 3 / (time.perf_counter() - t0)
+    for c in ctxs:
+        c.destroy()
+    vals, cnts = np.unique(theta, return_counts=True)
+    return {"workload": "256 independent systems, N log-uniform in [1024, 262144] "
+                        f"({int(p.n)} particles), half uniform cubes, half Plummer a in "
+                        "[0.5, 2]; 50 ticks of Euler dt=1e-3",
+            "ensemble_ticks_per_s": ticks / dt, "particle_ticks_per_s": p.n * ticks / dt,
+            "autotuner": {"target_median_rel_error": target,
+                          "theta_per_class": {str(float(t)): int(c) for t, c in zip(vals, cnts)},
+                          "grid_scale": scale},
+            "one_system_at_a_time_ticks_per_s": seq,
+            "speedup_over_one_at_a_time": (ticks / dt) / seq}
 
 
 def main():
