@@ -51,3 +51,31 @@ def test_two_plummer_velocities():
     assert vx[:n1].mean() > 0 > vx[n1:].mean()
     # centre-of-mass momentum ~ 0
     assert abs(vx.mean()) < 0.01
+
+
+def test_clumpy_plummer_family():
+    p = W.clumpy_plummer(20000, 5)
+    assert p.n == 20000 and np.allclose(p.mass, 1.0 / p.n)
+    q = W.clumpy_plummer(20000, 5)
+    assert np.array_equal(p.x, q.x)
+    r = np.sqrt(p.x.astype(np.float64) ** 2 + p.y ** 2 + p.z ** 2)
+    assert r.max() < 16.0
+    # 30% of the particles sit in 32 small clumps: far denser cores than the host
+    H, _ = np.histogramdd(np.stack([p.x, p.y, p.z], 1), bins=64, range=[(-4, 4)] * 3)
+    assert H.max() > 20 * np.percentile(H[H > 0], 90)
+
+
+def test_ensemble_family():
+    counts, p, vx, vy, vz = W.ensemble(40, 3)
+    assert len(counts) == 40 and p.n == counts.sum() == vx.size
+    assert counts.min() >= 1024 and counts.max() <= 262144
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    for k in range(40):
+        a, b = offs[k], offs[k + 1]
+        assert np.array_equal(p.id[a:b], np.arange(b - a, dtype=np.uint32))
+        if k % 2 == 0:  # uniform cubes at rest
+            assert np.all(np.abs(p.x[a:b]) <= 1.0) and not vx[a:b].any()
+        else:           # Plummer spheres with velocities, mass 1/N
+            assert np.allclose(p.mass[a:b], 1.0 / (b - a)) and vx[a:b].any()
+    c2, p2, *_ = W.ensemble(40, 3)
+    assert np.array_equal(c2, counts) and np.array_equal(p2.x, p.x)
