@@ -21,7 +21,9 @@
 // node p (a "group") start from the same candidates
 //   cand(p) = {root}                                         if depth(p) <= 1
 //   cand(p) = U_{s in NS(p)} (s leaf ? {s} : children(s))    otherwise.
-// One warp owns a group.  Candidates are tested 32 at a time, one per lane;
+// One warp owns a group (with the closure's order-1 accumulators, half a
+// group: children 0-3 or 4-7, so that the 4 x 9 accumulators leave room for
+// 4 blocks per SM).  Candidates are tested 32 at a time, one per lane;
 // each carries the set of the group's children it must be tested against,
 // and the lane loads the candidate once and runs the MAC (and M2L, into
 // per-child register accumulators) for each of those children.  What is
@@ -458,14 +460,20 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
     }
     __syncwarp();
     const uint32_t batch = MODE == MODE_INTERNAL ? 4u : 8u;
+    // the closure's order-1 accumulators take a group's children 4 at a time:
+    // a work item is (group, half)
+    constexpr uint32_t SL = GRAD ? 4u : 8u;
+    constexpr uint32_t NH = 8u / SL;
+    const uint32_t items = total * NH;
 
     for (;;) {
         uint32_t g0 = 0;
         if (lane == 0) g0 = atomicAdd(work, batch);
         g0 = __shfl_sync(0xFFFFFFFFu, g0, 0);
-        if (g0 >= total) break;
+        if (g0 >= items) break;
 #pragma unroll 1
-        for (uint32_t g = g0; g < g0 + batch && g < total; ++g) {
+        for (uint32_t gi = g0; gi < g0 + batch && gi < items; ++gi) {
+            const uint32_t g = gi / NH, base = (gi % NH) * SL;
             uint32_t pid, dp;
             if (MODE == MODE_INTERNAL) {
                 dp = A.level - 1;
@@ -495,7 +503,8 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             const uint32_t leaf_mask =
                 __ballot_sync(0xFFFFFFFFu, lane < nc && (cl >> 28) == 0) & 0xFFu;
             const uint32_t tgt_mask =
-                MODE == MODE_INTERNAL ? (((1u << nc) - 1u) & ~leaf_mask) : leaf_mask;
+                (MODE == MODE_INTERNAL ? (((1u << nc) - 1u) & ~leaf_mask) : leaf_mask) &
+                (((1u << SL) - 1u) << base);
             if (tgt_mask == 0) continue;
             if constexpr (MODE == MODE_LEAF) {
                 if ((tgt_mask >> lane) & 1u) {
@@ -555,13 +564,13 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             }
             __syncwarp();
 
-            float acc[8][3];
+            float acc[SL][3];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.f;
-            float gacc[GRAD ? 8 : 1][6];
+            for (int q = 0; q < (int)SL; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.f;
+            float gacc[GRAD ? SL : 1][6];
             if constexpr (GRAD) {
 #pragma unroll
-                for (int q = 0; q < 8; ++q)
+                for (int q = 0; q < (int)SL; ++q)
 #pragma unroll
                     for (int k = 0; k < 6; ++k) gacc[q][k] = 0.f;
             }
@@ -655,7 +664,8 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     const uint32_t chunk_mask = __reduce_or_sync(0xFFFFFFFFu, smask);
                     uint32_t near_bits = 0;
 #pragma unroll
-                    for (uint32_t q = 0; q < 8; ++q) {
+                    for (uint32_t k = 0; k < SL; ++k) {
+                        const uint32_t q = base + k;
                         if (!((chunk_mask >> q) & 1u)) continue;
                         const float4 ug = sm.cgeo[q];
                         float dx, dy, dz, d2;
@@ -669,18 +679,18 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                             m2l_field_grad(dx, dy, dz, d2, smp, fx, fy, fz, g3, gi);
                             g3 = sep ? g3 : 0.f;
                             gi = sep ? gi : 0.f;
-                            gacc[q][0] += fmaf(g3 * dx, dx, -gi);
-                            gacc[q][1] += fmaf(g3 * dy, dy, -gi);
-                            gacc[q][2] += fmaf(g3 * dz, dz, -gi);
-                            gacc[q][3] += g3 * dx * dy;
-                            gacc[q][4] += g3 * dx * dz;
-                            gacc[q][5] += g3 * dy * dz;
+                            gacc[k][0] += fmaf(g3 * dx, dx, -gi);
+                            gacc[k][1] += fmaf(g3 * dy, dy, -gi);
+                            gacc[k][2] += fmaf(g3 * dz, dz, -gi);
+                            gacc[k][3] += g3 * dx * dy;
+                            gacc[k][4] += g3 * dx * dz;
+                            gacc[k][5] += g3 * dy * dz;
                         } else {
                             m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
                         }
-                        acc[q][0] += sep ? fx : 0.f;
-                        acc[q][1] += sep ? fy : 0.f;
-                        acc[q][2] += sep ? fz : 0.f;
+                        acc[k][0] += sep ? fx : 0.f;
+                        acc[k][1] += sep ? fy : 0.f;
+                        acc[k][2] += sep ? fz : 0.f;
                         if (act && !sep) near_bits |= 1u << q;
                         if (DEBUG) {
                             const uint32_t bm = __ballot_sync(0xFFFFFFFFu, sep);
@@ -765,11 +775,12 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 }
             }
 #pragma unroll
-            for (uint32_t q = 0; q < 8; ++q) {
+            for (uint32_t k = 0; k < SL; ++k) {
+                const uint32_t q = base + k;
                 if (!((tgt_mask >> q) & 1u)) continue;
-                const float ax = warp_sum(acc[q][0]);
-                const float ay = warp_sum(acc[q][1]);
-                const float az = warp_sum(acc[q][2]);
+                const float ax = warp_sum(acc[k][0]);
+                const float ay = warp_sum(acc[k][1]);
+                const float az = warp_sum(acc[k][2]);
                 float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
                                        __fadd_rn(az, Lp.w));
                 float4 G0 = Gp0;
@@ -780,12 +791,12 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     L.y += sh.x;
                     L.z += sh.y;
                     L.w += sh.z;
-                    G0.x += warp_sum(gacc[q][0]);
-                    G0.y += warp_sum(gacc[q][1]);
-                    G0.z += warp_sum(gacc[q][2]);
-                    G0.w += warp_sum(gacc[q][3]);
-                    G1.x += warp_sum(gacc[q][4]);
-                    G1.y += warp_sum(gacc[q][5]);
+                    G0.x += warp_sum(gacc[k][0]);
+                    G0.y += warp_sum(gacc[k][1]);
+                    G0.z += warp_sum(gacc[k][2]);
+                    G0.w += warp_sum(gacc[k][3]);
+                    G1.x += warp_sum(gacc[k][4]);
+                    G1.y += warp_sum(gacc[k][5]);
                 }
                 if (lane == 0) {
                     const uint32_t u = fc + q;
@@ -1138,14 +1149,15 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
 
 // the leaf pass's work counter starts past the groups of depths 0 ..
 // heavy_depth-1, whose leaf children k_heavy_leaf takes
-__global__ void k_leaf_start(Status* status, int heavy_depth) {
+__global__ void k_leaf_start(Status* status, int heavy_depth, uint32_t parts) {
     uint32_t skip = 0;
     for (int d = 0; d < heavy_depth && d < kMaxDepth; ++d) skip += status->lvl_count[d];
-    status->work[0] = skip;
+    status->work[0] = skip * parts;
 }
 
-void launch_leaf_start(Status* status, int heavy_depth, cudaStream_t st) {
-    k_leaf_start<<<1, 1, 0, st>>>(status, heavy_depth);
+void launch_leaf_start(Status* status, int heavy_depth, int order, cudaStream_t st) {
+    // work items per group: 2 halves with the order-1 accumulators, else 1
+    k_leaf_start<<<1, 1, 0, st>>>(status, heavy_depth, order >= 1 ? 2u : 1u);
 }
 
 void launch_heavy_leaf(const TravArgs& A, int grid, cudaStream_t st) {

@@ -53,7 +53,7 @@ void launch_traverse_internal(const TravArgs& A, int level, int grid, cudaStream
 void launch_traverse_leaves(const TravArgs& A, const int grid[2], cudaStream_t st);
 void launch_dense_p2p(const TravArgs& A, int grid, cudaStream_t st);
 void launch_heavy_leaf(const TravArgs& A, int grid, cudaStream_t st);
-void launch_leaf_start(Status* status, int heavy_depth, cudaStream_t st);
+void launch_leaf_start(Status* status, int heavy_depth, int order, cudaStream_t st);
 
 
 // k_tick.cu -- the caller's tick loop on the device (README.md:65-111)

@@ -406,7 +406,7 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
     launch_heavy_leaf(A, scaled(s->heavy_slots), s->aux);
     PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
-    launch_leaf_start(s->d_status, A.heavy_depth, s->stream);
+    launch_leaf_start(s->d_status, A.heavy_depth, o, s->stream);
     const int lg[2] = {scaled(s->trav_grid[o][0]), scaled(s->trav_grid[o][1])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
