@@ -145,8 +145,9 @@ ps_result_t ps_b200_closure_forward(ps_context_t* ctx, const float* x, size_t n,
 
 /* training on the GPU with the project's own kernels: the mean squared error
  * over outputs 0..2 of MLP(x) against t (n x 3) and its gradient for one
- * batch (grad), or Adam over `epochs` shuffled passes of `batch` samples
- * (params in: initial values, out: trained; loss_out: per-epoch MSE) */
+ * batch (grad), or Adam over `epochs` shuffled passes of `batch` samples,
+ * the learning rate decaying from lr along a cosine to 5 % of it (params in:
+ * initial values, out: trained; loss_out: per-epoch MSE) */
 ps_result_t ps_b200_closure_grad(ps_context_t* ctx, const float* x, const float* t, size_t n,
                                  const float* params, float* grad_out, float* loss_out);
 ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float* t, size_t n,

@@ -1504,7 +1504,7 @@ int psg_closure_features(void* mem, const uint32_t* idx, size_t k, float* x_out,
 }
 
 // Train the closure MLP with Adam on (x, t) pairs (host arrays, n x 16 and
-// n x 3).  params (kMlpParams) holds the initial values and receives the
+// n x 3), the learning rate decaying from lr along a cosine to 5 % of it.  params (kMlpParams) holds the initial values and receives the
 // trained ones; loss_out (epochs) receives each epoch's mean squared error.
 int psg_closure_train(void* mem, const float* x, const float* t, size_t n, float* params,
                       uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* loss_out) {
@@ -1556,6 +1556,9 @@ int psg_closure_train(void* mem, const float* x, const float* t, size_t n, float
             perm[j] = tmp;
         }
         PSG_CHECK(cudaMemcpyAsync(d_perm, perm, n * 4, cudaMemcpyHostToDevice, st));
+        // cosine decay of the learning rate over the epochs, to 5 % of lr
+        const float lr_ep =
+            lr * (0.05f + 0.95f * 0.5f * (1.0f + cosf(3.14159265f * (float)ep / (float)epochs)));
         for (size_t b0 = 0; b0 < n; b0 += batch) {
             const size_t cnt = n - b0 < batch ? n - b0 : batch;
             PSG_CHECK(cudaMemsetAsync(d_g, 0, P * 4, st));
@@ -1565,7 +1568,7 @@ int psg_closure_train(void* mem, const float* x, const float* t, size_t n, float
             ++step;
             const float bc1 = 1.0f - powf(beta1, (float)step);
             const float bc2 = 1.0f - powf(beta2, (float)step);
-            psg::launch_mlp_adam(d_p, d_m, d_v, d_g, P, lr, beta1, beta2, eps, bc1, bc2, st);
+            psg::launch_mlp_adam(d_p, d_m, d_v, d_g, P, lr_ep, beta1, beta2, eps, bc1, bc2, st);
         }
         if (cudaGetLastError() != cudaSuccess) r = PSG_EDEVICE;
     }

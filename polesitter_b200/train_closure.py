@@ -1,6 +1,6 @@
 """Train the learned far-field closure and write its weights.
 
-    python -m polesitter_b200.train_closure --theta 7 --out polesitter_b200/closure_weights.npz
+    python -m polesitter_b200.train_closure --theta 6.5 --out polesitter_b200/closure_weights.npz
 
 Steps (all on the GPU through the library's C API):
   1. snapshots: ``--snapshots`` clumpy Plummer spheres of ``--n`` particles
@@ -44,11 +44,11 @@ def evaluate(ctx, params, n: int, theta: float, count: int, seed: int):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--theta", type=float, default=7.0)
+    ap.add_argument("--theta", type=float, default=6.5)
     ap.add_argument("--n", type=int, default=65536)
     ap.add_argument("--snapshots", type=int, default=2048)
-    ap.add_argument("--samples", type=int, default=1024)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--samples", type=int, default=4096)
+    ap.add_argument("--epochs", type=int, default=100)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=1)
