@@ -432,11 +432,14 @@ def run_b200(args):
             "clocks": clocks.summary(),
             "gpu_launches": KERNELS_PER_TICK[args.workload] * args.steps}
 
-    if closure and rank == 0 and not args.no_plain_curve:
+    # the extra lines run on single-GPU runs only (a multi-GPU run is the
+    # replica scaling measurement)
+    extras = world == 1 and not args.minimal
+    if closure and extras and not args.no_plain_curve:
         line["equal_error"] = plain_curve(ctx, P, d, pristine, codes, flush, n, value,
                                           accuracy["judge"]["max_of_tick_medians"])
     ctx.destroy()
-    if closure and rank == 0 and not args.minimal:
+    if closure and extras:
         line["plain_c2"] = plain_c2(P, torch, dev, flush)
         line["tick_loop"] = tick_loop(P, torch, dev)
         line["ensemble"] = ensemble_run(P, torch, dev)

@@ -114,7 +114,6 @@ int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n
 #define PSG_OPT_THETA 2
 #define PSG_OPT_MORTON_VARIANT 3
 #define PSG_OPT_TIMING 4         /* 1: time phases with CUDA events */
-#define PSG_OPT_USE_GRAPH 5      /* 1: replay calc_forces as a CUDA graph */
 #define PSG_OPT_KAHAN 6          /* 1: compensated FP32 sums in P2P */
 #define PSG_OPT_CLOSURE 7        /* 0 reference, 1 order-1 local, 2 + learned correction */
 #define PSG_OPT_JUDGE 8          /* 1: sampled FP64 judge in closure mode 1 too */

@@ -1,6 +1,7 @@
 // Device runtime behind the C ABI: per-context device memory, the tick's
-// launch sequence, host-pointer mirrors, status checks and the optional CUDA
-// graph replay of ps_calc_forces.
+// launch sequence, host-pointer mirrors, status checks with capacity regrow,
+// the learned closure's per-tick steps and training driver, the device tick
+// loop, and the batched ensemble's CUDA graphs.
 //
 // Ownership follows the reference (polesitter.h:1699-1767): the caller owns
 // every particle array and the ps_config_t buffer, and the host-side state
