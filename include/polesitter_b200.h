@@ -22,6 +22,9 @@ size_t ps_b200_context_size(void);
 #define PS_B200_OPT_KAHAN 6          /* compensated (Kahan) FP32 sums in P2P */
 #define PS_B200_OPT_CLOSURE 7        /* learned far-field closure, see below */
 #define PS_B200_OPT_JUDGE 8          /* 1: run the closure's judge in mode 1 too */
+#define PS_B200_OPT_HEAVY_DEPTH 9    /* leaves at most this deep (0..5) are walked by a whole
+                                        block each; -1 (default): the largest d with
+                                        2^d <= 4 theta */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
 
 /* Morton quantisation of ps_prepare_particles, process-wide (it takes no

@@ -25,6 +25,7 @@ RESULT_NAMES = {0: "PS_OK", -1: "PS_EOOM", -2: "PS_EINVAL", -3: "PS_ETHRD",
                 -4: "PS_EALLOC", -5: "PS_EDEVICE"}
 
 OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN, OPT_CLOSURE, OPT_JUDGE = 1, 2, 4, 6, 7, 8
+OPT_HEAVY_DEPTH = 9
 CLOSURE_PARAMS = 9928
 MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 
