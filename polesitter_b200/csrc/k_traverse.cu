@@ -60,7 +60,7 @@ constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-en
 constexpr int kP2PCap = 128;              // staged P2P sources of a group
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
-constexpr uint32_t kDenseGroup = 8;       // DENSE: groups with this many leaf particles go to k_dense_p2p
+constexpr uint32_t kDenseGroup = 4;       // DENSE: groups with this many leaf particles go to k_dense_p2p
 constexpr uint32_t kDenseChunk = 32;      // target particles per dense work record
 constexpr uint32_t kDenseSwitch = 32;     // fullest leaf from which the DENSE leaf pass runs
 constexpr uint32_t kBigSource = 16;       // DENSE: sources this full are summed by all lanes
@@ -841,10 +841,11 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
 }
 
 // L2P + P2P of the full leaves recorded by the leaf pass.  A warp takes one
-// record (a leaf, up to 32 of its particles, its source chain) at a time
-// from a shared counter; the lanes own the target particles and walk the
-// leaf's P2P sources together, so each source particle is one broadcast
-// load for the warp.  The sources are summed in chain order, so the result
+// record (a run of leaves, up to 32 of their particles, the group's source
+// chain) at a time from a shared counter; T lanes own the record's target
+// particles (T the smallest power of two >= their count) and the 32 / T
+// slices of lanes take every (32 / T)-th source each, so a record with few
+// targets still keeps the warp busy; the slices' sums are added at the end.  The sources are summed in chain order, so the result
 // does not depend on scheduling.
 template <bool DEBUG, bool GRAD>
 __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
@@ -861,9 +862,15 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         r = __shfl_sync(0xFFFFFFFFu, r, 0);
         if (r >= total) break;
         const uint4 rec = A.dense_rec[r];
-        const uint32_t fc = rec.x, run = rec.w >> 8;
-        const bool active = lane < (rec.w & 0xFFu);
-        const uint32_t i = rec.z + (active ? lane : 0u);
+        const uint32_t fc = rec.x, run = rec.w >> 8, cnt_t = rec.w & 0xFFu;
+        // T lanes per target set (the smallest power of two >= the record's
+        // targets); the 32 / T slices of lanes split the sources between them
+        uint32_t T = 1;
+        while (T < cnt_t) T <<= 1;
+        const uint32_t S = 32u / T;
+        const uint32_t tl = lane & (T - 1u), slice = lane / T;
+        const bool active = tl < cnt_t;
+        const uint32_t i = rec.z + (active ? tl : 0u);
         // this lane's leaf: the child of the run whose particles hold i
         uint32_t q = __ffs(run) - 1;
         for (uint32_t m = run; m; m &= m - 1) {
@@ -875,14 +882,24 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
         for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
             const uint32_t cnt = A.p2p.cnt[c];
-            for (uint32_t k = 0; k < cnt; ++k) {
+            for (uint32_t k = slice; k < cnt; k += S) {
                 if (!((A.p2p.mask[(size_t)c * kP2PChunk + k] >> q) & 1u)) continue;
                 const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + k]];
                 p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz, cx, cy, cz);
                 if (DEBUG) inter += active ? si.y : 0u;
             }
         }
-        if (active) {
+        // sum the slices' partial sums (fixed order)
+        bx -= cx;
+        by -= cy;
+        bz -= cz;
+        cx = cy = cz = 0.f;
+        for (uint32_t o = T; o < 32u; o <<= 1) {
+            bx += __shfl_xor_sync(0xFFFFFFFFu, bx, o);
+            by += __shfl_xor_sync(0xFFFFFFFFu, by, o);
+            bz += __shfl_xor_sync(0xFFFFFFFFu, bz, o);
+        }
+        if (active && slice == 0) {
             const float4 L = tv.lt[u];
             float lx = L.y, ly = L.z, lz = L.w;
             if constexpr (GRAD) {
