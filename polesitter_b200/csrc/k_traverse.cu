@@ -60,7 +60,7 @@ constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-en
 constexpr int kP2PCap = 128;              // staged P2P sources of a group
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
-constexpr uint32_t kDenseGroup = 4;       // DENSE: groups with this many leaf particles go to k_dense_p2p
+constexpr uint32_t kDenseGroup = 1;       // DENSE: groups with this many leaf particles (all) go to k_dense_p2p
 constexpr uint32_t kDenseChunk = 32;      // target particles per dense work record
 constexpr uint32_t kDenseSwitch = 32;     // fullest leaf from which the DENSE leaf pass runs
 constexpr uint32_t kBigSource = 16;       // DENSE: sources this full are summed by all lanes
