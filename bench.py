@@ -82,12 +82,12 @@ KERNELS_PER_TICK = {"plain": 39, "closure": 44}
 # DRAM bytes (read + write) of one leaf-pass launch, from the ncu captures
 # summarised under profiles/: the plain one at this size; the closure one
 # captured at N=131072 and scaled by the M2L pair count (x 8.28) to N=1M
-LEAF_PASS_DRAM_BYTES = {"plain": 255.3e6, "closure": 1.45e9}
+LEAF_PASS_DRAM_BYTES = {"plain": 255.3e6, "closure": 1.48e9}
 TRAFFIC_NOTE = {
     "plain": "dram read+write bytes per launch, ncu capture of this workload "
              "(profiles/traversal_leaf_plummer1m.md)",
     "closure": "dram read+write bytes per launch, ncu capture of the same kernel at N=131072 "
-               "(174.9 MB) scaled by the M2L pair count (x 8.28) to N=1M "
+               "(179.1 MB) scaled by the M2L pair count (x 8.28) to N=1M "
                "(profiles/traversal_leaf_closure_clumpy131k.md)"}
 FLOP_M2L = 35         # per M2L pair: polesitter.h:1065-1092
 FLOP_M2L_ORDER1 = 59  # ... plus the monopole field gradient (closure order 1)
