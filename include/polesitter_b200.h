@@ -25,6 +25,10 @@ size_t ps_b200_context_size(void);
 #define PS_B200_OPT_HEAVY_DEPTH 9    /* leaves at most this deep (0..5) are walked by a whole
                                         block each; -1 (default): the largest d with
                                         2^d <= 4 theta */
+#define PS_B200_OPT_LEAF_CAP 10      /* leaf capacity B (1..256): a node below the root
+                                        holding more than B particles is split (the
+                                        reference: 1, polesitter.h:911); the root is split
+                                        whenever it holds 2 or more */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
 
 /* Morton quantisation of ps_prepare_particles, process-wide (it takes no
@@ -167,7 +171,7 @@ ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float
  * of DEVICE arrays: system k holds counts[k] particles from the sum of the
  * counts before it, its ids are local (0 .. counts[k]-1) and, like its
  * positions, come back sorted within its range.  Results equal running each
- * system through ps_b200_run_ticks with its own theta. */
+ * system through ps_b200_run_ticks with its own theta and leaf capacity. */
 typedef struct ps_b200_ensemble ps_b200_ensemble_t;
 
 /* theta per system (NULL: 2.0 for all) */
@@ -175,13 +179,17 @@ ps_result_t ps_b200_ensemble_create(ps_b200_ensemble_t** out, const size_t* coun
                                     size_t n_systems, const float* theta);
 
 /* The autotuner, on copies of the given state (arrs and the codes array are
- * not changed): per size class (systems with equal floor(log2 N)), the
- * smallest theta of {1, 1.5, 2, 3, 4, 6, 8} whose median relative force
- * error against an FP64 direct sum (1024 sampled particles of the class's
- * first system) is at most target_median_error; then the traversal grids'
+ * not changed): per size class (systems with equal floor(log2 N)) and per
+ * leaf capacity of the ladder (default {1, 16, 32, 64}), the smallest theta
+ * of {1, 1.5, 2, 3, 4, 6, 8} whose median relative force error against an
+ * FP64 direct sum (1024 sampled particles of the class's first system) is at
+ * most target_median_error, then the device time of one tick of that system
+ * there; the class takes the fastest (theta, leaf capacity) that meets the
+ * target (if none does, the smallest error).  Then the traversal grids'
  * scale among {1, 1/2, 1/4} of one system's persistent grids, by the time of
  * one forces replay of the whole ensemble.  theta_out (n_systems) and
- * grid_scale_out receive the choice (either may be NULL). */
+ * grid_scale_out receive the choice (either may be NULL);
+ * ps_b200_ensemble_leaf_caps reads the leaf capacities. */
 ps_result_t ps_b200_ensemble_autotune(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
                                       uint32_t* morton_codes, float target_median_error,
                                       float* theta_out, double* grid_scale_out);
@@ -191,6 +199,13 @@ ps_result_t ps_b200_ensemble_run(ps_b200_ensemble_t* ens, const ps_particle_arrs
                                  uint32_t* morton_codes, float* vx, float* vy, float* vz,
                                  float dt, uint32_t ticks);
 ps_result_t ps_b200_ensemble_theta(ps_b200_ensemble_t* ens, float* theta_out, size_t n);
+/* leaf capacity (PS_B200_OPT_LEAF_CAP) of each system: read, set (n = n_systems) */
+ps_result_t ps_b200_ensemble_leaf_caps(ps_b200_ensemble_t* ens, uint32_t* cap_out, size_t n);
+ps_result_t ps_b200_ensemble_set_leaf_caps(ps_b200_ensemble_t* ens, const uint32_t* caps,
+                                           size_t n);
+/* the leaf capacities the autotuner tries (each 1..256) */
+ps_result_t ps_b200_ensemble_set_leaf_ladder(ps_b200_ensemble_t* ens, const uint32_t* caps,
+                                             size_t n);
 ps_result_t ps_b200_ensemble_destroy(ps_b200_ensemble_t* ens);
 
 /* message of the last CUDA-side failure on this thread */

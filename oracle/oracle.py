@@ -60,6 +60,7 @@ class Oracle:
         lib.pso_p2p_pair.argtypes = [vp] * 7 + [C.c_uint32] * 4
         lib.pso_euler_step.argtypes = [sz] + [vp] * 11 + [f32, vp]
         lib.pso_set_closure.argtypes = [vp, C.c_int, vp]
+        lib.pso_set_leaf_cap.argtypes = [vp, C.c_uint32]
         self.lib = lib
 
     def morton_encode(self, x, y, z) -> int:
@@ -77,12 +78,16 @@ class Oracle:
                           _ptr(p.z), _ptr(p.mass))
 
     def calc(self, p, codes, cx, cy, cz, hw, theta=2.0, mt=True, accum_mode=0,
-             want_tree=True, want_p2p=False, order=0, feat=None):
+             want_tree=True, want_p2p=False, order=0, feat=None, leaf_cap=1):
         """ps_calc_forces on arrays that are already sorted (``sort``).
         ``order`` 1 selects the closure's order-1 local expansion; ``feat``
-        (n x 16 float32) then receives the raw per-particle closure features."""
+        (n x 16 float32) then receives the raw per-particle closure features.
+        ``leaf_cap`` > 1 splits only nodes holding more particles than that
+        (the reference splits every node holding two or more)."""
         h = self.lib.pso_new()
         try:
+            if leaf_cap != 1:
+                self.lib.pso_set_leaf_cap(h, int(leaf_cap))
             if order or feat is not None:
                 assert feat is None or (feat.dtype == np.float32 and feat.shape == (p.n, 16))
                 self.lib.pso_set_closure(h, order, None if feat is None else _ptr(feat))
@@ -122,7 +127,7 @@ class Oracle:
             self.lib.pso_free(h)
 
     def tick(self, p, theta=2.0, variant=MORTON_AVX2, mt=True, accum_mode=0,
-             want_tree=True, want_p2p=False, order=0, feat=None):
+             want_tree=True, want_p2p=False, order=0, feat=None, leaf_cap=1):
         """prepare + calc on ``p`` in place (arrays end sorted, forces set)."""
         rc, codes, mn, mx, rg = self.prepare(p, variant)
         assert rc == 0
@@ -131,7 +136,7 @@ class Oracle:
         hw = f32(rg) / f32(2.0)
         self.sort(p, codes)
         out = self.calc(p, codes, float(c), float(c), float(c), float(hw), theta, mt,
-                        accum_mode, want_tree, want_p2p, order, feat)
+                        accum_mode, want_tree, want_p2p, order, feat, leaf_cap)
         out.update(codes=codes, min=mn, max=mx, range=rg, root_c=float(c), root_hw=float(hw))
         return out
 
@@ -143,13 +148,13 @@ class Oracle:
                                 _ptr(p.y), _ptr(p.z), _ptr(p.mass), _ptr(p.fx), _ptr(p.fy),
                                 _ptr(p.fz), dt, _ptr(tmp))
 
-    def run_ticks(self, p, vx, vy, vz, dt, ticks, theta=2.0):
+    def run_ticks(self, p, vx, vy, vz, dt, ticks, theta=2.0, leaf_cap=1):
         """``ticks`` iterations of README.md:65-111: ids reset, prepare +
         calc, velocity permutation, Euler.  Returns the last tick's codes."""
         codes = None
         for _ in range(ticks):
             p.id[:] = np.arange(p.n, dtype=np.uint32)
-            codes = self.tick(p, theta=theta, want_tree=False)["codes"]
+            codes = self.tick(p, theta=theta, want_tree=False, leaf_cap=leaf_cap)["codes"]
             self.euler_step(p, vx, vy, vz, dt)
         return codes
 

@@ -230,6 +230,7 @@ typedef struct {
     float        theta;
     int          accum_mode; /* 0: reference lane structure; 1: plain */
     int          order;      /* closure: 0 reference (order-0 local), 1 order-1 */
+    uint32_t     leaf_cap;   /* split nodes holding more than this (0 or 1: the reference) */
     float*       feat;       /* closure: raw per-particle features, 16 each */
 } pso_ctx_t;
 
@@ -271,7 +272,9 @@ static size_t pso_find_split(const uint32_t* codes, size_t lo, size_t hi,
 }
 
 /* ps_impl_build_tree (polesitter.h:906-967) done breadth-first: a node at
- * depth d is a leaf iff d == 10 or it holds <= 1 particle (:911-916);
+ * depth d is a leaf iff d == 10 or it holds <= 1 particle (:911-916) --
+ * <= leaf_cap particles with pso_set_leaf_cap, an extension that still
+ * splits a root holding two or more;
  * otherwise one child per non-empty octant of digit (code >> (27-3d)) & 7,
  * in octant order, centred at parent +/- hw/2 per axis bit (x = bit 0,
  * y = bit 1, z = bit 2) with hw_child = hw * 0.5 (:935-939). */
@@ -289,12 +292,13 @@ static void pso_build(pso_ctx_t* c, const uint32_t* codes, size_t n, float cx,
     r->parent = 0xFFFFFFFFu;
     r->octant = -1;
     c->level_start[0] = 0;
+    const uint32_t cap = c->leaf_cap > 1 ? c->leaf_cap : 1u;
     size_t lvl_lo = 0, lvl_hi = 1;
     for (int d = 0; d <= PSO_MAX_DEPTH; ++d) {
         c->level_start[d + 1] = (uint32_t)lvl_hi;
         for (size_t k = lvl_lo; k < lvl_hi; ++k) {
             pso_node_t p = c->nodes[k];
-            if (d == PSO_MAX_DEPTH || p.count <= 1) {
+            if (d == PSO_MAX_DEPTH || p.count <= (d == 0 ? 1u : cap)) {
                 c->nodes[k].nchild      = 0;
                 c->nodes[k].first_child = 0;
                 continue;
@@ -625,6 +629,13 @@ PSO_API void pso_set_closure(void* h, int order, float* feat) {
     pso_ctx_t* c = (pso_ctx_t*)h;
     c->order = order;
     c->feat  = feat;
+}
+
+/* leaf capacity of the next pso_calc's tree: nodes with more than `cap`
+ * particles are split (the reference: 1) */
+PSO_API void pso_set_leaf_cap(void* h, uint32_t cap) {
+    pso_ctx_t* c = (pso_ctx_t*)h;
+    c->leaf_cap = cap;
 }
 
 /* ps_calc_forces (polesitter.h:1840-1909) on arrays already sorted by

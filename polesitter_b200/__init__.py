@@ -26,6 +26,7 @@ RESULT_NAMES = {0: "PS_OK", -1: "PS_EOOM", -2: "PS_EINVAL", -3: "PS_ETHRD",
 
 OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN, OPT_CLOSURE, OPT_JUDGE = 1, 2, 4, 6, 7, 8
 OPT_HEAVY_DEPTH = 9
+OPT_LEAF_CAP = 10
 CLOSURE_PARAMS = 9928
 MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 
@@ -37,7 +38,9 @@ EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
             "ps_b200_closure_set_weights", "ps_b200_closure_last", "ps_b200_closure_features",
             "ps_b200_closure_correction", "ps_b200_closure_forward", "ps_b200_closure_grad",
             "ps_b200_closure_train", "ps_b200_ensemble_create", "ps_b200_ensemble_autotune",
-            "ps_b200_ensemble_run", "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy")
+            "ps_b200_ensemble_run", "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy",
+            "ps_b200_ensemble_leaf_caps", "ps_b200_ensemble_set_leaf_caps",
+            "ps_b200_ensemble_set_leaf_ladder")
 
 
 class ParticleArrs(C.Structure):
@@ -122,8 +125,13 @@ def lib() -> C.CDLL:
                                        C.c_uint32]
     L.ps_b200_ensemble_theta.argtypes = [vp, vp, sz]
     L.ps_b200_ensemble_destroy.argtypes = [vp]
+    L.ps_b200_ensemble_leaf_caps.argtypes = [vp, vp, sz]
+    L.ps_b200_ensemble_set_leaf_caps.argtypes = [vp, vp, sz]
+    L.ps_b200_ensemble_set_leaf_ladder.argtypes = [vp, vp, sz]
     for name in ("ps_b200_ensemble_create", "ps_b200_ensemble_autotune", "ps_b200_ensemble_run",
-                 "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy"):
+                 "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy",
+                 "ps_b200_ensemble_leaf_caps", "ps_b200_ensemble_set_leaf_caps",
+                 "ps_b200_ensemble_set_leaf_ladder"):
         getattr(L, name).restype = C.c_int
     L.ps_b200_run_ticks.restype = C.c_int
     L.ps_b200_run_ticks.argtypes = [vp, C.POINTER(ParticleArrs), vp, vp, vp, vp, f32, C.c_uint32]
@@ -389,6 +397,26 @@ class Ensemble:
         _check("ps_b200_ensemble_theta", lib().ps_b200_ensemble_theta(
             self.ptr, th.ctypes.data, len(th)))
         return th
+
+    def leaf_caps(self):
+        import numpy as np
+        caps = np.zeros(len(self.counts), np.uint32)
+        _check("ps_b200_ensemble_leaf_caps", lib().ps_b200_ensemble_leaf_caps(
+            self.ptr, caps.ctypes.data, len(caps)))
+        return caps
+
+    def set_leaf_caps(self, caps):
+        import numpy as np
+        c = np.ascontiguousarray(caps, np.uint32)
+        _check("ps_b200_ensemble_set_leaf_caps", lib().ps_b200_ensemble_set_leaf_caps(
+            self.ptr, c.ctypes.data, len(c)))
+
+    def set_leaf_ladder(self, caps):
+        """The leaf capacities ``autotune`` tries (default 1, 16, 32, 64)."""
+        import numpy as np
+        c = np.ascontiguousarray(caps, np.uint32)
+        _check("ps_b200_ensemble_set_leaf_ladder", lib().ps_b200_ensemble_set_leaf_ladder(
+            self.ptr, c.ctypes.data, len(c)))
 
     def destroy(self):
         if self.ptr:

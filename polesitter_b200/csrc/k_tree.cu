@@ -11,6 +11,16 @@
 // so the whole tree comes from one pass of flags and a 10-wide prefix scan,
 // with no recursion.  Levels are stored contiguously in Morton order.
 //
+// Leaf capacity B > 1 (an extension: nodes holding <= B particles are
+// leaves): "its parent run has >= 2" becomes "> B".  The depth-k runs
+// around i shrink as k grows, and the depth-k run holding i has > B
+// particles iff some window [j, j+B] containing i lies inside it, so a
+// depth-d node starts at i iff a depth-d run starts there and
+//     d - 1 <= W(i) = max over j in [i-B, i] of cpl2(codes[j], codes[j+B])
+// (cpl2 = common octal prefix length).  With B = 1 this is the rule above.
+// The root is split whenever it holds >= 2 particles, so every particle has
+// a leaf below the root (W(i) >= 0).
+//
 // Child centres follow the reference's float chain exactly (:935-939):
 // hw_child = hw * 0.5 and c_child = c_parent +/- hw_child, replayed from the
 // root for each node.
@@ -25,22 +35,27 @@ constexpr int kTreeTile = kTreeThreads * kTreePer;  // 1024 positions
 
 int tree_tile_size() { return kTreeTile; }
 
-__device__ __forceinline__ int cpl_at(const uint32_t* __restrict__ c, size_t i, size_t n) {
-    // common octal prefix length of codes[i-1], codes[i]; -1 outside [1, n)
-    if (i == 0 || i >= n) return -1;
-    uint32_t x = (c[i - 1] ^ c[i]) & 0x3FFFFFFFu;
+__device__ __forceinline__ int cpl2(uint32_t a, uint32_t b) {
+    // common octal prefix length of two codes (0 .. 10)
+    const uint32_t x = (a ^ b) & 0x3FFFFFFFu;
     if (x == 0u) return kMaxDepth;
     return (__clz(x) - 2) / 3;
 }
 
-// 10 one-bit flags (bit d-1 <=> a depth-d node starts at i)
-__device__ __forceinline__ uint32_t node_flags(int cpl_i, int cpl_next, bool first) {
+__device__ __forceinline__ int cpl_at(const uint32_t* __restrict__ c, size_t i, size_t n) {
+    // common octal prefix length of codes[i-1], codes[i]; -1 outside [1, n)
+    if (i == 0 || i >= n) return -1;
+    return cpl2(c[i - 1], c[i]);
+}
+
+// 10 one-bit flags (bit d-1 <=> a depth-d node starts at i); w = W(i), the
+// deepest level whose run around i holds more than the leaf capacity
+__device__ __forceinline__ uint32_t node_flags(int cpl_i, int w, bool first) {
     uint32_t f = 0;
 #pragma unroll
     for (int d = 1; d <= kMaxDepth; ++d) {
         bool start = first || cpl_i < d;
-        bool pge2 = (cpl_i >= d - 1) || (cpl_next >= d - 1);
-        if (start && pge2) f |= 1u << (d - 1);
+        if (start && w >= d - 1) f |= 1u << (d - 1);
     }
     return f;
 }
@@ -62,23 +77,50 @@ __device__ __forceinline__ uint32_t get_cnt(unsigned long long lo, unsigned long
 }
 
 __device__ __forceinline__ void thread_flags(const uint32_t* __restrict__ codes, size_t n,
-                                             size_t p0, uint32_t (&f)[kTreePer]) {
+                                             size_t p0, uint32_t cap,
+                                             uint32_t (&f)[kTreePer]) {
     int cprev = cpl_at(codes, p0, n);
+    if (cap <= 1u) {
+        // W(i) = max(cpl(i), cpl(i+1))
+#pragma unroll
+        for (int q = 0; q < kTreePer; ++q) {
+            size_t i = p0 + q;
+            int cnext = cpl_at(codes, i + 1, n);
+            f[q] = (i < n) ? node_flags(cprev, max(cprev, cnext), i == 0) : 0u;
+            cprev = cnext;
+        }
+        return;
+    }
+    // W over the windows [j, j + cap] with j in [p0 - cap, p0 + kTreePer - 1],
+    // 0 <= j and j + cap < n; at least 0 (the root is split) once n >= 2
+    int w[kTreePer];
+#pragma unroll
+    for (int q = 0; q < kTreePer; ++q) w[q] = n >= 2 ? 0 : -1;
+    const long long jlo = max(0ll, (long long)p0 - (long long)cap);
+    const long long jhi = min((long long)p0 + kTreePer - 1, (long long)n - 1 - (long long)cap);
+#pragma unroll 4
+    for (long long j = jlo; j <= jhi; ++j) {
+        const int c = cpl2(codes[j], codes[j + cap]);
+#pragma unroll
+        for (int q = 0; q < kTreePer; ++q) {
+            const long long i = (long long)p0 + q;
+            if (j <= i && j + (long long)cap >= i) w[q] = max(w[q], c);
+        }
+    }
 #pragma unroll
     for (int q = 0; q < kTreePer; ++q) {
         size_t i = p0 + q;
-        int cnext = cpl_at(codes, i + 1, n);
-        f[q] = (i < n) ? node_flags(cprev, cnext, i == 0) : 0u;
-        cprev = cnext;
+        f[q] = (i < n) ? node_flags(cprev, w[q], i == 0) : 0u;
+        cprev = cpl_at(codes, i + 1, n);
     }
 }
 
 __global__ void __launch_bounds__(kTreeThreads) k_tree_count(const uint32_t* __restrict__ codes,
-                                                            size_t n,
+                                                            size_t n, uint32_t cap,
                                                             uint32_t* __restrict__ tile_cnt) {
     const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
     uint32_t f[kTreePer];
-    thread_flags(codes, n, p0, f);
+    thread_flags(codes, n, p0, cap, f);
     unsigned long long lo = 0, hi = 0;
 #pragma unroll
     for (int q = 0; q < kTreePer; ++q) add_flags(lo, hi, f[q]);
@@ -174,7 +216,8 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
                                                            TreeView tv, const Status* status,
                                                            float cx, float cy, float cz,
                                                            float hw,
-                                                           const float* __restrict__ bbox) {
+                                                           const float* __restrict__ bbox,
+                                                           uint32_t cap) {
     if (bbox) {
         // root from a device-side bounding box (min, max, range), as the
         // caller's loop derives it: c = min + range / 2, hw = range / 2
@@ -184,7 +227,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
     }
     const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
     uint32_t f[kTreePer];
-    thread_flags(codes, n, p0, f);
+    thread_flags(codes, n, p0, cap, f);
     unsigned long long lo = 0, hi = 0;
 #pragma unroll
     for (int q = 0; q < kTreePer; ++q) add_flags(lo, hi, f[q]);
@@ -328,12 +371,12 @@ __global__ void __launch_bounds__(256) k_upward_level(TreeView tv, const Status*
 
 void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView tv,
                  Status* status, float cx, float cy, float cz, float hw, int grid,
-                 cudaStream_t st, const float* bbox) {
+                 cudaStream_t st, const float* bbox, uint32_t leaf_cap) {
     const int tiles = (int)((n + kTreeTile - 1) / kTreeTile);
-    k_tree_count<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf);
+    k_tree_count<<<tiles, kTreeThreads, 0, st>>>(codes, n, leaf_cap, tile_buf);
     k_tree_scan<<<1, 1024, 0, st>>>(tile_buf, tiles, tv, status);
     k_tree_emit<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf, tv, status, cx, cy, cz, hw,
-                                                bbox);
+                                                bbox, leaf_cap);
     k_tree_link<<<grid, 256, 0, st>>>(tv, status);
 }
 

@@ -102,6 +102,9 @@ int psg_ensemble_run(void* ens, const psg_arrays_t* a, float* vx, float* vy, flo
 int psg_ensemble_autotune(void* ens, const psg_arrays_t* a, float target, float* theta_out,
                           double* grid_scale_out);
 int psg_ensemble_systems(void* ens, float* theta_out, size_t n);
+int psg_ensemble_leaf_caps(void* ens, uint32_t* cap_out, size_t n);
+/* ladder != 0: the leaf capacities the autotuner tries; else one per system */
+int psg_ensemble_set_leaf_caps(void* ens, const uint32_t* caps, size_t n, int ladder);
 const char* psg_last_error(void);
 void psg_set_error(const char* msg);
 
@@ -118,6 +121,8 @@ int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n
 #define PSG_OPT_CLOSURE 7        /* 0 reference, 1 order-1 local, 2 + learned correction */
 #define PSG_OPT_JUDGE 8          /* 1: sampled FP64 judge in closure mode 1 too */
 #define PSG_OPT_HEAVY_DEPTH 9    /* leaves this shallow walk block-parallel (-1: from theta) */
+#define PSG_OPT_LEAF_CAP 10      /* split nodes holding more particles than this (1..256) */
+#define PSG_MAX_LEAF_CAP 256
 
 /* the learned far-field closure (k_closure.cu) */
 #define PSG_CLOSURE_PARAMS 9928

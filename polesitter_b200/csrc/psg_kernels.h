@@ -39,7 +39,7 @@ void launch_writeback(const float4* xyzm, const uint32_t* ids, size_t n, float* 
 int tree_tile_size();
 void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView tv,
                  Status* status, float cx, float cy, float cz, float hw, int grid,
-                 cudaStream_t st, const float* bbox = nullptr);
+                 cudaStream_t st, const float* bbox = nullptr, uint32_t leaf_cap = 1);
 void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int grid,
                    cudaStream_t st);
 

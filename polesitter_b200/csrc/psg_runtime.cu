@@ -107,6 +107,7 @@ struct State {
     cudaStream_t aux;      // k_heavy_leaf, beside the leaf pass
     cudaEvent_t ev_levels, ev_heavy;
     int heavy_depth;       // option; < 0: derived from theta
+    uint32_t leaf_cap;     // option: nodes holding more particles are split (1: the reference)
     double grid_scale;     // traversal grids x this (ensemble autotuner); 0: 1
     int kahan;
     Status* d_status;
@@ -305,6 +306,7 @@ static int init_state(State* s, size_t maxp, float theta) {
     r = alloc_heavy(s, (uint32_t)(n / 4 + 4096));
     if (r != PSG_OK) return r;
     s->heavy_depth = -1;
+    s->leaf_cap = 1;
     PSG_CHECK(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
     PSG_CHECK(cudaEventCreateWithFlags(&s->ev_levels, cudaEventDisableTiming));
     PSG_CHECK(cudaEventCreateWithFlags(&s->ev_heavy, cudaEventDisableTiming));
@@ -350,6 +352,7 @@ static int closure_alloc(State* s) {
 // sources within about theta H / 2^(d-1), a large part of the tree once
 // 2^d <= 4 theta.
 static int heavy_depth_for(const State* s) {
+    if (s->leaf_cap > 1) return 0;  // k_heavy_leaf walks one-particle leaves only
     if (s->heavy_depth >= 0) return s->heavy_depth > 5 ? 5 : s->heavy_depth;
     int d = 0;
     while (d < 5 && (float)(2 << d) <= 4.0f * s->theta) ++d;
@@ -563,7 +566,8 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
         PSG_CHECK(cudaMemsetAsync(s->tv.dbg_m2l, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
         PSG_CHECK(cudaMemsetAsync(s->tv.dbg_p2p, 0, (size_t)s->tv.lvl_base[kLevels] * 4, st));
     }
-    launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, cx, cy, cz, hw, gt, st, bbox);
+    launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, cx, cy, cz, hw, gt, st, bbox,
+                s->leaf_cap);
     record(s, PH_TREE);
     launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
     record(s, PH_UP);
@@ -830,6 +834,7 @@ struct Ensemble {
     float* vtmp = nullptr;    // 3 x total velocity scratch
     double grid_scale = 1.0;
     int variant = PSG_MORTON_AVX2;
+    std::vector<uint32_t> leaf_ladder{1u, 16u, 32u, 64u};  // leaf capacities the autotuner tries
 };
 
 static int ensure_tick_scratch(State* s) {
@@ -864,7 +869,7 @@ static int enqueue_system_forces(State* s, const DevArrays& d, size_t n, int var
     launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
     const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
     launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, 0.f, 0.f, 0.f, 0.f, gt, st,
-                s->tk_bbox);
+                s->tk_bbox, s->leaf_cap);
     launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
     if (n > 1) {
         int r = enqueue_traversal(s, s->xyzm, d.fx, d.fy, d.fz);
@@ -1114,6 +1119,7 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
     std::vector<int> cls(e->nsys);
     for (size_t k = 0; k < e->nsys; ++k) cls[k] = (int)std::floor(std::log2((double)e->count[k] + 1));
     std::vector<float> chosen(e->nsys, 0.f);
+    std::vector<uint32_t> chosen_cap(e->nsys, 1u);
     uint32_t* d_tg = nullptr;
     double* d_f64 = nullptr;
     const size_t kSample = 1024;
@@ -1121,55 +1127,112 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
     PSG_ALLOC(d_f64, kSample * 3 * sizeof(double));
     std::vector<uint32_t> tg(kSample);
     std::vector<double> f64(kSample * 3);
-    std::vector<float> fx(kSample), fy(kSample), fz(kSample);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PSG_CHECK(cudaEventCreate(&e0));
+    PSG_CHECK(cudaEventCreate(&e1));
+    // one tick of system k from the saved state at its current theta and
+    // leaf capacity; *ms = its device time
+    auto one_tick = [&](State* s, const DevArrays& ck, size_t n, float* ms) -> int {
+        int rr = restore();
+        if (rr != PSG_OK) return rr;
+        PSG_CHECK(cudaEventRecord(e0, s->stream));
+        launch_tick_reset_ids(ck.id, n, grid_for(s, n, 1024), s->stream);
+        int gp = (int)((n + 1023) / 1024);
+        if (gp > s->tk_grid) gp = s->tk_grid;
+        launch_prepare(ck.x, ck.y, ck.z, n, s->tk_partial, gp, ck.codes, s->tk_bbox,
+                       e->variant, s->stream);
+        rr = tick_core(s, ck, n, 0.f, 0.f, 0.f, 0.f, s->tk_bbox);
+        if (rr != PSG_OK) return rr;
+        PSG_CHECK(cudaEventRecord(e1, s->stream));
+        PSG_CHECK(cudaEventSynchronize(e1));
+        PSG_CHECK(cudaEventElapsedTime(ms, e0, e1));
+        return PSG_OK;
+    };
+    // median relative force error of that tick on kSample particles
+    auto median_error = [&](State* s, const DevArrays& ck, size_t n, double* med) -> int {
+        const size_t ns = n < kSample ? n : kSample;
+        for (size_t i = 0; i < ns; ++i) tg[i] = (uint32_t)(i * n / ns);
+        PSG_CHECK(cudaMemcpyAsync(d_tg, tg.data(), ns * 4, cudaMemcpyHostToDevice, s->stream));
+        launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, s->sms * 8, s->stream);
+        PSG_CHECK(cudaMemcpyAsync(f64.data(), d_f64, ns * 3 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s->stream));
+        std::vector<float> hf[3] = {std::vector<float>(n), std::vector<float>(n),
+                                    std::vector<float>(n)};
+        PSG_CHECK(cudaMemcpyAsync(hf[0].data(), ck.fx, n * 4, cudaMemcpyDeviceToHost, s->stream));
+        PSG_CHECK(cudaMemcpyAsync(hf[1].data(), ck.fy, n * 4, cudaMemcpyDeviceToHost, s->stream));
+        PSG_CHECK(cudaMemcpyAsync(hf[2].data(), ck.fz, n * 4, cudaMemcpyDeviceToHost, s->stream));
+        PSG_CHECK(cudaStreamSynchronize(s->stream));
+        std::vector<double> rel(ns);
+        for (size_t i = 0; i < ns; ++i) {
+            const double gx = f64[3 * i], gy = f64[3 * i + 1], gz = f64[3 * i + 2];
+            const double ex = hf[0][tg[i]] - gx, ey = hf[1][tg[i]] - gy, ez = hf[2][tg[i]] - gz;
+            const double nr = std::sqrt(gx * gx + gy * gy + gz * gz);
+            rel[i] = nr > 0 ? std::sqrt(ex * ex + ey * ey + ez * ez) / nr : 0.0;
+        }
+        std::nth_element(rel.begin(), rel.begin() + ns / 2, rel.end());
+        *med = rel[ns / 2];
+        return PSG_OK;
+    };
     for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
         if (chosen[k] > 0.f) continue;
         State* s = e->sys[k];
         const size_t n = e->count[k];
         const DevArrays ck = slice(c, e->offset[k]);
-        float pick = ladder[nl - 1];
-        for (int li = 0; li < nl && r == PSG_OK; ++li) {
-            if ((r = restore()) != PSG_OK) break;
-            s->theta = ladder[li];
-            launch_tick_reset_ids(ck.id, n, grid_for(s, n, 1024), s->stream);
-            int gp = (int)((n + 1023) / 1024);
-            if (gp > s->tk_grid) gp = s->tk_grid;
-            launch_prepare(ck.x, ck.y, ck.z, n, s->tk_partial, gp, ck.codes, s->tk_bbox,
-                           e->variant, s->stream);
-            r = tick_core(s, ck, n, 0.f, 0.f, 0.f, 0.f, s->tk_bbox);
-            if (r != PSG_OK) break;
-            const size_t ns = n < kSample ? n : kSample;
-            for (size_t i = 0; i < ns; ++i) tg[i] = (uint32_t)(i * n / ns);
-            PSG_CHECK(cudaMemcpyAsync(d_tg, tg.data(), ns * 4, cudaMemcpyHostToDevice, s->stream));
-            launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, s->sms * 8, s->stream);
-            PSG_CHECK(cudaMemcpyAsync(f64.data(), d_f64, ns * 3 * sizeof(double),
-                                      cudaMemcpyDeviceToHost, s->stream));
-            std::vector<float> hf[3] = {std::vector<float>(n), std::vector<float>(n),
-                                        std::vector<float>(n)};
-            PSG_CHECK(cudaMemcpyAsync(hf[0].data(), ck.fx, n * 4, cudaMemcpyDeviceToHost, s->stream));
-            PSG_CHECK(cudaMemcpyAsync(hf[1].data(), ck.fy, n * 4, cudaMemcpyDeviceToHost, s->stream));
-            PSG_CHECK(cudaMemcpyAsync(hf[2].data(), ck.fz, n * 4, cudaMemcpyDeviceToHost, s->stream));
-            PSG_CHECK(cudaStreamSynchronize(s->stream));
-            std::vector<double> rel(ns);
-            for (size_t i = 0; i < ns; ++i) {
-                const double gx = f64[3 * i], gy = f64[3 * i + 1], gz = f64[3 * i + 2];
-                const double ex = hf[0][tg[i]] - gx, ey = hf[1][tg[i]] - gy, ez = hf[2][tg[i]] - gz;
-                const double nr = std::sqrt(gx * gx + gy * gy + gz * gz);
-                rel[i] = nr > 0 ? std::sqrt(ex * ex + ey * ey + ez * ez) / nr : 0.0;
+        // per leaf capacity: the smallest theta meeting the target, then the
+        // time of one tick there; the fastest that meets it wins (none
+        // meets it: the smallest error at the largest theta)
+        bool best_met = false;
+        double best_ms = 1e300, best_err = 1e300;
+        float best_theta = ladder[nl - 1];
+        uint32_t best_cap = e->leaf_ladder.empty() ? 1u : e->leaf_ladder[0];
+        for (uint32_t cap : e->leaf_ladder) {
+            s->leaf_cap = cap;
+            float pick = ladder[nl - 1];
+            double err = 1e300;
+            bool met = false;
+            float ms = 0.f;
+            for (int li = 0; li < nl && r == PSG_OK; ++li) {
+                s->theta = ladder[li];
+                if ((r = one_tick(s, ck, n, &ms)) != PSG_OK) break;
+                if ((r = median_error(s, ck, n, &err)) != PSG_OK) break;
+                if (err <= (double)target) {
+                    pick = ladder[li];
+                    met = true;
+                    break;
+                }
             }
-            std::nth_element(rel.begin(), rel.begin() + ns / 2, rel.end());
-            if (rel[ns / 2] <= (double)target) {
-                pick = ladder[li];
-                break;
+            if (r != PSG_OK) break;
+            // the stores have grown for this (theta, cap): time a clean tick
+            s->theta = pick;
+            if ((r = one_tick(s, ck, n, &ms)) != PSG_OK) break;
+            const bool better = (met && !best_met) ||
+                                (met == best_met && (met ? ms < best_ms : err < best_err));
+            if (better) {
+                best_met = met;
+                best_ms = ms;
+                best_err = err;
+                best_theta = pick;
+                best_cap = cap;
             }
         }
-        for (size_t j = 0; j < e->nsys; ++j)
-            if (cls[j] == cls[k]) chosen[j] = pick;
+        s->leaf_cap = best_cap;
+        s->theta = best_theta;
+        for (size_t j = 0; j < e->nsys; ++j) {
+            if (cls[j] == cls[k]) {
+                chosen[j] = best_theta;
+                chosen_cap[j] = best_cap;
+            }
+        }
     }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     cudaFree(d_tg);
     cudaFree(d_f64);
     if (r == PSG_OK) {
-        for (size_t k = 0; k < e->nsys; ++k) e->sys[k]->theta = chosen[k];
+        for (size_t k = 0; k < e->nsys; ++k) {
+            e->sys[k]->theta = chosen[k];
+            e->sys[k]->leaf_cap = chosen_cap[k];
+        }
         // launch shape: one forces replay of the copies per grid scale
         static const double scales[] = {1.0, 0.5, 0.25};
         float* vdummy[3] = {c.fx, c.fy, c.fz};
@@ -1281,6 +1344,11 @@ int psg_set_option(void* mem, int key, double value) {
         case PSG_OPT_HEAVY_DEPTH:
             if (value > 5) return PSG_EINVAL;
             s->heavy_depth = value < 0 ? -1 : (int)value;
+            return PSG_OK;
+        case PSG_OPT_LEAF_CAP:
+            if (value < 1 || value > PSG_MAX_LEAF_CAP || (double)(int)value != value)
+                return PSG_EINVAL;
+            s->leaf_cap = (uint32_t)value;
             return PSG_OK;
         default: return PSG_EINVAL;
     }
@@ -1437,6 +1505,28 @@ int psg_ensemble_systems(void* h, float* theta_out, size_t n) {
     psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
     if (!e || e->magic != psg::kEnsMagic || !theta_out || n != e->nsys) return PSG_EINVAL;
     for (size_t k = 0; k < n; ++k) theta_out[k] = e->sys[k]->theta;
+    return PSG_OK;
+}
+
+int psg_ensemble_leaf_caps(void* h, uint32_t* cap_out, size_t n) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || !cap_out || n != e->nsys) return PSG_EINVAL;
+    for (size_t k = 0; k < n; ++k) cap_out[k] = e->sys[k]->leaf_cap;
+    return PSG_OK;
+}
+
+int psg_ensemble_set_leaf_caps(void* h, const uint32_t* caps, size_t n, int ladder) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || !caps || n == 0) return PSG_EINVAL;
+    for (size_t k = 0; k < n; ++k)
+        if (caps[k] < 1u || caps[k] > (uint32_t)PSG_MAX_LEAF_CAP) return PSG_EINVAL;
+    if (ladder) {
+        e->leaf_ladder.assign(caps, caps + n);
+        return PSG_OK;
+    }
+    if (n != e->nsys) return PSG_EINVAL;
+    for (size_t k = 0; k < n; ++k) e->sys[k]->leaf_cap = caps[k];
+    e->dirty = true;
     return PSG_OK;
 }
 

@@ -330,6 +330,29 @@ ps_result_t ps_b200_ensemble_theta(ps_b200_ensemble_t* ens, float* theta_out, si
     return to_ps(psg_ensemble_systems(ens, theta_out, n));
 }
 
+ps_result_t ps_b200_ensemble_leaf_caps(ps_b200_ensemble_t* ens, uint32_t* cap_out, size_t n) {
+    if (!ens) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_leaf_caps(ens, cap_out, n));
+}
+
+ps_result_t ps_b200_ensemble_set_leaf_caps(ps_b200_ensemble_t* ens, const uint32_t* caps,
+                                           size_t n) {
+    if (!ens) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_set_leaf_caps(ens, caps, n, 0));
+}
+
+ps_result_t ps_b200_ensemble_set_leaf_ladder(ps_b200_ensemble_t* ens, const uint32_t* caps,
+                                             size_t n) {
+    if (!ens) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_set_leaf_caps(ens, caps, n, 1));
+}
+
 ps_result_t ps_b200_ensemble_destroy(ps_b200_ensemble_t* ens) {
     if (!ens) {
         return PS_EINVAL;

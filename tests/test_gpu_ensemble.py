@@ -2,9 +2,10 @@
 
 Many independent systems advanced together in replayed CUDA graphs must give
 exactly what each system gives on its own: the same sorted positions, ids,
-forces and velocities as ps_b200_run_ticks per system with the same theta,
-bit for bit.  The autotuner must leave the state untouched and choose, per
-size class, a theta whose error meets its target."""
+forces and velocities as ps_b200_run_ticks per system with the same theta
+and leaf capacity, bit for bit.  The autotuner must leave the state
+untouched and choose, per size class, a theta and leaf capacity whose error
+meets its target."""
 
 from __future__ import annotations
 
@@ -37,7 +38,9 @@ def _part(p, a, b):
     return q
 
 
-def test_ensemble_equals_each_system_alone():
+@pytest.mark.parametrize("caps", [None, [1, 16, 32, 1, 64, 8, 2, 16, 16]],
+                         ids=["leaf1", "mixed_leaf_caps"])
+def test_ensemble_equals_each_system_alone(caps):
     torch = pytest.importorskip("torch")
     counts, p, vx, vy, vz = W.ensemble(7, 3, n_min=64, n_max=40000)
     counts = np.concatenate([counts, [1, 2]])  # tiny systems too
@@ -52,6 +55,9 @@ def test_ensemble_equals_each_system_alone():
     v = [torch.from_numpy(a.copy()).cuda() for a in (vx, vy, vz)]
     codes = torch.zeros(p.n, dtype=torch.int32, device="cuda")
     with P.Ensemble(counts, theta) as ens:
+        if caps is not None:
+            ens.set_leaf_caps(caps)
+            assert np.array_equal(ens.leaf_caps(), caps)
         ens.run(d, codes, *v, 1e-3, 3)
     torch.cuda.synchronize()
     for k in range(len(counts)):
@@ -59,6 +65,8 @@ def test_ensemble_equals_each_system_alone():
         q = _part(p, a, b)
         vk = [vx[a:b].copy(), vy[a:b].copy(), vz[a:b].copy()]
         with P.Context(int(b - a), theta=float(theta[k])) as ctx:
+            if caps is not None:
+                ctx.set_option(P.OPT_LEAF_CAP, caps[k])
             ctx.run_ticks(q, np.zeros(b - a, np.uint32), *vk, 1e-3, 3)
         for key in KEYS:
             assert np.array_equal(getattr(d, key)[a:b].cpu().numpy(), getattr(q, key)), (k, key)
@@ -76,6 +84,8 @@ def test_autotune_meets_target_and_leaves_state():
     target = 3e-2
     with P.Ensemble(counts) as ens:
         theta, scale = ens.autotune(d, codes, target)
+        caps = ens.leaf_caps()
+        assert set(caps.tolist()) <= {1, 16, 32, 64}
         assert np.array_equal(ens.theta(), theta)
         for k, v in before.items():
             assert torch.equal(getattr(d, k), v), k
@@ -90,12 +100,28 @@ def test_autotune_meets_target_and_leaves_state():
         a, b = offs[k], offs[k + 1]
         q = _part(p, a, b)
         with P.Context(int(b - a), theta=float(theta[k])) as ctx:
+            ctx.set_option(P.OPT_LEAF_CAP, int(caps[k]))
             ctx.tick(q, np.zeros(b - a, np.uint32))
             tg = np.arange(0, b - a, max(1, (b - a) // 512), dtype=np.uint32)
             f64 = ctx.direct_f64(q, tg)
         F = np.stack([q.fx, q.fy, q.fz], 1)[tg].astype(np.float64)
         err = np.median(np.linalg.norm(F - f64, axis=1) / np.linalg.norm(f64, axis=1))
         assert err <= 1.5 * target or theta[k] == 8.0, (k, theta[k], err)
+
+
+def test_autotune_leaf_ladder_of_one_keeps_the_reference_tree():
+    torch = pytest.importorskip("torch")
+    counts, p, vx, vy, vz = W.ensemble(3, 6, n_min=2048, n_max=8000)
+    d = _device(torch, p)
+    codes = torch.zeros(p.n, dtype=torch.int32, device="cuda")
+    with P.Ensemble(counts) as ens:
+        ens.set_leaf_ladder([1])
+        ens.autotune(d, codes, 3e-2)
+        assert np.all(ens.leaf_caps() == 1)
+        with pytest.raises(P.PolesitterError):
+            ens.set_leaf_ladder([0])
+        with pytest.raises(P.PolesitterError):
+            ens.set_leaf_caps([16])  # one per system
 
 
 def test_ensemble_rejects_host_arrays_and_wrong_sizes():

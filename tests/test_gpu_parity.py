@@ -23,12 +23,14 @@ FORCE_REL_MAX = 1e-4
 TOPO = ("depth", "start", "count", "nchild", "octant")
 
 
-def gpu_tick(p, theta, debug=True, kahan=False, max_particles=None):
+def gpu_tick(p, theta, debug=True, kahan=False, max_particles=None, leaf_cap=1):
     with P.Context(max_particles or p.n, theta=theta) as ctx:
         if debug:
             ctx.set_option(P.OPT_DEBUG, 1)
         if kahan:
             ctx.set_option(P.OPT_KAHAN, 1)
+        if leaf_cap != 1:
+            ctx.set_option(P.OPT_LEAF_CAP, leaf_cap)
         codes = np.zeros(p.n, np.uint32)
         mn, mx, rg = ctx.tick(p, codes)
         return {"codes": codes, "bbox": np.array([mn, mx, rg], np.float32),
@@ -81,10 +83,10 @@ CASES = [
 ]
 
 
-def _vs_oracle(oracle, p, theta):
+def _vs_oracle(oracle, p, theta, leaf_cap=1, per_particle=FORCE_REL_MAX):
     a, b = p.copy(), p.copy()
-    ro = oracle.tick(a, theta=theta)
-    rg = gpu_tick(b, theta)
+    ro = oracle.tick(a, theta=theta, leaf_cap=leaf_cap)
+    rg = gpu_tick(b, theta, leaf_cap=leaf_cap)
     assert np.array_equal(rg["codes"], ro["codes"])
     assert np.array_equal(b.id, a.id)
     t, o = rg["tree"], ro["tree"]
@@ -99,7 +101,7 @@ def _vs_oracle(oracle, p, theta):
     assert rg["stats"]["m2l_pairs"] == ro["stats"]["m2l_pairs"]
     assert rg["stats"]["p2p_pairs"] == ro["stats"]["p2p_pairs"]
     assert rel_l2(t["local_exp"], o["l_tot"]) < FORCE_REL_L2
-    assert_forces_close(forces(b), forces(a))
+    assert_forces_close(forces(b), forces(a), mx=per_particle)
     return rg, ro
 
 
@@ -112,6 +114,50 @@ def test_plummer_1m_full_size(oracle):
     # the benchmark workload itself: N = 2^20 Plummer, theta = 2
     rg, ro = _vs_oracle(oracle, W.plummer(1 << 20, 42), 2.0)
     assert ro["stats"]["m2l_pairs"] > 100_000_000
+
+
+LEAF_CAP_CASES = [
+    ("plummer65536_b16", lambda: W.plummer(65536, 3), 2.0, 16),
+    ("plummer65536_b64", lambda: W.plummer(65536, 3), 4.0, 64),
+    ("clumpy20000_b8", lambda: W.clumpy_plummer(20000, 3), 2.0, 8),
+    ("clumpy20000_b32", lambda: W.clumpy_plummer(20000, 3), 6.0, 32),
+    ("ragged12345_b2", lambda: W.uniform_cube(12345, 6), 2.0, 2),
+    ("clusters4096_b256", lambda: W.lcg_two_clusters(4096), 1.0, 256),
+]
+
+
+@pytest.mark.parametrize("name,gen,theta,cap", LEAF_CAP_CASES,
+                         ids=[c[0] for c in LEAF_CAP_CASES])
+def test_leaf_capacity_vs_oracle(oracle, name, gen, theta, cap):
+    # PS_B200_OPT_LEAF_CAP: the same bar as the reference's leaf capacity 1,
+    # except per particle: a particle's P2P sum now runs over thousands of
+    # sources, summed in another order than the oracle's, so a particle whose
+    # net force nearly cancels can differ by more than 1e-4 relative
+    rg, ro = _vs_oracle(oracle, gen(), theta, leaf_cap=cap, per_particle=1e-3)
+    t = rg["tree"]
+    leaf = t["nchild"] == 0
+    assert t["count"][leaf & (t["depth"] < 10) & (t["depth"] > 0)].max() <= cap
+    assert t["count"][~leaf & (t["depth"] > 0)].min() > cap
+
+
+@pytest.mark.parametrize("n,cap", [(2, 16), (3, 16), (17, 16), (16, 16), (40, 64)])
+def test_leaf_capacity_tiny_counts(oracle, n, cap):
+    # a root holding <= cap particles is still split
+    p = W.uniform_cube(n, 300 + n)
+    a, b = p.copy(), p.copy()
+    oracle.tick(a, theta=2.0, leaf_cap=cap)
+    gpu_tick(b, 2.0, leaf_cap=cap)
+    assert np.array_equal(a.id, b.id)
+    assert_forces_close(forces(b), forces(a))
+
+
+def test_leaf_capacity_option_bounds():
+    with P.Context(64) as ctx:
+        for bad in (0, -1, 257, 2.5):
+            with pytest.raises(P.PolesitterError):
+                ctx.set_option(P.OPT_LEAF_CAP, bad)
+        ctx.set_option(P.OPT_LEAF_CAP, 256)
+        ctx.set_option(P.OPT_LEAF_CAP, 1)
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 8, 9, 17])

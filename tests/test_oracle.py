@@ -266,3 +266,65 @@ def test_bf16_rounding_is_round_to_nearest_even():
     vals = np.array([one, one + ulp / 2, one + ulp / 2 + ulp / 8, one + 1.5 * ulp], np.float32)
     got = CO.bf16(vals)
     assert got.tolist() == [1.0, 1.0, float(one + ulp), float(one + 2 * ulp)]
+
+
+def _starts_by_window_rule(codes, cap):
+    """Node starts per depth from sorted codes by the flag rule the GPU tree
+    build uses: a depth-d node starts at i iff a depth-d run starts there
+    and d - 1 <= W(i) = max over j in [i-cap, i] of cpl2(codes[j], codes[j+cap]),
+    with W >= 0 (the root is split) once n >= 2."""
+    c = codes.astype(np.int64) & 0x3FFFFFFF
+    n = len(c)
+
+    def cpl2(a, b):
+        x = a ^ b
+        out = np.full(x.shape, 10, np.int64)
+        nz = x != 0
+        out[nz] = (29 - np.floor(np.log2(x[nz])).astype(np.int64)) // 3
+        return out
+
+    cpl = np.full(n, -1, np.int64)
+    cpl[1:] = cpl2(c[:-1], c[1:])
+    w = np.full(n, 0 if n >= 2 else -1, np.int64)
+    if n > cap:
+        wj = cpl2(c[: n - cap], c[cap:])  # window starting at j
+        for i in range(n):
+            lo, hi = max(0, i - cap), min(i, n - 1 - cap)
+            if lo <= hi:
+                w[i] = max(w[i], wj[lo:hi + 1].max())
+    out = {}
+    for d in range(1, 11):
+        start = (cpl < d)
+        start[0] = True
+        out[d] = np.nonzero(start & (w >= d - 1))[0]
+    return out
+
+
+@pytest.mark.parametrize("cap", [1, 2, 5, 16, 64])
+def test_leaf_capacity_start_rule_matches_the_split_recursion(oracle, cap):
+    # the GPU's one-pass flag rule against the oracle's recursive splitting
+    p = W.clumpy_plummer(3000, 11)
+    r = oracle.tick(p, theta=2.0, leaf_cap=cap)
+    t = r["tree"]
+    rule = _starts_by_window_rule(r["codes"], cap)
+    for d in range(1, 11):
+        got = np.sort(t["start"][t["depth"] == d])
+        assert np.array_equal(got, rule[d]), d
+
+
+def test_leaf_capacity_tree_shape(oracle):
+    p = W.plummer(4000, 12)
+    base = oracle.tick(p.copy(), theta=2.0)
+    one = oracle.tick(p.copy(), theta=2.0, leaf_cap=1)
+    assert np.array_equal(base["tree"]["start"], one["tree"]["start"])
+    for cap in (8, 32):
+        t = oracle.tick(p.copy(), theta=2.0, leaf_cap=cap)["tree"]
+        leaf = t["nchild"] == 0
+        below = t["depth"] > 0
+        assert t["count"][leaf & below & (t["depth"] < 10)].max() <= cap
+        assert t["count"][~leaf & below].min() > cap
+        assert t["nchild"][0] > 0
+    # a root holding fewer than cap particles is split all the same
+    q = W.uniform_cube(5, 1)
+    t = oracle.tick(q, theta=2.0, leaf_cap=16)["tree"]
+    assert t["nchild"][0] > 0 and np.all(t["nchild"][1:] == 0)
