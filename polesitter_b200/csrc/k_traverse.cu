@@ -933,7 +933,9 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
 // candidates at one level is tested by all threads (separated: M2L, leaf:
 // P2P, else: its children go to the next frontier, placed by a block scan).
 // Frontier order and the final reduction are fixed, so the result does not
-// depend on scheduling.  Shallow leaves (depth < 10) hold one particle.
+// depend on scheduling.  A one-particle leaf sums its P2P during the walk; a
+// leaf holding more (leaf capacity > 1) lists its P2P sources in frontier
+// order and sums them per particle afterwards.
 constexpr int kHeavyThreads = 512;
 constexpr int kHeavyWarps = kHeavyThreads / 32;
 
@@ -959,6 +961,8 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
     __shared__ uint32_t s_w[kHeavyWarps];
     __shared__ uint32_t s_rec;
     __shared__ float s_red[kHeavyWarps][12];
+    __shared__ float4 s_g[2];  // multi-particle leaf: field gradient (xx yy zz xy), local field
+    __shared__ float2 s_g1;
     __shared__ unsigned long long s_cnt[kHeavyWarps][3];
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_HEAVY_OVERFLOW)) return;
@@ -973,8 +977,9 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
     if (total == 0) return;
     const uint32_t tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
     const float theta2 = __fmul_rn(A.theta, A.theta);
-    uint32_t* fa = A.heavy_frontier + (size_t)blockIdx.x * 2 * A.heavy_fcap;
+    uint32_t* fa = A.heavy_frontier + (size_t)blockIdx.x * 3 * A.heavy_fcap;
     uint32_t* fb = fa + A.heavy_fcap;
+    uint32_t* const fp = fa + 2 * (size_t)A.heavy_fcap;  // P2P sources of a multi-particle leaf
     uint32_t leaves = 0, pid = 0, dp = 0, fc = 0;  // current group's leaf children
     for (;;) {
         if (leaves == 0) {
@@ -999,6 +1004,8 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
         const float4 ug = tv.geo[u];
         const uint4 ui = tv.info[u];
         const float4 t = A.xyzm[ui.x];
+        const bool multi = ui.y > 1u;  // the same for the whole block
+        uint32_t np2p = 0;
         // initial candidates: cand(p)
         uint32_t F = 0;
         if (dp <= 1) {
@@ -1035,9 +1042,9 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
             uint32_t Fn = 0;
             for (uint32_t i0 = 0; i0 < F; i0 += kHeavyThreads) {
                 const uint32_t i = i0 + tid;
-                uint32_t c = 0, link = 0;
+                uint32_t c = 0, link = 0, pf = 0, sn = 0;
                 if (i < F) {
-                    const uint32_t sn = fa[i];
+                    sn = fa[i];
                     const float4 sg = tv.geo[sn];
                     float dx, dy, dz, d2;
                     if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w, theta2, dx,
@@ -1065,12 +1072,26 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
                         c = link >> 28;
                         if (c == 0) {  // leaf x leaf: P2P
                             const uint4 si = tv.info[sn];
-                            p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz, cx,
-                                      cy, cz);
+                            if (multi) {
+                                pf = 1;
+                            } else {
+                                p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz,
+                                          cx, cy, cz);
+                            }
                             ++n_p2p;
-                            n_inter += si.y;
+                            n_inter += (unsigned long long)si.y * ui.y;
                         }
                     }
+                }
+                if (multi) {
+                    uint32_t pex;
+                    const uint32_t ptot = block_scan(pf, pex, s_w);
+                    if (np2p + ptot > A.heavy_fcap) {
+                        if (tid == 0) set_err(status, PSG_ERR_HEAVY_OVERFLOW);
+                        return;
+                    }
+                    if (pf) fp[np2p + pex] = sn;
+                    np2p += ptot;
                 }
                 uint32_t ex;
                 const uint32_t tot = block_scan(c, ex, s_w);
@@ -1135,17 +1156,22 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
                 }
                 tv.lg0[u] = G0;
                 tv.lg1[u] = G1;
+                s_g[0] = G0;
+                s_g1 = G1;
                 const float3 at = grad_apply(G0, G1, t.x - ug.x, t.y - ug.y, t.z - ug.z);
                 lx = L.y + at.x;
                 ly = L.z + at.y;
                 lz = L.w + at.z;
-                if (A.leaf_of) A.leaf_of[ui.x] = u;
+                if (A.leaf_of && !multi) A.leaf_of[ui.x] = u;
             }
             tv.lt[u] = L;
-            const double mm = (double)t.w;
-            A.fx[ui.x] = (float)(mm * ((double)lx + (double)sum[9]));
-            A.fy[ui.x] = (float)(mm * ((double)ly + (double)sum[10]));
-            A.fz[ui.x] = (float)(mm * ((double)lz + (double)sum[11]));
+            s_g[1] = L;
+            if (!multi) {
+                const double mm = (double)t.w;
+                A.fx[ui.x] = (float)(mm * ((double)lx + (double)sum[9]));
+                A.fy[ui.x] = (float)(mm * ((double)ly + (double)sum[10]));
+                A.fz[ui.x] = (float)(mm * ((double)lz + (double)sum[11]));
+            }
             if (DEBUG) {
                 unsigned long long c0 = 0, c1 = 0, c2 = 0;
                 for (int q = 0; q < kHeavyWarps; ++q) {
@@ -1161,6 +1187,49 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
             }
         }
         __syncthreads();
+        if (multi) {
+            // P2P + L2P per particle over the listed sources, fixed-order sums
+            const float4 L = s_g[1];
+            for (uint32_t k = 0; k < ui.y; ++k) {
+                const float4 tk = A.xyzm[ui.x + k];
+                float px = 0.f, py = 0.f, pz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
+                for (uint32_t e = tid; e < np2p; e += kHeavyThreads) {
+                    const uint4 si = tv.info[fp[e]];
+                    p2p_range(A.xyzm, make_uint2(si.x, si.y), tk, A.kahan, px, py, pz, qx, qy,
+                              qz);
+                }
+                const float r0 = warp_sum(px - qx), r1 = warp_sum(py - qy),
+                            r2 = warp_sum(pz - qz);
+                if (lane == 0) {
+                    s_red[w][0] = r0;
+                    s_red[w][1] = r1;
+                    s_red[w][2] = r2;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    float sx = 0.f, sy = 0.f, sz = 0.f;
+                    for (int q = 0; q < kHeavyWarps; ++q) {
+                        sx += s_red[q][0];
+                        sy += s_red[q][1];
+                        sz += s_red[q][2];
+                    }
+                    float lx = L.y, ly = L.z, lz = L.w;
+                    if constexpr (GRAD) {
+                        const float3 at =
+                            grad_apply(s_g[0], s_g1, tk.x - ug.x, tk.y - ug.y, tk.z - ug.z);
+                        lx += at.x;
+                        ly += at.y;
+                        lz += at.z;
+                        if (A.leaf_of) A.leaf_of[ui.x + k] = u;
+                    }
+                    const double mm = (double)tk.w;
+                    A.fx[ui.x + k] = (float)(mm * ((double)lx + (double)sx));
+                    A.fy[ui.x + k] = (float)(mm * ((double)ly + (double)sy));
+                    A.fz[ui.x + k] = (float)(mm * ((double)lz + (double)sz));
+                }
+                __syncthreads();
+            }
+        }
     }
 }
 

@@ -171,7 +171,8 @@ static int alloc_dense(State* s, uint32_t cap) {
 static int alloc_heavy(State* s, uint32_t cap) {
     if (s->heavy_frontier) cudaFree(s->heavy_frontier);
     s->heavy_frontier = nullptr;
-    PSG_ALLOC(s->heavy_frontier, (size_t)s->heavy_slots * 2 * cap * 4);
+    // per block: two frontiers and the P2P source list of a multi-particle leaf
+    PSG_ALLOC(s->heavy_frontier, (size_t)s->heavy_slots * 3 * cap * 4);
     s->heavy_fcap = cap;
     return PSG_OK;
 }
@@ -352,7 +353,6 @@ static int closure_alloc(State* s) {
 // sources within about theta H / 2^(d-1), a large part of the tree once
 // 2^d <= 4 theta.
 static int heavy_depth_for(const State* s) {
-    if (s->leaf_cap > 1) return 0;  // k_heavy_leaf walks one-particle leaves only
     if (s->heavy_depth >= 0) return s->heavy_depth > 5 ? 5 : s->heavy_depth;
     int d = 0;
     while (d < 5 && (float)(2 << d) <= 4.0f * s->theta) ++d;

@@ -55,6 +55,28 @@ def test_order1_matches_oracle(oracle):
     assert np.abs(scale - so).max() <= 1e-4 * np.abs(so).max()
 
 
+@pytest.mark.parametrize("cap,heavy", [(16, None), (32, 5)])
+def test_order1_with_leaf_capacity_matches_oracle(oracle, cap, heavy):
+    # multi-particle leaves: L2P of the order-1 expansion per particle, in the
+    # leaf pass and in the block-wide walk of shallow leaves
+    n, theta = 20000, 6.0
+    p0 = W.clumpy_plummer(n, 7)
+    a, b = p0.copy(), p0.copy()
+    ro = oracle.tick(a, theta=theta, order=1, leaf_cap=cap)
+    with P.Context(n, theta=theta) as ctx:
+        ctx.set_closure(1)
+        ctx.set_option(P.OPT_DEBUG, 1)
+        ctx.set_option(P.OPT_LEAF_CAP, cap)
+        if heavy is not None:
+            ctx.set_option(P.OPT_HEAVY_DEPTH, heavy)
+        ctx.tick(b, np.zeros(n, np.uint32))
+        t = ctx.tree()
+    assert np.array_equal(a.id, b.id)
+    assert np.array_equal(t["m2l_cnt"], ro["tree"]["m2l_cnt"])
+    assert np.array_equal(t["p2p_cnt"], ro["tree"]["p2p_cnt"])
+    assert rel_l2(forces(b), forces(a)) < FORCE_REL_L2
+
+
 def test_order1_is_more_accurate_than_order0(oracle):
     n = 16384
     p0 = W.clumpy_plummer(n, 6)

@@ -23,7 +23,8 @@ FORCE_REL_MAX = 1e-4
 TOPO = ("depth", "start", "count", "nchild", "octant")
 
 
-def gpu_tick(p, theta, debug=True, kahan=False, max_particles=None, leaf_cap=1):
+def gpu_tick(p, theta, debug=True, kahan=False, max_particles=None, leaf_cap=1,
+             heavy_depth=None):
     with P.Context(max_particles or p.n, theta=theta) as ctx:
         if debug:
             ctx.set_option(P.OPT_DEBUG, 1)
@@ -31,6 +32,8 @@ def gpu_tick(p, theta, debug=True, kahan=False, max_particles=None, leaf_cap=1):
             ctx.set_option(P.OPT_KAHAN, 1)
         if leaf_cap != 1:
             ctx.set_option(P.OPT_LEAF_CAP, leaf_cap)
+        if heavy_depth is not None:
+            ctx.set_option(P.OPT_HEAVY_DEPTH, heavy_depth)
         codes = np.zeros(p.n, np.uint32)
         mn, mx, rg = ctx.tick(p, codes)
         return {"codes": codes, "bbox": np.array([mn, mx, rg], np.float32),
@@ -83,10 +86,10 @@ CASES = [
 ]
 
 
-def _vs_oracle(oracle, p, theta, leaf_cap=1, per_particle=FORCE_REL_MAX):
+def _vs_oracle(oracle, p, theta, leaf_cap=1, per_particle=FORCE_REL_MAX, heavy_depth=None):
     a, b = p.copy(), p.copy()
     ro = oracle.tick(a, theta=theta, leaf_cap=leaf_cap)
-    rg = gpu_tick(b, theta, leaf_cap=leaf_cap)
+    rg = gpu_tick(b, theta, leaf_cap=leaf_cap, heavy_depth=heavy_depth)
     assert np.array_equal(rg["codes"], ro["codes"])
     assert np.array_equal(b.id, a.id)
     t, o = rg["tree"], ro["tree"]
@@ -116,24 +119,29 @@ def test_plummer_1m_full_size(oracle):
     assert ro["stats"]["m2l_pairs"] > 100_000_000
 
 
+# (name, particles, theta, leaf capacity, shallow-leaf depth: None = from
+# theta; 5 sends every leaf of depth <= 5 through the block-wide walk)
 LEAF_CAP_CASES = [
-    ("plummer65536_b16", lambda: W.plummer(65536, 3), 2.0, 16),
-    ("plummer65536_b64", lambda: W.plummer(65536, 3), 4.0, 64),
-    ("clumpy20000_b8", lambda: W.clumpy_plummer(20000, 3), 2.0, 8),
-    ("clumpy20000_b32", lambda: W.clumpy_plummer(20000, 3), 6.0, 32),
-    ("ragged12345_b2", lambda: W.uniform_cube(12345, 6), 2.0, 2),
-    ("clusters4096_b256", lambda: W.lcg_two_clusters(4096), 1.0, 256),
+    ("plummer65536_b16", lambda: W.plummer(65536, 3), 2.0, 16, None),
+    ("plummer65536_b64", lambda: W.plummer(65536, 3), 4.0, 64, None),
+    ("clumpy20000_b8", lambda: W.clumpy_plummer(20000, 3), 2.0, 8, None),
+    ("clumpy20000_b32", lambda: W.clumpy_plummer(20000, 3), 6.0, 32, None),
+    ("ragged12345_b2", lambda: W.uniform_cube(12345, 6), 2.0, 2, None),
+    ("clusters4096_b256", lambda: W.lcg_two_clusters(4096), 1.0, 256, None),
+    ("plummer65536_b32_shallow5", lambda: W.plummer(65536, 5), 4.0, 32, 5),
+    ("clumpy20000_b16_shallow5", lambda: W.clumpy_plummer(20000, 4), 6.0, 16, 5),
 ]
 
 
-@pytest.mark.parametrize("name,gen,theta,cap", LEAF_CAP_CASES,
+@pytest.mark.parametrize("name,gen,theta,cap,heavy", LEAF_CAP_CASES,
                          ids=[c[0] for c in LEAF_CAP_CASES])
-def test_leaf_capacity_vs_oracle(oracle, name, gen, theta, cap):
+def test_leaf_capacity_vs_oracle(oracle, name, gen, theta, cap, heavy):
     # PS_B200_OPT_LEAF_CAP: the same bar as the reference's leaf capacity 1,
     # except per particle: a particle's P2P sum now runs over thousands of
     # sources, summed in another order than the oracle's, so a particle whose
     # net force nearly cancels can differ by more than 1e-4 relative
-    rg, ro = _vs_oracle(oracle, gen(), theta, leaf_cap=cap, per_particle=1e-3)
+    rg, ro = _vs_oracle(oracle, gen(), theta, leaf_cap=cap, per_particle=1e-3,
+                        heavy_depth=heavy)
     t = rg["tree"]
     leaf = t["nchild"] == 0
     assert t["count"][leaf & (t["depth"] < 10) & (t["depth"] > 0)].max() <= cap
