@@ -179,15 +179,15 @@ ps_result_t ps_b200_ensemble_create(ps_b200_ensemble_t** out, const size_t* coun
                                     size_t n_systems, const float* theta);
 
 /* The autotuner, on copies of the given state (arrs and the codes array are
- * not changed): per size class (systems with equal floor(log2 N)) and per
- * leaf capacity of the ladder (default {1, 16, 32, 64}), the smallest theta
- * of {1, 1.5, 2, 3, 4, 6, 8} whose median relative force error against an
- * FP64 direct sum (1024 sampled particles of the class's first system) is at
- * most target_median_error, then the device time of one tick of that system
- * there; the class takes the fastest (theta, leaf capacity) that meets the
- * target (if none does, the smallest error).  Then the traversal grids'
- * scale among {1, 1/2, 1/4} of one system's persistent grids, by the time of
- * one forces replay of the whole ensemble.  theta_out (n_systems) and
+ * not changed): per leaf capacity of the ladder (default {1, 16, 32, 64})
+ * and size class (systems with equal floor(log2 N)), the smallest theta of
+ * {1, 1.5, 2, 3, 4, 6, 8} whose median relative force error against an FP64
+ * direct sum (1024 sampled particles of the class's first system) is at
+ * most target_median_error (none: 8); then one leaf capacity for all
+ * systems, the one whose forces replay of the whole ensemble is fastest
+ * among those where every class met the target; then the traversal grids'
+ * scale among {1, 1/2, 1/4} of one system's persistent grids, by the same
+ * replay time.  theta_out (n_systems) and
  * grid_scale_out receive the choice (either may be NULL);
  * ps_b200_ensemble_leaf_caps reads the leaf capacities. */
 ps_result_t ps_b200_ensemble_autotune(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,

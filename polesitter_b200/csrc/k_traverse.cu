@@ -844,11 +844,70 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
 // record (a run of leaves, up to 32 of their particles, the group's source
 // chain) at a time from a shared counter; T lanes own the record's target
 // particles (T the smallest power of two >= their count) and the 32 / T
-// slices of lanes take every (32 / T)-th source each, so a record with few
-// targets still keeps the warp busy; the slices' sums are added at the end.  The sources are summed in chain order, so the result
-// does not depend on scheduling.
-template <bool DEBUG, bool GRAD>
+// slices of lanes split the sources, so a record with few targets still
+// keeps the warp busy; the slices' sums are added at the end.
+//
+// Sources go through the warp in tiles of 32 particles: a chunk's entries
+// (source leaves that serve at least one leaf of the record) are laid end to
+// end by a prefix sum of their particle counts, lane j finds the entry of
+// particle b + j by a binary search over those sums, loads it (coalesced
+// within a leaf) with the entry's child mask into the warp's shared tile,
+// and every lane then runs its target against the tile's particles from
+// shared memory.  When every entry of a chunk serves every leaf of the run,
+// the per-pair mask test is dropped.  Sources are summed in chain order, so
+// the result does not depend on scheduling.
+struct DenseTile {
+    float4 p[32];
+    uint32_t m[32];
+};
+
+// one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
+// a source counts only if its child mask holds the target's leaf q
+template <bool MASKED, bool KAHAN>
+__device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, uint32_t S,
+                                           uint32_t nt, uint32_t q, float4 t, float& ax,
+                                           float& ay, float& az, float& cx, float& cy, float& cz,
+                                           uint32_t& used) {
+#pragma unroll 4
+    for (uint32_t j = j0; j < nt; j += S) {
+        const float4 p = tile.p[j];
+        float w = p.w;
+        if (MASKED) {
+            const bool on = (tile.m[j] >> q) & 1u;
+            w = on ? w : 0.f;
+            used += on ? 1u : 0u;
+        } else {
+            ++used;
+        }
+        const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
+        const float inv = rsqrtf(r2);
+        const float f = w * (inv * inv * inv);
+        if (KAHAN) {
+            const float yx = __fsub_rn(__fmul_rn(dx, f), cx);
+            const float yy = __fsub_rn(__fmul_rn(dy, f), cy);
+            const float yz = __fsub_rn(__fmul_rn(dz, f), cz);
+            const float tx = __fadd_rn(ax, yx);
+            const float ty = __fadd_rn(ay, yy);
+            const float tz = __fadd_rn(az, yz);
+            cx = __fsub_rn(__fsub_rn(tx, ax), yx);
+            cy = __fsub_rn(__fsub_rn(ty, ay), yy);
+            cz = __fsub_rn(__fsub_rn(tz, az), yz);
+            ax = tx;
+            ay = ty;
+            az = tz;
+        } else {
+            ax = fmaf(dx, f, ax);
+            ay = fmaf(dy, f, ay);
+            az = fmaf(dz, f, az);
+        }
+    }
+}
+
+template <bool DEBUG, bool GRAD, bool KAHAN>
 __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
+    __shared__ DenseTile tiles[kTravWarps];
+    DenseTile& tile = tiles[threadIdx.x >> 5];
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_DENSE_OVERFLOW)) return;
     const TreeView& tv = A.tv;
@@ -863,8 +922,6 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         if (r >= total) break;
         const uint4 rec = A.dense_rec[r];
         const uint32_t fc = rec.x, run = rec.w >> 8, cnt_t = rec.w & 0xFFu;
-        // T lanes per target set (the smallest power of two >= the record's
-        // targets); the 32 / T slices of lanes split the sources between them
         uint32_t T = 1;
         while (T < cnt_t) T <<= 1;
         const uint32_t S = 32u / T;
@@ -880,20 +937,52 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         const uint32_t u = fc + q;
         const float4 t = A.xyzm[i];
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+        uint32_t used = 0;
         for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
             const uint32_t cnt = A.p2p.cnt[c];
-            for (uint32_t k = slice; k < cnt; k += S) {
-                if (!((A.p2p.mask[(size_t)c * kP2PChunk + k] >> q) & 1u)) continue;
-                const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + k]];
-                p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz, cx, cy, cz);
-                if (DEBUG) inter += active ? si.y : 0u;
+            uint32_t es = 0, en = 0, em = 0;
+            if (lane < cnt) {
+                em = A.p2p.mask[(size_t)c * kP2PChunk + lane] & run;
+                if (em) {
+                    const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
+                    es = si.x;
+                    en = si.y;
+                }
+            }
+            const uint32_t incl = warp_incl_scan(en);
+            const uint32_t ptot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            const bool masked = __ballot_sync(0xFFFFFFFFu, en && em != run) != 0u;
+            for (uint32_t b = 0; b < ptot; b += 32) {
+                // lane j: flat source particle b + j -> entry e (incl[e-1] <= f < incl[e])
+                const uint32_t f = b + lane;
+                uint32_t e = 0;
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1) {
+                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, e + step - 1);
+                    if (v <= f) e += step;
+                }
+                const uint32_t e_start = __shfl_sync(0xFFFFFFFFu, es, e);
+                const uint32_t e_excl = __shfl_sync(0xFFFFFFFFu, incl - en, e);
+                const uint32_t e_mask = __shfl_sync(0xFFFFFFFFu, em, e);
+                __syncwarp();
+                if (f < ptot) {
+                    tile.p[lane] = A.xyzm[e_start + (f - e_excl)];
+                    tile.m[lane] = e_mask;
+                }
+                __syncwarp();
+                const uint32_t nt = min(32u, ptot - b);
+                if (masked)
+                    dense_tile<true, KAHAN>(tile, slice, S, nt, q, t, bx, by, bz, cx, cy, cz, used);
+                else
+                    dense_tile<false, KAHAN>(tile, slice, S, nt, q, t, bx, by, bz, cx, cy, cz,
+                                             used);
             }
         }
+        if (DEBUG) inter += active ? used : 0u;
         // sum the slices' partial sums (fixed order)
         bx -= cx;
         by -= cy;
         bz -= cz;
-        cx = cy = cz = 0.f;
         for (uint32_t o = T; o < 32u; o <<= 1) {
             bx += __shfl_xor_sync(0xFFFFFFFFu, bx, o);
             by += __shfl_xor_sync(0xFFFFFFFFu, by, o);
@@ -912,9 +1001,9 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
                 if (A.leaf_of) A.leaf_of[i] = u;
             }
             const double mm = (double)t.w;
-            A.fx[i] = (float)(mm * ((double)lx + (double)(bx - cx)));
-            A.fy[i] = (float)(mm * ((double)ly + (double)(by - cy)));
-            A.fz[i] = (float)(mm * ((double)lz + (double)(bz - cz)));
+            A.fx[i] = (float)(mm * ((double)lx + (double)bx));
+            A.fy[i] = (float)(mm * ((double)ly + (double)by));
+            A.fz[i] = (float)(mm * ((double)lz + (double)bz));
         }
     }
     if (DEBUG) {
@@ -1256,13 +1345,19 @@ void launch_heavy_leaf(const TravArgs& A, int grid, cudaStream_t st) {
     }
 }
 
+template <bool DEBUG, bool GRAD>
+static void launch_dense_kahan(const TravArgs& A, int grid, cudaStream_t st) {
+    if (A.kahan) k_dense_p2p<DEBUG, GRAD, true><<<grid, kTravThreads, 0, st>>>(A);
+    else k_dense_p2p<DEBUG, GRAD, false><<<grid, kTravThreads, 0, st>>>(A);
+}
+
 void launch_dense_p2p(const TravArgs& A, int grid, cudaStream_t st) {
     if (A.order >= 1) {
-        if (A.debug) k_dense_p2p<true, true><<<grid, kTravThreads, 0, st>>>(A);
-        else k_dense_p2p<false, true><<<grid, kTravThreads, 0, st>>>(A);
+        if (A.debug) launch_dense_kahan<true, true>(A, grid, st);
+        else launch_dense_kahan<false, true>(A, grid, st);
     } else {
-        if (A.debug) k_dense_p2p<true, false><<<grid, kTravThreads, 0, st>>>(A);
-        else k_dense_p2p<false, false><<<grid, kTravThreads, 0, st>>>(A);
+        if (A.debug) launch_dense_kahan<true, false>(A, grid, st);
+        else launch_dense_kahan<false, false>(A, grid, st);
     }
 }
 

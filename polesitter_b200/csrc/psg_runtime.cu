@@ -1173,25 +1173,26 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
         *med = rel[ns / 2];
         return PSG_OK;
     };
-    for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
-        if (chosen[k] > 0.f) continue;
-        State* s = e->sys[k];
-        const size_t n = e->count[k];
-        const DevArrays ck = slice(c, e->offset[k]);
-        // per leaf capacity: the smallest theta meeting the target, then the
-        // time of one tick there; the fastest that meets it wins (none
-        // meets it: the smallest error at the largest theta)
-        bool best_met = false;
-        double best_ms = 1e300, best_err = 1e300;
-        float best_theta = ladder[nl - 1];
-        uint32_t best_cap = e->leaf_ladder.empty() ? 1u : e->leaf_ladder[0];
-        for (uint32_t cap : e->leaf_ladder) {
+    // per leaf capacity of the ladder and size class: the smallest theta
+    // meeting the target (none meets it: the largest), from the class's
+    // first system
+    const size_t nl_cap = e->leaf_ladder.size();
+    std::vector<std::vector<float>> th_cap(nl_cap, std::vector<float>(e->nsys, ladder[nl - 1]));
+    std::vector<bool> all_met(nl_cap, true);
+    for (size_t ci = 0; ci < nl_cap && r == PSG_OK; ++ci) {
+        const uint32_t cap = e->leaf_ladder[ci];
+        std::vector<bool> done(e->nsys, false);
+        for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
+            if (done[k]) continue;
+            State* s = e->sys[k];
+            const size_t n = e->count[k];
+            const DevArrays ck = slice(c, e->offset[k]);
             s->leaf_cap = cap;
             float pick = ladder[nl - 1];
-            double err = 1e300;
             bool met = false;
-            float ms = 0.f;
             for (int li = 0; li < nl && r == PSG_OK; ++li) {
+                float ms = 0.f;
+                double err = 0.0;
                 s->theta = ladder[li];
                 if ((r = one_tick(s, ck, n, &ms)) != PSG_OK) break;
                 if ((r = median_error(s, ck, n, &err)) != PSG_OK) break;
@@ -1201,27 +1202,52 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
                     break;
                 }
             }
-            if (r != PSG_OK) break;
-            // the stores have grown for this (theta, cap): time a clean tick
-            s->theta = pick;
-            if ((r = one_tick(s, ck, n, &ms)) != PSG_OK) break;
-            const bool better = (met && !best_met) ||
-                                (met == best_met && (met ? ms < best_ms : err < best_err));
-            if (better) {
-                best_met = met;
-                best_ms = ms;
-                best_err = err;
-                best_theta = pick;
-                best_cap = cap;
+            if (!met) all_met[ci] = false;
+            for (size_t j = 0; j < e->nsys; ++j) {
+                if (cls[j] == cls[k]) {
+                    th_cap[ci][j] = pick;
+                    done[j] = true;
+                }
             }
         }
-        s->leaf_cap = best_cap;
-        s->theta = best_theta;
-        for (size_t j = 0; j < e->nsys; ++j) {
-            if (cls[j] == cls[k]) {
-                chosen[j] = best_theta;
-                chosen_cap[j] = best_cap;
+    }
+    // then one leaf capacity for the whole ensemble: the fastest forces replay
+    // among those whose every class met the target (none did: the first)
+    size_t best_ci = 0;
+    if (r == PSG_OK && nl_cap > 1) {
+        float* vdummy[3] = {c.fx, c.fy, c.fz};
+        double best = 1e300;
+        for (size_t ci = 0; ci < nl_cap && r == PSG_OK; ++ci) {
+            if (!all_met[ci] && all_met[best_ci]) continue;
+            for (size_t k = 0; k < e->nsys; ++k) {
+                e->sys[k]->theta = th_cap[ci][k];
+                e->sys[k]->leaf_cap = e->leaf_ladder[ci];
             }
+            e->dirty = true;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && r == PSG_OK; ++rep) {  // the first replay grows stores
+                if ((r = restore()) != PSG_OK) break;
+                if ((r = ensure_graphs(e, c, vdummy, 0.f)) != PSG_OK) break;
+                PSG_CHECK(cudaEventRecord(e0, e->root));
+                PSG_CHECK(cudaGraphLaunch(e->g_force, e->root));
+                PSG_CHECK(cudaEventRecord(e1, e->root));
+                PSG_CHECK(cudaStreamSynchronize(e->root));
+                if ((r = check_systems(e, c)) != PSG_OK) break;
+                cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (r != PSG_OK) break;
+            const bool eligible = all_met[ci] || !all_met[best_ci];
+            if (eligible && (ms < best || (all_met[ci] && !all_met[best_ci]))) {
+                best = ms;
+                best_ci = ci;
+            }
+        }
+        drop_graphs(e);
+    }
+    if (nl_cap > 0) {
+        for (size_t k = 0; k < e->nsys; ++k) {
+            chosen[k] = th_cap[best_ci][k];
+            chosen_cap[k] = e->leaf_ladder[best_ci];
         }
     }
     cudaEventDestroy(e0);
