@@ -12,11 +12,12 @@ timed step.
 
 --workload closure (default; the headline metric): N = 1,048,576 particles of
 the learned closure's snapshot family (an equal-mass Plummer sphere plus 32
-sub-clumps holding 30% of the mass, seeded), theta = 6.5, closure mode 2: the
-order-1 local expansion, the shipped MLP correction and the per-tick FP64
-judge on 4096 sampled particles.  Beside it, the plain GPU FMM (the
-reference's far field, mode 0) on the same snapshot over a range of theta,
-each with its median relative force error: the plain method's ticks/s at
+sub-clumps holding 30% of the mass, seeded), theta = 6.5, leaf capacity 16,
+closure mode 2: the order-1 local expansion, the shipped MLP correction and
+the per-tick FP64 judge on 4096 sampled particles.  Beside it, the plain GPU FMM (the
+reference's far field, mode 0) on the same snapshot over a range of theta
+(on the reference's tree, and on leaf capacity 16), each with its median
+relative force error: the plain method's ticks/s at
 the closure's error bound (<= 1e-3) is bounded by the fastest plain setting
 that still misses it.
 --workload plain: the reference's plain tick on an N = 1,048,576 Plummer
@@ -27,8 +28,9 @@ Reported (one JSON line on rank 0):
   e2e        ticks/s through the same C ABI with pinned HOST arrays, the
              host<->device copies inside each step
   accuracy   median relative force error against FP64 direct sums
-  roofline   the dominant phase, the leaf pass (MAC + M2L + L2L + P2P + L2P),
-             FP32-bound, from its CUDA-event time and algorithmic flop count
+  roofline   the dominant phase (the leaf pass: MAC + M2L + L2L + P2P + L2P,
+             or the full-leaf P2P + L2P), FP32-bound, from its CUDA-event time
+             and algorithmic flop count
   cpu_baseline  the reference's own threaded CPU tick (oracle/_ref) on the
              same workload, timed on this host's cores
   plain_c2, tick_loop, ensemble  (closure workload, unless --minimal) the
@@ -63,6 +65,8 @@ UNIT = "ticks/s"
 N_DEFAULT = 1 << 20
 ERROR_TARGET = 1e-3
 CLOSURE_THETA = 6.5        # the shipped weights' theta
+CLOSURE_LEAF_CAP = 16      # leaf capacity of the closure's tree (PS_B200_OPT_LEAF_CAP)
+PLAIN_LEAF_CAP_THETAS = (8.0, 12.0)  # plain rows on the closure's leaf capacity
 CLOSURE_SEED = 424242      # snapshot seed (the weights were trained on other seeds)
 PLAIN_THETAS = (2.0, 4.0, 8.0, 12.0)
 C2_THETA, C2_SEED = 2.0, 42
@@ -70,7 +74,7 @@ WORKLOADS = {
     "closure": ("learned-closure FMM tick (ps_prepare_particles + ps_calc_forces, closure mode 2: "
                 "order-1 local expansion + BF16 MLP correction + FP64 judge on 4096 particles), "
                 "N=1,048,576 clumpy Plummer (a=1, r<=10a, plus 32 sub-clumps with 30% of the mass, "
-                "equal mass 1/N), theta=6.5, float32 SoA"),
+                "equal mass 1/N), theta=6.5, leaf capacity 16, float32 SoA"),
     "plain": ("plain FMM tick (ps_prepare_particles + ps_calc_forces), Plummer sphere "
               "N=1,048,576, a=1, r<=10a, equal mass 1/N, theta=2, float32 SoA"),
 }
@@ -79,16 +83,14 @@ WORKLOADS = {
 # 2 leaf-pass variants + shallow leaves + full leaves; the closure adds the
 # judge (sample, FP64 direct sum, decision), the MLP and the apply kernel
 KERNELS_PER_TICK = {"plain": 39, "closure": 44}
-# DRAM bytes (read + write) of one leaf-pass launch, from the ncu captures
-# summarised under profiles/: the plain one at this size; the closure one
-# captured at N=131072 and scaled by the M2L pair count (x 8.28) to N=1M
-LEAF_PASS_DRAM_BYTES = {"plain": 255.3e6, "closure": 1.48e9}
+# DRAM bytes (read + write) of one launch of the dominant kernel, from the
+# ncu captures summarised under profiles/ (None: not captured for this
+# configuration)
+DOMINANT_DRAM_BYTES = {"plain": 255.3e6, "closure": None}
 TRAFFIC_NOTE = {
     "plain": "dram read+write bytes per launch, ncu capture of this workload "
              "(profiles/traversal_leaf_plummer1m.md)",
-    "closure": "dram read+write bytes per launch, ncu capture of the same kernel at N=131072 "
-               "(179.1 MB) scaled by the M2L pair count (x 8.28) to N=1M "
-               "(profiles/traversal_leaf_closure_clumpy131k.md)"}
+    "closure": "not captured for this configuration"}
 FLOP_M2L = 35         # per M2L pair: polesitter.h:1065-1092
 FLOP_M2L_ORDER1 = 59  # ... plus the monopole field gradient (closure order 1)
 FLOP_P2P = 20         # per particle pair: polesitter.h:1424-1444
@@ -103,6 +105,7 @@ def parse_args():
     ap.add_argument("--workload", choices=("closure", "plain"), default="closure")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--leaf-cap", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-curve", action="store_true")
@@ -186,6 +189,12 @@ def theta_of(args):
     if args.theta is not None:
         return args.theta
     return CLOSURE_THETA if args.workload == "closure" else C2_THETA
+
+
+def leaf_cap_of(args):
+    if args.leaf_cap is not None:
+        return args.leaf_cap
+    return CLOSURE_LEAF_CAP if args.workload == "closure" else 1
 
 
 def cpu_reference_ticks(p0, ticks, warmup, theta):
@@ -304,6 +313,8 @@ def run_b200(args):
         torch.cuda.synchronize()
 
     ctx = P.Context(n, theta=theta)
+    leaf_cap = leaf_cap_of(args)
+    ctx.set_option(P.OPT_LEAF_CAP, leaf_cap)
     if closure:
         params, meta = CL.load(CL.default_weights_path())
         ctx.closure_set_weights(params)
@@ -397,24 +408,34 @@ def run_b200(args):
     peaks, peak_src = measured_peaks()
     props = torch.cuda.get_device_properties(dev)
     fp32_peak = props.multi_processor_count * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
-    leaf_s = ph["leaves"] / 1e3
-    flops_leaf = (FLOP_M2L_ORDER1 if closure else FLOP_M2L) * m2l_leaf + \
-        FLOP_P2P * (p2p_inter - p2p_full)
-    achieved = flops_leaf / leaf_s / 1e12
-    roofline = {"kernel": "leaf pass: k_trav<MODE_LEAF> + k_heavy_leaf (MAC+M2L+L2L+P2P+L2P)",
+    # the dominant phase: the leaf pass (k_trav leaf + k_heavy_leaf: M2L of
+    # the leaf targets, P2P outside full leaves) or the full-leaf P2P
+    # (k_dense_p2p: P2P + L2P of the records)
+    m2l_flop = FLOP_M2L_ORDER1 if closure else FLOP_M2L
+    flops_leaf = m2l_flop * m2l_leaf + FLOP_P2P * (p2p_inter - p2p_full)
+    flops_full = FLOP_P2P * p2p_full
+    if ph["full_leaves"] > ph["leaves"]:
+        kern, launch_ms, flops = ("full-leaf P2P: k_dense_p2p (P2P + L2P of the leaf records)",
+                                  ph["full_leaves"], flops_full)
+        counts = {"p2p_particle_pairs": p2p_full, "flop_per_p2p": FLOP_P2P}
+    else:
+        kern, launch_ms, flops = ("leaf pass: k_trav<MODE_LEAF> + k_heavy_leaf "
+                                  "(MAC+M2L+L2L+P2P+L2P)", ph["leaves"], flops_leaf)
+        counts = {"m2l_pairs_leaf_targets": m2l_leaf,
+                  "p2p_particle_pairs": p2p_inter - p2p_full,
+                  "flop_per_m2l": m2l_flop, "flop_per_p2p": FLOP_P2P}
+    achieved = flops / (launch_ms / 1e3) / 1e12
+    roofline = {"kernel": kern,
                 "bound": "fp32", "achieved": achieved, "peak": fp32_peak / 1e12,
                 "unit": "TFLOP/s", "frac": achieved * 1e12 / fp32_peak,
                 "peak_source": f"computed: {props.multi_processor_count} SMs x 128 FP32 lanes x 2 x "
                                f"{peaks.get('sm_max_mhz', 1965.0)} MHz (sm_max_mhz, {peak_src}); "
                                "no measured FP32 peak exists",
-                "traffic": LEAF_PASS_DRAM_BYTES[args.workload],
+                "traffic": DOMINANT_DRAM_BYTES[args.workload],
                 "traffic_note": TRAFFIC_NOTE[args.workload],
-                "algorithmic_flop": flops_leaf,
-                "counts": {"m2l_pairs_leaf_targets": m2l_leaf,
-                           "p2p_particle_pairs": p2p_inter - p2p_full,
-                           "flop_per_m2l": FLOP_M2L_ORDER1 if closure else FLOP_M2L,
-                           "flop_per_p2p": FLOP_P2P},
-                "launch_ms": ph["leaves"]}
+                "algorithmic_flop": flops, "counts": counts, "launch_ms": launch_ms,
+                "other_phase": {"leaf_pass_ms": ph["leaves"], "leaf_pass_flop": flops_leaf,
+                                "full_leaf_ms": ph["full_leaves"], "full_leaf_flop": flops_full}}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -423,6 +444,7 @@ def run_b200(args):
             "data": "synthetic (seeded clumpy Plummer)" if closure
             else "synthetic (seeded Plummer sphere)",
             "config": {"workload": WORKLOADS[args.workload], "n": n, "theta": theta,
+                       "leaf_cap": leaf_cap,
                        "per_gpu": "independent replica of the workload",
                        "l2": "flushed (256 MB write) and inputs reset before every step, untimed",
                        "timing": "wall clock around the synchronous API call, max over ranks"},
@@ -463,8 +485,11 @@ def plain_curve(ctx, P, d, pristine, codes, flush, n, closure_value, closure_err
     ctx.set_closure(0)
     ctx.set_option(P.OPT_TIMING, 1)
     rows = []
-    for th in PLAIN_THETAS:
+    plan = [(th, 1) for th in PLAIN_THETAS] + \
+        [(th, CLOSURE_LEAF_CAP) for th in PLAIN_LEAF_CAP_THETAS]
+    for th, cap in plan:
         ctx.set_option(P.OPT_THETA, th)
+        ctx.set_option(P.OPT_LEAF_CAP, cap)
         for k in ("x", "y", "z", "mass", "id"):
             getattr(d, k).copy_(getattr(pristine, k))
         torch.cuda.synchronize()
@@ -479,15 +504,16 @@ def plain_curve(ctx, P, d, pristine, codes, flush, n, closure_value, closure_err
             ctx.tick(d, codes)
             ts.append(time.perf_counter() - t0)
         err = median_rel_error(ctx, d, n, 11)
-        rows.append({"theta": th, "ticks_per_s": 1.0 / min(ts),
+        rows.append({"theta": th, "leaf_cap": cap, "ticks_per_s": 1.0 / min(ts),
                      "median_rel_error": err["median_rel"]})
     missing = [r for r in rows if r["median_rel_error"] > ERROR_TARGET]
     # the most accurate setting measured (largest theta) still misses: reaching
     # the target needs a larger theta, i.e. more work than that setting's
-    bound = (min(missing, key=lambda r: -r["theta"])["ticks_per_s"]
+    bound = (min(missing, key=lambda r: r["median_rel_error"])["ticks_per_s"]
              if missing and len(missing) == len(rows) else None)
     return {"target_median_rel_error": ERROR_TARGET,
-            "closure": {"theta": CLOSURE_THETA, "ticks_per_s": closure_value,
+            "closure": {"theta": CLOSURE_THETA, "leaf_cap": CLOSURE_LEAF_CAP,
+                        "ticks_per_s": closure_value,
                         "max_tick_median_rel_error": closure_error},
             "plain_gpu_fmm": rows,
             "plain_reaches_target": len(missing) < len(rows),
@@ -495,7 +521,8 @@ def plain_curve(ctx, P, d, pristine, codes, flush, n, closure_value, closure_err
             "closure_speedup_lower_bound": (closure_value / bound) if bound else None,
             "note": "every plain setting measured misses the target; reaching it needs a "
                     "theta above the largest measured, and the plain tick only gets slower as "
-                    "theta grows, so its ticks/s at the target is at most the largest theta's"}
+                    "theta grows, so its ticks/s at the target is at most that of its most "
+                    "accurate setting measured"}
 
 
 def plain_c2(P, torch, dev, flush):
@@ -553,7 +580,8 @@ def ensemble_run(P, torch, dev):
     """The batched ensemble: 256 independent systems, N log-uniform in
     [1024, 262144], half uniform cubes and half Plummer spheres (a in
     [0.5, 2]); theta per size class and the traversal grid scale from the
-    autotuner (target median force error 3e-2); 50 ticks of semi-implicit
+    autotuner (target median force error 3e-2; leaf capacity per class from
+    {1, 16, 32, 64}); 50 ticks of semi-implicit
     Euler, dt=1e-3, each tick two replayed CUDA graphs.  Beside it, the same
     systems advanced one after the other through ps_b200_run_ticks."""
     from polesitter_b200 import workloads as W
@@ -571,6 +599,7 @@ def ensemble_run(P, torch, dev):
     codes = torch.zeros(p.n, dtype=torch.int32, device=dev)
     with P.Ensemble(counts) as ens:
         theta, scale = ens.autotune(a, codes, target)
+        caps = ens.leaf_caps()
         ens.run(a, codes, *v, 1e-3, 2)  # warm-up: captures the graphs, grows stores
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -581,6 +610,8 @@ def ensemble_run(P, torch, dev):
     b, w = arrays()
     offs = np.concatenate([[0], np.cumsum(counts)])
     ctxs = [P.Context(int(counts[k]), theta=float(theta[k])) for k in range(nsys)]
+    for k in range(nsys):
+        ctxs[k].set_option(P.OPT_LEAF_CAP, int(caps[k]))
 
     def one_pass():
         for k in range(nsys):
@@ -600,12 +631,15 @@ def ensemble_run(P, torch, dev):
     for c in ctxs:
         c.destroy()
     vals, cnts = np.unique(theta, return_counts=True)
+    cvals, ccnts = np.unique(caps, return_counts=True)
     return {"workload": "256 independent systems, N log-uniform in [1024, 262144] "
                         f"({int(p.n)} particles), half uniform cubes, half Plummer a in "
                         "[0.5, 2]; 50 ticks of Euler dt=1e-3",
             "ensemble_ticks_per_s": ticks / dt, "particle_ticks_per_s": p.n * ticks / dt,
             "autotuner": {"target_median_rel_error": target,
                           "theta_per_class": {str(float(t)): int(c) for t, c in zip(vals, cnts)},
+                          "leaf_cap_per_class": {str(int(t)): int(c)
+                                                 for t, c in zip(cvals, ccnts)},
                           "grid_scale": scale},
             "one_system_at_a_time_ticks_per_s": seq,
             "speedup_over_one_at_a_time": (ticks / dt) / seq}

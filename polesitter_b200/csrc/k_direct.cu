@@ -22,29 +22,34 @@ __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __rest
                                                             const uint32_t* __restrict__ targets,
                                                             size_t n_targets, size_t chunk,
                                                             double* __restrict__ out) {
-    __shared__ float4 tile[kDirThreads];
+    // the tile is widened to FP64 once per block, not once per pair
+    __shared__ double4 tile[kDirThreads];
     const size_t k = (size_t)blockIdx.x * kDirThreads + threadIdx.x;
     const uint32_t ti_raw = k < n_targets ? targets[k] : 0u;
     const bool active = k < n_targets && ti_raw < n;
     const uint32_t ti = active ? ti_raw : 0u;
     const float4 t = active ? xyzm[ti] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const double tx = (double)t.x, ty = (double)t.y, tz = (double)t.z;
     const double eps2 = (double)0.1f;
     const size_t src0 = (size_t)blockIdx.y * chunk;
     const size_t src1 = src0 + chunk < n ? src0 + chunk : n;
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (size_t j0 = src0; j0 < src1; j0 += kDirThreads) {
         const size_t j = j0 + threadIdx.x;
-        tile[threadIdx.x] = j < src1 ? xyzm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 sj = j < src1 ? xyzm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tile[threadIdx.x] = make_double4((double)sj.x, (double)sj.y, (double)sj.z, (double)sj.w);
         __syncthreads();
         const int cnt = (int)((src1 - j0) < (size_t)kDirThreads ? (src1 - j0) : kDirThreads);
         for (int q = 0; q < cnt; ++q) {
-            const float4 s = tile[q];
-            const double dx = (double)s.x - (double)t.x;
-            const double dy = (double)s.y - (double)t.y;
-            const double dz = (double)s.z - (double)t.z;
+            const double4 s = tile[q];
+            const double dx = s.x - tx;
+            const double dy = s.y - ty;
+            const double dz = s.z - tz;
             const double r2 = dx * dx + dy * dy + dz * dz + eps2;
             const double ir = rsqrt(r2);
-            const double w = ((j0 + q) == ti) ? 0.0 : (double)s.w * ir * ir * ir;
+            // the self pair (and any source at the target's position) has
+            // d = 0 and adds exactly 0, as j != i excludes it in the sum
+            const double w = s.w * ir * ir * ir;
             ax += dx * w;
             ay += dy * w;
             az += dz * w;

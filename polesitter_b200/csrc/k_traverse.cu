@@ -854,8 +854,11 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
 // within a leaf) with the entry's child mask into the warp's shared tile,
 // and every lane then runs its target against the tile's particles from
 // shared memory.  When every entry of a chunk serves every leaf of the run,
-// the per-pair mask test is dropped.  Sources are summed in chain order, so
-// the result does not depend on scheduling.
+// the per-pair mask test is dropped.  A record with at most 4 targets (8 or
+// more slices) skips the staging: each slice walks whole source leaves from
+// global memory, as the tile's binary search would cost more than its reuse
+// saves.  Sources are summed in chain order, so the result does not depend
+// on scheduling.
 struct DenseTile {
     float4 p[32];
     uint32_t m[32];
@@ -863,30 +866,37 @@ struct DenseTile {
 
 // one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
 // a source counts only if its child mask holds the target's leaf q
+// one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
+// a source counts only if its child mask holds the target's leaf q.  Plain
+// sums alternate between two accumulator sets (independent FMA chains),
+// added at the end of the tile.
 template <bool MASKED, bool KAHAN>
 __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, uint32_t S,
                                            uint32_t nt, uint32_t q, float4 t, float& ax,
                                            float& ay, float& az, float& cx, float& cy, float& cz,
                                            uint32_t& used) {
-#pragma unroll 4
-    for (uint32_t j = j0; j < nt; j += S) {
-        const float4 p = tile.p[j];
-        float w = p.w;
-        if (MASKED) {
-            const bool on = (tile.m[j] >> q) & 1u;
-            w = on ? w : 0.f;
-            used += on ? 1u : 0u;
-        } else {
-            ++used;
-        }
-        const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
-        const float inv = rsqrtf(r2);
-        const float f = w * (inv * inv * inv);
-        if (KAHAN) {
-            const float yx = __fsub_rn(__fmul_rn(dx, f), cx);
-            const float yy = __fsub_rn(__fmul_rn(dy, f), cy);
-            const float yz = __fsub_rn(__fmul_rn(dz, f), cz);
+    if constexpr (KAHAN) {
+        for (uint32_t j = j0; j < nt; j += S) {
+            const float4 p = tile.p[j];
+            float w = p.w;
+            if (MASKED) {
+                const bool on = (tile.m[j] >> q) & 1u;
+                w = on ? w : 0.f;
+                used += on ? 1u : 0u;
+            } else {
+                ++used;
+            }
+            float fx, fy, fz;
+            const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
+            const float inv = rsqrtf(r2);
+            const float f = w * (inv * inv * inv);
+            fx = __fmul_rn(dx, f);
+            fy = __fmul_rn(dy, f);
+            fz = __fmul_rn(dz, f);
+            const float yx = __fsub_rn(fx, cx);
+            const float yy = __fsub_rn(fy, cy);
+            const float yz = __fsub_rn(fz, cz);
             const float tx = __fadd_rn(ax, yx);
             const float ty = __fadd_rn(ay, yy);
             const float tz = __fadd_rn(az, yz);
@@ -896,11 +906,54 @@ __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, u
             ax = tx;
             ay = ty;
             az = tz;
-        } else {
+        }
+    } else {
+        float ex = 0.f, ey = 0.f, ez = 0.f;
+        uint32_t j = j0;
+#pragma unroll 2
+        for (; j + S < nt; j += 2 * S) {
+            const float4 p0 = tile.p[j], p1 = tile.p[j + S];
+            float w0 = p0.w, w1 = p1.w;
+            if (MASKED) {
+                const bool on0 = (tile.m[j] >> q) & 1u, on1 = (tile.m[j + S] >> q) & 1u;
+                w0 = on0 ? w0 : 0.f;
+                w1 = on1 ? w1 : 0.f;
+                used += (on0 ? 1u : 0u) + (on1 ? 1u : 0u);
+            } else {
+                used += 2;
+            }
+            const float dx0 = p0.x - t.x, dy0 = p0.y - t.y, dz0 = p0.z - t.z;
+            const float dx1 = p1.x - t.x, dy1 = p1.y - t.y, dz1 = p1.z - t.z;
+            const float i0 = rsqrtf(fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0)) + 0.1f);
+            const float i1 = rsqrtf(fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1)) + 0.1f);
+            const float f0 = w0 * (i0 * i0 * i0), f1 = w1 * (i1 * i1 * i1);
+            ax = fmaf(dx0, f0, ax);
+            ay = fmaf(dy0, f0, ay);
+            az = fmaf(dz0, f0, az);
+            ex = fmaf(dx1, f1, ex);
+            ey = fmaf(dy1, f1, ey);
+            ez = fmaf(dz1, f1, ez);
+        }
+        if (j < nt) {
+            const float4 p = tile.p[j];
+            float w = p.w;
+            if (MASKED) {
+                const bool on = (tile.m[j] >> q) & 1u;
+                w = on ? w : 0.f;
+                used += on ? 1u : 0u;
+            } else {
+                ++used;
+            }
+            const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
+            const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f);
+            const float f = w * (inv * inv * inv);
             ax = fmaf(dx, f, ax);
             ay = fmaf(dy, f, ay);
             az = fmaf(dz, f, az);
         }
+        ax += ex;
+        ay += ey;
+        az += ez;
     }
 }
 
@@ -940,6 +993,17 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         uint32_t used = 0;
         for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
             const uint32_t cnt = A.p2p.cnt[c];
+            if (S >= 8u) {
+                // few targets: each slice walks whole source leaves of the
+                // chunk from global memory (no staging)
+                for (uint32_t k = slice; k < cnt; k += S) {
+                    if (!((A.p2p.mask[(size_t)c * kP2PChunk + k] >> q) & 1u)) continue;
+                    const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + k]];
+                    p2p_range(A.xyzm, make_uint2(si.x, si.y), t, KAHAN, bx, by, bz, cx, cy, cz);
+                    used += si.y;
+                }
+                continue;
+            }
             uint32_t es = 0, en = 0, em = 0;
             if (lane < cnt) {
                 em = A.p2p.mask[(size_t)c * kP2PChunk + lane] & run;

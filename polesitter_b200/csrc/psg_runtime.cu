@@ -414,7 +414,7 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     const int lg[2] = {scaled(s->trav_grid[o][0]), scaled(s->trav_grid[o][1])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
-    launch_dense_p2p(A, scaled(s->sms * 8), s->stream);
+    launch_dense_p2p(A, scaled(s->sms * 12), s->stream);
     PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     record(s, PH_END);
     return PSG_OK;
