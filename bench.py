@@ -86,11 +86,13 @@ KERNELS_PER_TICK = {"plain": 39, "closure": 44}
 # DRAM bytes (read + write) of one launch of the dominant kernel, from the
 # ncu captures summarised under profiles/ (None: not captured for this
 # configuration)
-DOMINANT_DRAM_BYTES = {"plain": 255.3e6, "closure": None}
+DOMINANT_DRAM_BYTES = {"plain": 255.3e6, "closure": 0.59e9}
 TRAFFIC_NOTE = {
     "plain": "dram read+write bytes per launch, ncu capture of this workload "
              "(profiles/traversal_leaf_plummer1m.md)",
-    "closure": "not captured for this configuration"}
+    "closure": "dram read+write bytes per launch of k_dense_p2p, ncu capture of the same kernel "
+               "at N=131072 (61.8 MB) scaled by the full-leaf pair count (x 9.53) to N=1M "
+               "(profiles/full_leaf_p2p_closure_clumpy131k.md)"}
 FLOP_M2L = 35         # per M2L pair: polesitter.h:1065-1092
 FLOP_M2L_ORDER1 = 59  # ... plus the monopole field gradient (closure order 1)
 FLOP_P2P = 20         # per particle pair: polesitter.h:1424-1444
@@ -462,9 +464,9 @@ def run_b200(args):
                                           accuracy["judge"]["max_of_tick_medians"])
     ctx.destroy()
     if closure and extras:
+        line["ensemble"] = ensemble_run(P, torch, dev)
         line["plain_c2"] = plain_c2(P, torch, dev, flush)
         line["tick_loop"] = tick_loop(P, torch, dev)
-        line["ensemble"] = ensemble_run(P, torch, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference_ticks(p0, ticks=1 if closure else 3, warmup=1,
                                                    theta=theta)

@@ -127,6 +127,7 @@ struct State {
     ClosureState cl;
     int order;  // traversal's local expansion order: 0 (reference) or 1
     size_t last_n;  // particles of the last completed tick
+    size_t trav_n;  // particles of the tick whose traversal is being enqueued
     int attempts;   // traversal runs of the last tick (> 1: a capacity regrow)
 };
 
@@ -414,7 +415,12 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     const int lg[2] = {scaled(s->trav_grid[o][0]), scaled(s->trav_grid[o][1])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
-    launch_dense_p2p(A, scaled(s->sms * 12), s->stream);
+    // full-leaf records: 12 blocks per SM, fewer for a small system (whose
+    // records, if any, are few), so an ensemble of small systems does not
+    // launch thousands of idle blocks each
+    const size_t dense_blocks =
+        std::min<size_t>((size_t)s->sms * 12, std::max<size_t>(4, s->trav_n / 64));
+    launch_dense_p2p(A, scaled((int)dense_blocks), s->stream);
     PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     record(s, PH_END);
     return PSG_OK;
@@ -587,6 +593,7 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
         PSG_CHECK(cudaStreamSynchronize(st));
         err = s->h_status->err;
     } else {
+        s->trav_n = n;
         int r = run_traversal(s, s->xyzm, d.fx, d.fy, d.fz, &err);
         if (r != PSG_OK) {
             if (judge) cudaStreamSynchronize(cj.side);  // leave no judge work running
@@ -872,6 +879,7 @@ static int enqueue_system_forces(State* s, const DevArrays& d, size_t n, int var
                 s->tk_bbox, s->leaf_cap);
     launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
     if (n > 1) {
+        s->trav_n = n;
         int r = enqueue_traversal(s, s->xyzm, d.fx, d.fy, d.fz);
         if (r != PSG_OK) return r;
     } else {
