@@ -12,7 +12,7 @@ timed step.
 
 --workload closure (default; the headline metric): N = 1,048,576 particles of
 the learned closure's snapshot family (an equal-mass Plummer sphere plus 32
-sub-clumps holding 30% of the mass, seeded), theta = 6.5, leaf capacity 16,
+sub-clumps holding 30% of the mass, seeded), theta = 6.25, leaf capacity 16,
 closure mode 2: the order-1 local expansion, the shipped MLP correction and
 the per-tick FP64 judge on 4096 sampled particles.  Beside it, the plain GPU FMM (the
 reference's far field, mode 0) on the same snapshot over a range of theta
@@ -64,7 +64,8 @@ METRIC = "ticks/s at N=1M, learned-closure vs plain GPU FMM at equal 1e-3 force 
 UNIT = "ticks/s"
 N_DEFAULT = 1 << 20
 ERROR_TARGET = 1e-3
-CLOSURE_THETA = 6.5        # the shipped weights' theta
+CLOSURE_THETA = 6.25       # operating point: every tick's judge <= 8.7e-4 with the shipped
+                           # weights (trained at theta 6.5); 6.0 sits at 9.8e-4
 CLOSURE_LEAF_CAP = 16      # leaf capacity of the closure's tree (PS_B200_OPT_LEAF_CAP)
 PLAIN_LEAF_CAP_THETAS = (8.0, 12.0)  # plain rows on the closure's leaf capacity
 CLOSURE_SEED = 424242      # snapshot seed (the weights were trained on other seeds)
@@ -74,7 +75,7 @@ WORKLOADS = {
     "closure": ("learned-closure FMM tick (ps_prepare_particles + ps_calc_forces, closure mode 2: "
                 "order-1 local expansion + BF16 MLP correction + FP64 judge on 4096 particles), "
                 "N=1,048,576 clumpy Plummer (a=1, r<=10a, plus 32 sub-clumps with 30% of the mass, "
-                "equal mass 1/N), theta=6.5, leaf capacity 16, float32 SoA"),
+                "equal mass 1/N), theta=6.25, leaf capacity 16, float32 SoA"),
     "plain": ("plain FMM tick (ps_prepare_particles + ps_calc_forces), Plummer sphere "
               "N=1,048,576, a=1, r<=10a, equal mass 1/N, theta=2, float32 SoA"),
 }

@@ -924,8 +924,8 @@ __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, u
             }
             const float dx0 = p0.x - t.x, dy0 = p0.y - t.y, dz0 = p0.z - t.z;
             const float dx1 = p1.x - t.x, dy1 = p1.y - t.y, dz1 = p1.z - t.z;
-            const float i0 = rsqrtf(fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0)) + 0.1f);
-            const float i1 = rsqrtf(fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1)) + 0.1f);
+            const float i0 = rsqrtf(fmaf(dx0, dx0, fmaf(dy0, dy0, fmaf(dz0, dz0, 0.1f))));
+            const float i1 = rsqrtf(fmaf(dx1, dx1, fmaf(dy1, dy1, fmaf(dz1, dz1, 0.1f))));
             const float f0 = w0 * (i0 * i0 * i0), f1 = w1 * (i1 * i1 * i1);
             ax = fmaf(dx0, f0, ax);
             ay = fmaf(dy0, f0, ay);
@@ -945,7 +945,7 @@ __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, u
                 ++used;
             }
             const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
-            const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f);
+            const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 0.1f))));
             const float f = w * (inv * inv * inv);
             ax = fmaf(dx, f, ax);
             ay = fmaf(dy, f, ay);
