@@ -246,9 +246,11 @@ def run_reference(args):
             "data": "synthetic (seeded clumpy Plummer)" if args.workload == "closure"
             else "synthetic (seeded Plummer sphere)",
             "config": {"workload": WORKLOADS[args.workload], "n": args.n, "theta": theta,
-                       "note": "the reference has only the plain far field; at this theta its "
-                               "error is ~10x the closure's, so it does less work than the "
-                               "1e-3 bound needs"} if args.workload == "closure"
+                       "leaf_cap": 1,
+                       "note": "the reference has only the plain far field on its own tree "
+                               "(leaf capacity 1); at this theta its error is ~10x the "
+                               "closure's, so it does less work than the 1e-3 bound needs"}
+            if args.workload == "closure"
             else {"workload": WORKLOADS[args.workload], "n": args.n, "theta": theta},
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
