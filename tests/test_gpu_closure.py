@@ -207,3 +207,24 @@ def test_shipped_weights_gain_over_the_method_without_them():
             mlp.append(j["median_mlp"])
             assert j["used"]
     assert np.mean(mlp) < 0.85 * np.mean(base), (base, mlp)
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no shipped closure weights")
+def test_shipped_weights_gain_on_leaf_capacity_16():
+    # the benchmark's tree: leaves of up to 16 particles; the judge must keep
+    # applying the correction and the correction must still pay
+    params, meta = CL.load(WEIGHTS)
+    n, theta = int(meta["n"]), float(meta["theta"])
+    base, mlp = [], []
+    with P.Context(n, theta=theta) as ctx:
+        ctx.closure_set_weights(params)
+        ctx.set_option(P.OPT_LEAF_CAP, 16)
+        ctx.set_closure(2)
+        for k in range(3):
+            p = W.clumpy_plummer(n, 56_000_000 + k)
+            ctx.tick(p, np.zeros(n, np.uint32))
+            j = ctx.closure_last()
+            assert j["used"]
+            base.append(j["median_base"])
+            mlp.append(j["median_mlp"])
+    assert np.mean(mlp) < 0.6 * np.mean(base), (base, mlp)
