@@ -60,10 +60,8 @@ constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-en
 constexpr int kP2PCap = 128;              // staged P2P sources of a group
 constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves at once
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
-constexpr uint32_t kDenseGroup = 1;       // DENSE: groups with this many leaf particles (all) go to k_dense_p2p
 constexpr uint32_t kDenseChunk = 32;      // target particles per dense work record
 constexpr uint32_t kDenseSwitch = 32;     // fullest leaf from which the DENSE leaf pass runs
-constexpr uint32_t kBigSource = 16;       // DENSE: sources this full are summed by all lanes
 
 enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
@@ -92,7 +90,6 @@ struct SmemLeaf {
     uint8_t cand_mask[kCandBuf];
     uint8_t stk_mask[kStackCap];
     uint8_t p2p_mask[kP2PCap];
-    uint8_t big[kP2PCap];   // staged sources with more than kBigSource particles
 };
 
 template <int MODE>
@@ -263,53 +260,33 @@ struct LeafOut {
 };
 
 // L2P + P2P of a group's leaf children once its candidates are done: with
-// DENSE, a group holding kDenseGroup or more leaf particles is handed to
-// k_dense_p2p; the others get F = m (L + P2P sum) here, one target particle
-// at a time with the lanes over its sources.
+// DENSE, every group is handed to k_dense_p2p (which adds L and the P2P sum);
+// otherwise F = m (L + P2P sum) here, one target particle at a time with the
+// lanes over its sources.
 template <bool DEBUG, bool GRAD, bool DENSE>
 __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uint32_t tgt_mask,
                                            uint32_t fc, uint32_t pfill, uint32_t phead,
                                            Status* status) {
     const uint32_t lane = lane_id();
-    // ---- full leaves (depth-10 cells with many particles) go to
-    // k_dense_p2p: the group's whole source list to HBM chunks,
-    // then one work record per 32 target particles ----
-    uint32_t dense_mask = 0;
     if constexpr (DENSE) {
-        uint32_t cnt = 0;
-        if (lane < 8 && ((tgt_mask >> lane) & 1u)) cnt = sm.cpart[lane].y;
-        if (warp_sum(cnt) >= kDenseGroup) dense_mask = tgt_mask;
-    }
-    if (DENSE && dense_mask) {
-        if (pfill) {
-            phead = spill_p2p(sm, pfill, phead, o.p2p, status);
-            pfill = 0;
+        // the group's whole source list to HBM chunks, then k_dense_p2p work
+        // records of up to 32 target particles
+        if (pfill) phead = spill_p2p(sm, pfill, phead, o.p2p, status);
+        record_dense(sm, tgt_mask, fc, phead, o.dense_rec, o.dense_cap, status);
+        if (DEBUG && lane == 0) {
+            for (uint32_t m = tgt_mask; m; m &= m - 1) {
+                const uint32_t q = __ffs(m) - 1;
+                o.dbg_p2p[fc + q] = sm.dbg_p2p[q];
+                atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS], (unsigned long long)sm.dbg_p2p[q]);
+            }
         }
-        record_dense(sm, dense_mask, fc, phead, o.dense_rec, o.dense_cap, status);
+        __syncwarp();
+        return;
     }
     // ---- L2P + P2P: F = m * (L(u) + sum of u's P2P sources) ----
-    // A lane takes whole source leaves; with DENSE, a source leaf holding more
-    // than kBigSource particles is shared by all lanes instead, so no lane
-    // walks a full leaf alone while the others wait.
-    uint32_t nbig = 0;
-    if constexpr (DENSE) {
-        for (uint32_t e0 = 0; e0 < pfill; e0 += 32) {
-            const uint32_t e = e0 + lane;
-            bool big = false;
-            if (e < pfill) {
-                const uint4 si = o.info[sm.p2p_node[e]];
-                sm.p2p_range[e] = make_uint2(si.x, si.y);
-                big = si.y > kBigSource;
-            }
-            const uint32_t bm = __ballot_sync(0xFFFFFFFFu, big);
-            if (big) sm.big[nbig + __popc(bm & lanemask_lt())] = (uint8_t)e;
-            nbig += __popc(bm);
-        }
-    } else {
-        for (uint32_t e = lane; e < pfill; e += 32) {
-            const uint4 si = o.info[sm.p2p_node[e]];
-            sm.p2p_range[e] = make_uint2(si.x, si.y);
-        }
+    for (uint32_t e = lane; e < pfill; e += 32) {
+        const uint4 si = o.info[sm.p2p_node[e]];
+        sm.p2p_range[e] = make_uint2(si.x, si.y);
     }
     __syncwarp();
     unsigned long long inter = 0;
@@ -318,66 +295,23 @@ __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uin
         const uint32_t q = __ffs(m) - 1;
         const uint2 up = sm.cpart[q];
         const float4 L = sm.sL[q];
-        for (uint32_t ti = 0; (!DENSE || !((dense_mask >> q) & 1u)) && ti < up.y; ++ti) {
+        for (uint32_t ti = 0; ti < up.y; ++ti) {
             const float4 t = o.xyzm[up.x + ti];
             float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
             for (uint32_t e = lane; e < pfill; e += 32) {
                 if ((sm.p2p_mask[e] >> q) & 1u) {
                     const uint2 r = sm.p2p_range[e];
-                    if (!DENSE || r.y <= kBigSource) {
-                        p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
-                        if (DEBUG) inter += r.y;
-                    }
+                    p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
+                    if (DEBUG) inter += r.y;
                 }
             }
-            if constexpr (DENSE) {
-                for (uint32_t b = 0; b < nbig; ++b) {
-                    const uint32_t e = sm.big[b];
-                    if (!((sm.p2p_mask[e] >> q) & 1u)) continue;
-                    const uint2 r = sm.p2p_range[e];
-                    for (uint32_t j = lane; j < r.y; j += 32) {
-                        p2p_range(o.xyzm, make_uint2(r.x + j, 1u), t, o.kahan, bx, by, bz, cx, cy,
-                                  cz);
-                        if (DEBUG) inter += 1;
-                    }
-                }
-            }
-            if constexpr (DENSE) {
-                for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
-                    const bool has = lane < o.p2p.cnt[c] &&
-                                     ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u);
-                    uint2 r = make_uint2(0u, 0u);
-                    if (has) {
-                        const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
-                        r = make_uint2(si.x, si.y);
-                    }
-                    const bool big = DENSE && has && r.y > kBigSource;
-                    if (has && !big) {
-                        p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
-                        if (DEBUG) inter += r.y;
-                    }
-                    if constexpr (DENSE) {
-                        for (uint32_t bm = __ballot_sync(0xFFFFFFFFu, big); bm; bm &= bm - 1) {
-                            const int l = __ffs(bm) - 1;
-                            const uint32_t bx0 = __shfl_sync(0xFFFFFFFFu, r.x, l);
-                            const uint32_t bn = __shfl_sync(0xFFFFFFFFu, r.y, l);
-                            for (uint32_t jj = lane; jj < bn; jj += 32) {
-                                p2p_range(o.xyzm, make_uint2(bx0 + jj, 1u), t, o.kahan, bx, by, bz,
-                                          cx, cy, cz);
-                                if (DEBUG) inter += 1;
-                            }
-                        }
-                    }
-                }
-            } else {
-                for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
-                    if (lane < o.p2p.cnt[c] &&
-                        ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
-                        const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
-                        p2p_range(o.xyzm, make_uint2(si.x, si.y), t, o.kahan, bx, by, bz,
-                                  cx, cy, cz);
-                        if (DEBUG) inter += si.y;
-                    }
+            for (uint32_t c = phead; c != kNone; c = o.p2p.next[c]) {
+                if (lane < o.p2p.cnt[c] &&
+                    ((o.p2p.mask[(size_t)c * kP2PChunk + lane] >> q) & 1u)) {
+                    const uint4 si = o.info[o.p2p.src[(size_t)c * kP2PChunk + lane]];
+                    p2p_range(o.xyzm, make_uint2(si.x, si.y), t, o.kahan, bx, by, bz,
+                              cx, cy, cz);
+                    if (DEBUG) inter += si.y;
                 }
             }
             const float sx = warp_sum(bx - cx);
