@@ -12,6 +12,7 @@
 namespace psg {
 
 constexpr int kDirThreads = 128;
+constexpr int kDirPer = 2;  // targets per thread
 
 // 1/sqrt(x) in FP64 for x >= 0.1 (softened squared distances): the hardware's
 // approximate reciprocal square root (PTX rsqrt.approx.ftz.f64) refined by two
@@ -37,18 +38,29 @@ __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __rest
                                                             const uint32_t* __restrict__ targets,
                                                             size_t n_targets, size_t chunk,
                                                             double* __restrict__ out) {
-    // the tile is widened to FP64 once per block, not once per pair
+    // the tile is widened to FP64 once per block, not once per pair; each
+    // thread owns kDirPer targets, so each tile read serves kDirPer pairs
     __shared__ double4 tile[kDirThreads];
-    const size_t k = (size_t)blockIdx.x * kDirThreads + threadIdx.x;
-    const uint32_t ti_raw = k < n_targets ? targets[k] : 0u;
-    const bool active = k < n_targets && ti_raw < n;
-    const uint32_t ti = active ? ti_raw : 0u;
-    const float4 t = active ? xyzm[ti] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const double tx = (double)t.x, ty = (double)t.y, tz = (double)t.z;
+    size_t k[kDirPer];
+    bool active[kDirPer];
+    double tx[kDirPer], ty[kDirPer], tz[kDirPer], tm[kDirPer];
+    double ax[kDirPer], ay[kDirPer], az[kDirPer];
+#pragma unroll
+    for (int p = 0; p < kDirPer; ++p) {
+        k[p] = (size_t)blockIdx.x * (kDirThreads * kDirPer) + (size_t)p * kDirThreads +
+               threadIdx.x;
+        const uint32_t ti_raw = k[p] < n_targets ? targets[k[p]] : 0u;
+        active[p] = k[p] < n_targets && ti_raw < n;
+        const float4 t = active[p] ? xyzm[ti_raw] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tx[p] = (double)t.x;
+        ty[p] = (double)t.y;
+        tz[p] = (double)t.z;
+        tm[p] = (double)t.w;
+        ax[p] = ay[p] = az[p] = 0.0;
+    }
     const double eps2 = (double)0.1f;
     const size_t src0 = (size_t)blockIdx.y * chunk;
     const size_t src1 = src0 + chunk < n ? src0 + chunk : n;
-    double ax = 0.0, ay = 0.0, az = 0.0;
     for (size_t j0 = src0; j0 < src1; j0 += kDirThreads) {
         const size_t j = j0 + threadIdx.x;
         const float4 sj = j < src1 ? xyzm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -57,31 +69,36 @@ __global__ void __launch_bounds__(kDirThreads) k_direct_f64(const float4* __rest
         const int cnt = (int)((src1 - j0) < (size_t)kDirThreads ? (src1 - j0) : kDirThreads);
         for (int q = 0; q < cnt; ++q) {
             const double4 s = tile[q];
-            const double dx = s.x - tx;
-            const double dy = s.y - ty;
-            const double dz = s.z - tz;
-            const double r2 = dx * dx + dy * dy + dz * dz + eps2;
-            const double ir = rsqrt_newton(r2);
-            // the self pair (and any source at the target's position) has
-            // d = 0 and adds exactly 0, as j != i excludes it in the sum
-            const double w = s.w * ir * ir * ir;
-            ax += dx * w;
-            ay += dy * w;
-            az += dz * w;
+#pragma unroll
+            for (int p = 0; p < kDirPer; ++p) {
+                const double dx = s.x - tx[p];
+                const double dy = s.y - ty[p];
+                const double dz = s.z - tz[p];
+                const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+                const double ir = rsqrt_newton(r2);
+                // the self pair (and any source at the target's position) has
+                // d = 0 and adds exactly 0, as j != i excludes it in the sum
+                const double w = s.w * ir * ir * ir;
+                ax[p] += dx * w;
+                ay[p] += dy * w;
+                az[p] += dz * w;
+            }
         }
         __syncthreads();
     }
-    if (k < n_targets && !active && blockIdx.y == 0) {
-        const double nan = __longlong_as_double(0x7FF8000000000000ll);
-        atomicAdd(&out[3 * k + 0], nan);
-        atomicAdd(&out[3 * k + 1], nan);
-        atomicAdd(&out[3 * k + 2], nan);
-    }
-    if (active) {
-        const double m = (double)t.w;
-        atomicAdd(&out[3 * k + 0], m * ax);
-        atomicAdd(&out[3 * k + 1], m * ay);
-        atomicAdd(&out[3 * k + 2], m * az);
+#pragma unroll
+    for (int p = 0; p < kDirPer; ++p) {
+        if (k[p] < n_targets && !active[p] && blockIdx.y == 0) {
+            const double nan = __longlong_as_double(0x7FF8000000000000ll);
+            atomicAdd(&out[3 * k[p] + 0], nan);
+            atomicAdd(&out[3 * k[p] + 1], nan);
+            atomicAdd(&out[3 * k[p] + 2], nan);
+        }
+        if (active[p]) {
+            atomicAdd(&out[3 * k[p] + 0], tm[p] * ax[p]);
+            atomicAdd(&out[3 * k[p] + 1], tm[p] * ay[p]);
+            atomicAdd(&out[3 * k[p] + 2], tm[p] * az[p]);
+        }
     }
 }
 
@@ -89,7 +106,7 @@ void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, si
                        double* out, int blocks, cudaStream_t st) {
     if (n_targets == 0) return;
     cudaMemsetAsync(out, 0, n_targets * 3 * sizeof(double), st);
-    const size_t tblocks = (n_targets + kDirThreads - 1) / kDirThreads;
+    const size_t tblocks = (n_targets + kDirThreads * kDirPer - 1) / (kDirThreads * kDirPer);
     // about `blocks` blocks in total, each source chunk at least 1024 particles
     size_t splits = ((size_t)blocks + tblocks - 1) / tblocks;
     const size_t max_splits = (n + 1023) / 1024;
