@@ -242,13 +242,22 @@ def test_error_results():
         assert e.value.code == P.PS_EINVAL
 
 
-def test_kahan_option_is_at_least_as_accurate(oracle):
-    p = W.plummer(20000, 21)
+# (particles, leaf capacity, plain-vs-Kahan bound: L2, per particle): the
+# sparse leaf pass, and the full-leaf kernel (sub-clumps, leaf capacity 16)
+# with its tiles and direct few-target walks, whose sums run over thousands
+# of sources
+KAHAN_CASES = [(lambda: W.plummer(20000, 21), 1, 1e-6, 1e-5),
+               (lambda: W.clumpy_plummer(20000, 22), 16, 1e-5, 1e-3)]
+
+
+@pytest.mark.parametrize("gen,cap,l2,mx", KAHAN_CASES, ids=["plummer", "clumpy_b16"])
+def test_kahan_option_is_at_least_as_accurate(oracle, gen, cap, l2, mx):
+    p = gen()
     src = p.copy()
     a, b = p.copy(), p.copy()
-    gpu_tick(a, 8.0, debug=False)
-    gpu_tick(b, 8.0, debug=False, kahan=True)
-    assert_forces_close(forces(b), forces(a), l2=1e-6, mx=1e-5)
+    gpu_tick(a, 8.0, debug=False, leaf_cap=cap)
+    gpu_tick(b, 8.0, debug=False, kahan=True, leaf_cap=cap)
+    assert_forces_close(forces(b), forces(a), l2=l2, mx=mx)
     f64 = oracle.direct_f64(src)
     err_a = rel_l2(forces(a), f64[a.id])
     err_b = rel_l2(forces(b), f64[b.id])
