@@ -799,8 +799,6 @@ struct DenseTile {
 };
 
 // one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
-// a source counts only if its child mask holds the target's leaf q
-// one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
 // a source counts only if its child mask holds the target's leaf q.  Plain
 // sums alternate between two accumulator sets (independent FMA chains),
 // added at the end of the tile.
