@@ -74,16 +74,19 @@ ps_result_t ps_b200_direct_f64(ps_context_t* ctx, const ps_particle_arrs_t* arrs
 /* ps_prepare_particles for callers that cannot allocate memory.  No
  * counterpart in the reference.  The regular ps_prepare_particles creates a
  * workspace (device buffers, a stream, a pinned buffer) on its first call;
- * callers with a fixed, pre-reserved memory budget, or code recording into a
- * CUDA graph where cudaMalloc is not allowed, cannot let it.  This variant
- * allocates nothing: its scratch (the per-block partial bounding boxes) is a
- * static 32 KB device array loaded with the library.
+ * callers with a fixed, pre-reserved memory budget that forbid allocation
+ * inside their frame loop (so a frame never stalls on the allocator or fails
+ * for want of memory) cannot let it.  This variant allocates nothing: its
+ * scratch (the per-block partial bounding boxes) is a static 32 KB device
+ * array loaded with the library.
  *   - arrs->x, y, z and out_morton_codes must be device memory; the three
  *     float outputs are host pointers (any may be NULL), same meaning as in
  *     ps_prepare_particles.
  *   - arrs->cnt must be 1 .. 4,194,304; larger counts return PS_EINVAL.
- *   - The first call on a device resolves the scratch's device address;
- *     make it before any stream capture.
+ *   - The first call on a device resolves the scratch's device address and
+ *     keeps it for that device; make it before any stream capture.  After a
+ *     cudaDeviceReset that kept address is stale: do not mix this call with
+ *     device resets in one process.
  *   - Runs on the legacy default stream and returns when the results are
  *     final.  All calls share the one scratch array: calls that overlap on
  *     the GPU race, so serialise them. */

@@ -14,10 +14,11 @@
 #                                   fast-math, no FMA contraction): used to
 #                                   show the fast-math build computes the same
 #                                   Morton codes, order, tree and MAC decisions.
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]
+#   (default: $PS_REFERENCE_ROOT, else the checkout beside this repository)
 set -eu
-REF=${1:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${1:-${PS_REFERENCE_ROOT:-$HERE/../../reference}}
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/polesitter.h" ]; then
   echo "reference header not found under $REF; skipping" >&2

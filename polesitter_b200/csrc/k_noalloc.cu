@@ -5,10 +5,10 @@
 // first call (a stream, a device buffer for the per-block partial bounding
 // boxes, a pinned result buffer, and device mirrors when the caller passes
 // host arrays).  Some callers cannot allow that: an engine that reserves all
-// device memory up front and forbids allocation inside its frame loop (the
-// reference itself is built on the rule that the library never allocates,
-// polesitter.h:20-24), or code that records its work into a CUDA graph, where
-// cudaMalloc is not permitted.  This entry point allocates nothing: its only
+// device memory up front and forbids allocation inside its frame loop, so
+// that a frame never stalls on the allocator or fails half-way for want of
+// memory (the reference itself is built on the rule that the library never
+// allocates, polesitter.h:20-24).  This entry point allocates nothing: its only
 // scratch -- the partial boxes and the final box -- lives in the file-scope
 // device array below, of fixed size, loaded with the library.
 //
@@ -18,8 +18,11 @@
 //   * cnt must be 1 .. kNoAllocMaxParticles (4,194,304); larger counts are
 //     rejected with PS_EINVAL and a message in ps_b200_last_error().
 //   * The first call on each device resolves the scratch array's device
-//     address (cudaGetSymbolAddress) and caches it; make that first call
-//     before any stream capture.
+//     address (cudaGetSymbolAddress) and caches it for that device; make
+//     that first call before any stream capture.  The cached address belongs
+//     to the device's context at that time: after cudaDeviceReset the next
+//     call would pass a stale address, so do not mix this entry point with
+//     device resets in one process.
 //   * Work runs on the legacy default stream and the call returns after the
 //     codes and the box are final.  All calls share the one scratch array, so
 //     calls that overlap on the GPU (e.g. from several host threads) race;
@@ -79,7 +82,10 @@ extern "C" int psg_prepare_noalloc(const float* x, const float* y, const float* 
                                    uint32_t* codes, float* out_min, float* out_max,
                                    float* out_range, int variant) {
     using namespace psg;
-    if (!x || !y || !z || !codes || n == 0) return PSG_EINVAL;
+    if (!x || !y || !z || !codes || n == 0) {
+        psg_set_error("ps_b200_prepare_particles_noalloc: null array or zero count");
+        return PSG_EINVAL;
+    }
     if (n > kNoAllocMaxParticles) {
         char msg[160];
         std::snprintf(msg, sizeof(msg),

@@ -366,6 +366,7 @@ ps_result_t ps_b200_prepare_particles_noalloc(ps_particle_arrs_t* arrs,
                                               uint32_t* out_morton_codes, float* out_min_b,
                                               float* out_max_b, float* out_range) {
     if (!arrs || !out_morton_codes || arrs->cnt == 0) {
+        psg_set_error("ps_b200_prepare_particles_noalloc: null argument or zero count");
         return PS_EINVAL;
     }
     return to_ps(psg_prepare_noalloc(arrs->x, arrs->y, arrs->z, arrs->cnt, out_morton_codes,

@@ -68,7 +68,9 @@ def _probe_layout(include_dir):
 
 def test_struct_layout_and_result_codes_match_reference():
     ours = _probe_layout(INCLUDE)
-    ref_dir = "/root/reference/src"
+    ref_root = os.environ.get("PS_REFERENCE_ROOT",
+                              os.path.join(os.path.dirname(ROOT), "reference"))
+    ref_dir = os.path.join(ref_root, "src")
     if not os.path.exists(os.path.join(ref_dir, "polesitter.h")):
         # the reference's layout, restated: ps_config_t (polesitter.h:304-310)
         # and ps_particle_arrs_t (:312-322) on LP64, enum values (:294-300)
