@@ -29,6 +29,24 @@ size_t ps_b200_context_size(void);
                                         holding more than B particles is split (the
                                         reference: 1, polesitter.h:911); the root is split
                                         whenever it holds 2 or more */
+#define PS_B200_OPT_NEAR_LEVELS 11   /* store near lists for node depths <= this at most
+                                        (2..10, default 10); leaf groups below walk their
+                                        ancestor chains instead.  The library lowers it by
+                                        itself when the lists would not fit (plain far field
+                                        only), so every theta runs; the interaction set is
+                                        the same either way */
+#define PS_B200_OPT_STREAM 12        /* 1: sum each leaf group's P2P in the leaf pass as its
+                                        sources are found, with no source list in device
+                                        memory (chosen by the library when the lists would
+                                        not fit) */
+#define PS_B200_OPT_SHRINK_STORES 13 /* 1: shrink the traversal's growable stores (near
+                                        lists, P2P chunks, full-leaf records) to their
+                                        minimum now; the next tick grows them again */
+#define PS_B200_OPT_SORT_SPIN 14     /* test of the sort's bounded wait: > 0 lets a tile's
+                                        look-back poll only this many times while the first
+                                        tile of the first pass publishes ~200 us late; the
+                                        tick then returns PS_EDEVICE; 0 (default) restores
+                                        the normal limit */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
 
 /* Morton quantisation of ps_prepare_particles, process-wide (it takes no
@@ -40,7 +58,8 @@ ps_result_t ps_b200_set_morton_variant(int variant);
  * particle pairs, [9] deepest traversal stack (these need
  * PS_B200_OPT_DEBUG), [8] nodes, [10] P2P list chunks, [11] traversal runs
  * (> 1 when a capacity had to grow), [12] particles in the fullest leaf,
- * [13] full-leaf P2P work records */
+ * [13] full-leaf P2P work records, [14] deepest level whose near lists were
+ * stored, [15] 1 when the P2P was streamed */
 ps_result_t ps_b200_get_stats(ps_context_t* ctx, uint64_t* out, size_t n);
 
 /* per-phase device times of the last tick in ms (PS_B200_OPT_TIMING):

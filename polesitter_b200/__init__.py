@@ -27,6 +27,7 @@ RESULT_NAMES = {0: "PS_OK", -1: "PS_EOOM", -2: "PS_EINVAL", -3: "PS_ETHRD",
 OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN, OPT_CLOSURE, OPT_JUDGE = 1, 2, 4, 6, 7, 8
 OPT_HEAVY_DEPTH = 9
 OPT_LEAF_CAP = 10
+OPT_NEAR_LEVELS, OPT_STREAM, OPT_SHRINK_STORES, OPT_SORT_SPIN = 11, 12, 13, 14
 CLOSURE_PARAMS = 9928
 MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 
@@ -303,7 +304,8 @@ class Context:
                 "chunks_dfs": int(out[5]), "tests_first": int(out[6]), "tests_dfs": int(out[7]),
                 "nodes": int(out[8]), "max_stack": int(out[9]), "p2p_chunks": int(out[10]),
                 "traversal_runs": int(out[11]), "max_leaf": int(out[12]),
-                "dense_records": int(out[13]),
+                "dense_records": int(out[13]), "near_levels": int(out[14]),
+                "streamed": int(out[15]),
                 "lanes": int(out[16]), "leaf_groups": int(out[17]), "dfs_steps": int(out[18]),
                 "full_leaf_interactions": int(out[20]),
                 "slowest_group_cycles": int(out[19]) >> 28,

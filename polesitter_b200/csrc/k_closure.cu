@@ -539,9 +539,10 @@ void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const 
 }
 
 void launch_judge_direct(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
-                         uint32_t tick, int blocks, cudaStream_t st) {
+                         uint32_t tick, int blocks, cudaStream_t st, double* part,
+                         size_t part_doubles) {
     k_judge_sample<<<(s + 255) / 256, 256, 0, st>>>(tg, s, n, tick);
-    launch_direct_f64(xyzm, n, tg, (size_t)s, f64, blocks, st);
+    launch_direct_f64(xyzm, n, tg, (size_t)s, f64, blocks, st, part, part_doubles);
 }
 
 void launch_judge_decide(const uint32_t* tg, int s, const double* f64, const float* fx,

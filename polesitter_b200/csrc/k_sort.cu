@@ -22,6 +22,13 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
 constexpr int kSpinLimit = 1 << 22;
+constexpr unsigned long long kLateNs = 200000;  // the late tile of the wait test: 200 us
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 int sort_tile_size() { return kSortTile; }
 
@@ -67,7 +74,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int pass,
     const uint32_t* __restrict__ offs /*[4][256]*/, uint32_t* lookback /*[tiles][256]*/,
-    uint32_t* ticket, Status* status) {
+    uint32_t* ticket, Status* status, int spin_limit, int late) {
     __shared__ uint32_t s_wcnt[kSortWarps][256];
     __shared__ uint32_t s_keys[kSortTile];
     __shared__ uint32_t s_vals[kSortTile];
@@ -123,6 +130,14 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
     uint32_t* my = lookback + (size_t)tile * 256 + t;
     uint32_t prefix = 0;
     if (tile == 0) {
+        if (late) {
+            // test of the bounded wait: this tile publishes ~200 us late, so
+            // a successor polling fewer times gives up (bounded: at most
+            // 2^20 reads of the clock)
+            const unsigned long long t0 = global_ns();
+            for (int i = 0; i < (1 << 20) && global_ns() - t0 < kLateNs; ++i) {
+            }
+        }
         atomicExch(my, kFlagInc | total);
     } else {
         atomicExch(my, kFlagAgg | total);
@@ -132,7 +147,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
             uint32_t v = *((volatile uint32_t*)(lookback + (size_t)j * 256 + t));
             uint32_t f = v & ~kValMask;
             if (f == 0u) {
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit) {
                     set_err(status, PSG_ERR_SORT_SPIN);
                     break;
                 }
@@ -213,7 +228,10 @@ __global__ void __launch_bounds__(256) k_writeback(const float4* __restrict__ xy
 }
 
 void launch_sort(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* status,
-                 cudaStream_t st) {
+                 cudaStream_t st, int spin_limit) {
+    // spin_limit > 0: the wait test (that many polls; the first tile of the
+    // first pass publishes late)
+    const int limit = spin_limit > 0 ? spin_limit : kSpinLimit;
     const int tiles = (int)((n + kSortTile - 1) / kSortTile);
     cudaMemsetAsync(b.hist, 0, 4 * 256 * sizeof(uint32_t), st);
     cudaMemsetAsync(b.lookback, 0, (size_t)4 * tiles * 256 * sizeof(uint32_t), st);
@@ -227,7 +245,8 @@ void launch_sort(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* st
     for (int p = 0; p < 4; ++p) {
         k_sort_pass<<<tiles, kSortThreads, 0, st>>>(kin, vin, kouts[p], vouts[p], n, p, b.offs,
                                                    b.lookback + (size_t)p * tiles * 256,
-                                                   status->sort_tiles + p, status);
+                                                   status->sort_tiles + p, status, limit,
+                                                   spin_limit > 0 && p == 0 ? 1 : 0);
         kin = kouts[p];
         vin = vouts[p];
     }

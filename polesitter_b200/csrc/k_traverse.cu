@@ -76,6 +76,7 @@ struct SmemInternal {
 
 struct SmemLeaf {
     float4 cgeo[8];
+    float4 chain_geo[8];    // chain groups: the ancestors a_{K+1} .. p under test
     float4 sL[8];           // the children's local fields
     float4 sG0[8];          // closure order 1: the children's field gradients
     float2 sG1[8];
@@ -90,6 +91,8 @@ struct SmemLeaf {
     uint8_t cand_mask[kCandBuf];
     uint8_t stk_mask[kStackCap];
     uint8_t p2p_mask[kP2PCap];
+    uint8_t cand_lvl[kCandBuf];  // 0: tested against the children in the mask;
+    uint8_t stk_lvl[kStackCap];  // c > 0: against chain target c (chain groups)
 };
 
 template <int MODE>
@@ -259,6 +262,96 @@ struct LeafOut {
     int kahan;
 };
 
+// STREAM: the P2P sums of the staged sources [0, pfill) for every target
+// particle of the work item's leaf children (tgt_mask), computed where they
+// are found instead of spilled to HBM, so that no store grows with the size
+// of a source list.  The children's particles are enumerated flat (children
+// in mask order), 32 at a time; T lanes own targets (T the smallest power of
+// two >= their count) and the 32 / T slices of lanes split the staged source
+// leaves.  The slices' sums are added in a fixed order and kept in the force
+// arrays between flushes (accum: add to what an earlier flush of this item
+// left there).  fin: the item's last flush, which also applies L2P,
+// F = m (L + all P2P sums), with order 1's shift to the particle.
+template <bool DEBUG, bool GRAD>
+__device__ __noinline__ void stream_p2p(SmemLeaf& sm, const LeafOut& o, uint32_t tgt_mask,
+                                        uint32_t fc, uint32_t pfill, bool accum, bool fin,
+                                        unsigned long long& inter) {
+    const uint32_t lane = lane_id();
+    for (uint32_t e = lane; e < pfill; e += 32) {
+        const uint4 si = o.info[sm.p2p_node[e]];
+        sm.p2p_range[e] = make_uint2(si.x, si.y);
+    }
+    __syncwarp();
+    uint32_t total = 0;
+    for (uint32_t m = tgt_mask; m; m &= m - 1) total += sm.cpart[__ffs(m) - 1].y;
+    for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+        const uint32_t cnt = min(32u, total - r0);
+        uint32_t T = 1;
+        while (T < cnt) T <<= 1;
+        const uint32_t S = 32u / T, tl = lane & (T - 1u), slice = lane / T;
+        const bool active = tl < cnt;
+        const uint32_t f = r0 + (active ? tl : 0u);
+        uint32_t q = 0, i = 0, acc = 0;
+        for (uint32_t m = tgt_mask; m; m &= m - 1) {
+            const uint32_t qq = __ffs(m) - 1;
+            const uint2 cp = sm.cpart[qq];
+            if (f >= acc && f < acc + cp.y) {
+                q = qq;
+                i = cp.x + (f - acc);
+            }
+            acc += cp.y;
+        }
+        const float4 t = o.xyzm[i];
+        float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+        uint32_t used = 0;
+        for (uint32_t e = slice; e < pfill; e += S) {
+            if ((sm.p2p_mask[e] >> q) & 1u) {
+                const uint2 r = sm.p2p_range[e];
+                p2p_range(o.xyzm, r, t, o.kahan, bx, by, bz, cx, cy, cz);
+                used += r.y;
+            }
+        }
+        bx -= cx;
+        by -= cy;
+        bz -= cz;
+        for (uint32_t d = T; d < 32u; d <<= 1) {
+            bx += __shfl_xor_sync(0xFFFFFFFFu, bx, d);
+            by += __shfl_xor_sync(0xFFFFFFFFu, by, d);
+            bz += __shfl_xor_sync(0xFFFFFFFFu, bz, d);
+        }
+        if (DEBUG) inter += active ? used : 0u;
+        if (active && slice == 0) {
+            if (accum) {
+                bx += o.fx[i];
+                by += o.fy[i];
+                bz += o.fz[i];
+            }
+            if (!fin) {
+                o.fx[i] = bx;
+                o.fy[i] = by;
+                o.fz[i] = bz;
+            } else {
+                const float4 L = sm.sL[q];
+                float lx = L.y, ly = L.z, lz = L.w;
+                if constexpr (GRAD) {
+                    const float4 cu = sm.cgeo[q];
+                    const float3 sh = grad_apply(sm.sG0[q], sm.sG1[q], t.x - cu.x, t.y - cu.y,
+                                                 t.z - cu.z);
+                    lx += sh.x;
+                    ly += sh.y;
+                    lz += sh.z;
+                    if (o.leaf_of) o.leaf_of[i] = fc + q;
+                }
+                const double mm = (double)t.w;
+                o.fx[i] = (float)(mm * ((double)lx + (double)bx));
+                o.fy[i] = (float)(mm * ((double)ly + (double)by));
+                o.fz[i] = (float)(mm * ((double)lz + (double)bz));
+            }
+        }
+    }
+    __syncwarp();
+}
+
 // L2P + P2P of a group's leaf children once its candidates are done: with
 // DENSE, every group is handed to k_dense_p2p (which adds L and the P2P sum);
 // otherwise F = m (L + P2P sum) here, one target particle at a time with the
@@ -266,8 +359,28 @@ struct LeafOut {
 template <bool DEBUG, bool GRAD, bool DENSE>
 __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uint32_t tgt_mask,
                                            uint32_t fc, uint32_t pfill, uint32_t phead,
-                                           Status* status) {
+                                           bool stream, bool flushed,
+                                           unsigned long long inter0, Status* status) {
     const uint32_t lane = lane_id();
+    if (stream) {
+        // the staged remainder, then L2P, in the warp (no spill, no records)
+        unsigned long long inter = inter0;
+        stream_p2p<DEBUG, GRAD>(sm, o, tgt_mask, fc, pfill, flushed, true, inter);
+        if (DEBUG) {
+            if (lane == 0) {
+                for (uint32_t m = tgt_mask; m; m &= m - 1) {
+                    const uint32_t q = __ffs(m) - 1;
+                    o.dbg_p2p[fc + q] = sm.dbg_p2p[q];
+                    atomicAdd(&status->stat[PSG_STAT_P2P_PAIRS],
+                              (unsigned long long)sm.dbg_p2p[q]);
+                }
+            }
+            inter = warp_sum(inter);
+            if (lane == 0) atomicAdd(&status->stat[PSG_STAT_P2P_INTER], inter);
+        }
+        __syncwarp();
+        return;
+    }
     if constexpr (DENSE) {
         // the group's whole source list to HBM chunks, then k_dense_p2p work
         // records of up to 32 target particles
@@ -353,8 +466,16 @@ __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uin
 // DENSE (leaf pass only): the variant for trees whose fullest leaf holds at
 // least kDenseSwitch particles, which hands full leaves to k_dense_p2p.  Both
 // variants are launched; each returns at once unless the tree is its kind.
-template <int MODE, bool DEBUG, bool GRAD, bool DENSE>
-__global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
+// XL (leaf pass only): the variant that also serves chain groups and
+// streamed P2P, launched only when the near lists stop short of the deepest
+// level or the P2P is streamed, so the other variants keep their registers.
+// The plain sparse leaf variant (the reference's tree and far field) keeps
+// 7 blocks per SM (72 registers).
+template <int MODE, bool DEBUG, bool GRAD, bool DENSE, bool XL>
+__global__ void __launch_bounds__(kTravThreads,
+                                  (MODE == MODE_LEAF && !DEBUG && !GRAD && !DENSE && !XL) ? 7
+                                                                                          : 1)
+    k_trav(TravArgs A) {
     using Smem = typename SmemOf<MODE>::T;
     __shared__ Smem smem[kTravWarps];
     const uint32_t lane = lane_id();
@@ -364,6 +485,8 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
     if (MODE == MODE_LEAF && ((status->max_leaf >= kDenseSwitch) != DENSE)) return;
+    // a shallower level's near lists did not fit: this level's are void
+    if (MODE == MODE_INTERNAL && (status->ns_fail & ((1u << A.level) - 1u))) return;
     const float theta2 = __fmul_rn(A.theta, A.theta);
 
     // group index space: MODE_INTERNAL = the nodes at depth k-1; MODE_LEAF =
@@ -454,13 +577,41 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     if (DEBUG) sm.dbg_p2p[lane] = 0;
                 }
             }
-            const float4 Lp = tv.lt[pid];
+            // chain group (leaf pass, parent deeper than the near lists
+            // reach, K = ns_levels): start from the near list of p's ancestor
+            // a at depth K and test its candidates down p's ancestor chain
+            // a_{K+1} .. a_dp = p, as the reference's pair recursion does
+            // (polesitter.h:1097-1145); what p is not separated from is
+            // opened for the leaf children.  No near list below depth K is
+            // stored, so nothing grows with theta.
+            uint32_t nchain = 0, bnode = pid;
+            if constexpr (MODE == MODE_LEAF) {
+                if (XL && (int)dp > A.ns_levels) {
+                    nchain = dp - (uint32_t)A.ns_levels;
+                    uint32_t a = pid;
+                    if (lane == 0) {
+                        for (uint32_t c = nchain; c > 0; --c) {
+                            sm.chain_geo[c - 1] = tv.geo[a];
+                            a = tv.parent[a];
+                        }
+                    }
+                    bnode = __shfl_sync(0xFFFFFFFFu, a, 0);
+                    __syncwarp();
+                    if (GRAD) {
+                        // order 1 needs every ancestor's own gradient: chain
+                        // groups serve the reference's order 0 only
+                        if (lane == 0) set_err(status, PSG_ERR_CHAIN_ORDER);
+                        continue;
+                    }
+                }
+            }
+            const float4 Lp = tv.lt[bnode];
             const bool root_only = dp <= 1;
             const uint32_t* nsl = nullptr;
             uint32_t nsn = 0;
             if (!root_only) {
-                nsl = A.ns + tv.ns_off[pid];
-                nsn = tv.ns_cnt[pid];
+                nsl = A.ns + tv.ns_off[bnode];
+                nsn = tv.ns_cnt[bnode];
             }
             // MODE_INTERNAL: reserve |cand| near-list entries per target child
             uint32_t cand_total = 1;
@@ -492,7 +643,10 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 }
                 ns_base = sm.ns_next;
                 ns_ok = ns_base + need <= A.ns_cap;
-                if (!ns_ok && lane == 0) set_err(status, PSG_ERR_NS_OVERFLOW);
+                if (!ns_ok && lane == 0) {
+                    set_err(status, PSG_ERR_NS_OVERFLOW);
+                    atomicOr(&status->ns_fail, 1u << A.level);
+                }
                 __syncwarp();
                 if (lane == 0) sm.ns_next = ns_base + need;
             }
@@ -511,6 +665,9 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
             uint32_t ssize = 0, e0 = 0;
             uint32_t pfill = 0, phead = kNone;  // MODE_LEAF: staged / spilled P2P sources
             bool root_pending = root_only;
+            float cacc0 = 0.f, cacc1 = 0.f, cacc2 = 0.f;  // chain groups: ancestors' M2L
+            bool flushed = false;                         // STREAM: a flush has run
+            unsigned long long sinter = 0;                // ... its pairs (debug)
 
             for (;;) {
                 // ---- next batch of candidates into cand[0, tot) ----
@@ -519,6 +676,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     if (lane == 0) {
                         sm.cand_node[0] = 0;  // the root
                         sm.cand_mask[0] = (uint8_t)tgt_mask;
+                        if constexpr (MODE == MODE_LEAF && XL) sm.cand_lvl[0] = 0;
                     }
                     tot = 1;
                     root_pending = false;
@@ -540,29 +698,36 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     for (uint32_t i = 0; i < c; ++i) {
                         sm.cand_node[ex + i] = lf ? s0 : (link & kLinkMask) + i;
                         sm.cand_mask[ex + i] = (uint8_t)tgt_mask;
+                        if constexpr (MODE == MODE_LEAF && XL)
+                            sm.cand_lvl[ex + i] = nchain ? 1 : 0;
                     }
                     e0 += 32;
                 } else if (MODE == MODE_LEAF && ssize > 0) {
-                    // pop entries (bounded so the stack cannot overflow), open them
+                    // pop entries (bounded so the stack cannot overflow) and
+                    // open them: an internal node's candidates are its
+                    // children, a leaf's (pushed by a chain test) itself
                     const int room = ((int)kStackCap - kStackSlack - (int)ssize) / 7;
                     const uint32_t kp = (uint32_t)min(32, min((int)ssize, max(1, room)));
-                    uint32_t node = 0, mask = 0;
+                    uint32_t node = 0, mask = 0, lvl = 0;
                     if constexpr (MODE == MODE_LEAF) {
                         if (lane < kp) {
                             node = sm.stk_node[ssize - kp + lane];
                             mask = sm.stk_mask[ssize - kp + lane];
+                            if constexpr (XL) lvl = sm.stk_lvl[ssize - kp + lane];
                         }
                     }
                     __syncwarp();
                     ssize -= kp;
                     const uint32_t link = lane < kp ? tv.link[node] : 0u;
                     const uint32_t nch = link >> 28;
-                    const uint32_t inc = warp_incl_scan(nch);
+                    const uint32_t c = lane < kp ? (XL && nch == 0 ? 1u : nch) : 0u;
+                    const uint32_t inc = warp_incl_scan(c);
                     tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
-                    const uint32_t ex = inc - nch;
-                    for (uint32_t i = 0; i < nch; ++i) {
-                        sm.cand_node[ex + i] = (link & kLinkMask) + i;
+                    const uint32_t ex = inc - c;
+                    for (uint32_t i = 0; i < c; ++i) {
+                        sm.cand_node[ex + i] = nch ? (link & kLinkMask) + i : node;
                         sm.cand_mask[ex + i] = (uint8_t)mask;
+                        if constexpr (MODE == MODE_LEAF && XL) sm.cand_lvl[ex + i] = (uint8_t)lvl;
                     }
                 } else {
                     break;
@@ -571,25 +736,28 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
 
                 // ---- test the candidates, one per lane; the next chunk's node
                 // records are loaded while the current one is processed ----
-                uint32_t n_s = 0, n_mask = 0, n_link = 0;
+                uint32_t n_s = 0, n_mask = 0, n_link = 0, n_lvl = 0;
                 float4 n_g = make_float4(0.f, 0.f, 0.f, 0.f), n_mp = n_g;
                 if (lane < tot) {
                     n_s = sm.cand_node[lane];
                     n_mask = sm.cand_mask[lane];
+                    if constexpr (MODE == MODE_LEAF && XL) n_lvl = sm.cand_lvl[lane];
                     n_g = tv.geo[n_s];
                     n_mp = tv.mp[n_s];
                     n_link = tv.link[n_s];
                 }
 #pragma unroll 1
                 for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
-                    const uint32_t s = n_s, smask = n_mask, slink = n_link;
+                    const uint32_t s = n_s, smask = n_mask, slink = n_link, slvl = n_lvl;
                     const float4 sg = n_g, smp = n_mp;
                     {
                         const uint32_t jn = j0 + 32 + lane;
                         n_mask = 0;
+                        n_lvl = 0;
                         if (jn < tot) {
                             n_s = sm.cand_node[jn];
                             n_mask = sm.cand_mask[jn];
+                            if constexpr (MODE == MODE_LEAF && XL) n_lvl = sm.cand_lvl[jn];
                             n_g = tv.geo[n_s];
                             n_mp = tv.mp[n_s];
                             n_link = tv.link[n_s];
@@ -651,12 +819,46 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                         }
                     } else {
                         const bool sleaf = (slink >> 28) == 0;
+                        // chain candidates: the MAC against their ancestor
+                        // target; separated -> M2L into the chain's field,
+                        // else opened for the next ancestor (past p: for the
+                        // leaf children, with the whole target mask)
+                        bool cpush = false;
+                        uint32_t cmask = 0, clvl = 0;
+                        if (XL && nchain && __any_sync(0xFFFFFFFFu, slvl != 0)) {
+                            if (slvl) {
+                                const float4 cg = sm.chain_geo[slvl - 1];
+                                float dx, dy, dz, d2;
+                                if (mac_separated(cg.x, cg.y, cg.z, cg.w, sg.x, sg.y, sg.z, sg.w,
+                                                  theta2, dx, dy, dz, d2)) {
+                                    float fx, fy, fz;
+                                    m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
+                                    cacc0 += fx;
+                                    cacc1 += fy;
+                                    cacc2 += fz;
+                                } else {
+                                    cpush = true;
+                                    cmask = slvl == nchain ? tgt_mask : 0u;
+                                    clvl = slvl == nchain ? 0u : slvl + 1;
+                                }
+                            }
+                        }
                         // near leaf candidate: a P2P source of these children
                         const uint32_t pbits = sleaf ? near_bits : 0u;
                         const uint32_t pb = __ballot_sync(0xFFFFFFFFu, pbits != 0);
                         if (pb) {
                             if (pfill + __popc(pb) > (uint32_t)kP2PCap) {
-                                phead = spill_p2p(sm, pfill, phead, A.p2p, status);
+                                if (XL && A.stream) {
+                                    stream_p2p<DEBUG, GRAD>(
+                                        sm,
+                                        LeafOut{A.xyzm, tv.info, A.p2p, A.fx, A.fy, A.fz,
+                                                A.leaf_of, tv.dbg_p2p, A.dense_rec, A.dense_cap,
+                                                A.kahan},
+                                        tgt_mask, fc, pfill, flushed, false, sinter);
+                                    flushed = true;
+                                } else {
+                                    phead = spill_p2p(sm, pfill, phead, A.p2p, status);
+                                }
                                 pfill = 0;
                             }
                             if (pbits) {
@@ -677,12 +879,14 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                         }
                         // near internal candidate: open it later for these children
                         const uint32_t qbits = sleaf ? 0u : near_bits;
-                        const uint32_t qb = __ballot_sync(0xFFFFFFFFu, qbits != 0);
+                        const bool push = qbits != 0 || cpush;
+                        const uint32_t qb = __ballot_sync(0xFFFFFFFFu, push);
                         if (qb) {
                             const uint32_t pos = ssize + __popc(qb & lt_mask);
-                            if (qbits && pos < (uint32_t)kStackCap) {
+                            if (push && pos < (uint32_t)kStackCap) {
                                 sm.stk_node[pos] = s;
-                                sm.stk_mask[pos] = (uint8_t)qbits;
+                                sm.stk_mask[pos] = (uint8_t)(cpush ? cmask : qbits);
+                                if constexpr (XL) sm.stk_lvl[pos] = (uint8_t)(cpush ? clvl : 0u);
                             }
                             ssize += __popc(qb);
                             if (ssize > (uint32_t)kStackCap) {
@@ -698,7 +902,14 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
 
             // ---- L2L: L(u) = M2L(u) + L(parent)  (polesitter.h:1248-1250) ----
             // closure order 1 shifts the parent's field to the child's centre:
-            // L(u) = M2L(u) + L(p) + G(p) (c_u - c_p), G(u) = M2L_G(u) + G(p)
+            // L(u) = M2L(u) + L(p) + G(p) (c_u - c_p), G(u) = M2L_G(u) + G(p).
+            // A chain group's parent field is L(a) + the chain's M2L.
+            float4 Lb = Lp;
+            if (XL && nchain) {
+                Lb.y = __fadd_rn(Lb.y, warp_sum(cacc0));
+                Lb.z = __fadd_rn(Lb.z, warp_sum(cacc1));
+                Lb.w = __fadd_rn(Lb.w, warp_sum(cacc2));
+            }
             float4 Gp0 = make_float4(0.f, 0.f, 0.f, 0.f), cp = Gp0;
             float2 Gp1 = make_float2(0.f, 0.f);
             if constexpr (GRAD) {
@@ -715,8 +926,8 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                 const float ax = warp_sum(acc[k][0]);
                 const float ay = warp_sum(acc[k][1]);
                 const float az = warp_sum(acc[k][2]);
-                float4 L = make_float4(0.f, __fadd_rn(ax, Lp.y), __fadd_rn(ay, Lp.z),
-                                       __fadd_rn(az, Lp.w));
+                float4 L = make_float4(0.f, __fadd_rn(ax, Lb.y), __fadd_rn(ay, Lb.z),
+                                       __fadd_rn(az, Lb.w));
                 float4 G0 = Gp0;
                 float2 G1 = Gp1;
                 if constexpr (GRAD) {
@@ -763,7 +974,7 @@ __global__ void __launch_bounds__(kTravThreads) k_trav(TravArgs A) {
                     sm,
                     LeafOut{A.xyzm, tv.info, A.p2p, A.fx, A.fy, A.fz, A.leaf_of, tv.dbg_p2p,
                             A.dense_rec, A.dense_cap, A.kahan},
-                    tgt_mask, fc, pfill, phead, status);
+                    tgt_mask, fc, pfill, phead, XL && A.stream != 0, flushed, sinter, status);
                 if (DEBUG && lane == 0) {
                     const unsigned long long cyc = (unsigned long long)(clock64() - t_group);
                     atomicMax(&status->stat[PSG_STAT_SLOWEST_GROUP],
@@ -1357,40 +1568,55 @@ void launch_dense_p2p(const TravArgs& A, int grid, cudaStream_t st) {
     }
 }
 
-template <int MODE, bool DENSE>
+template <int MODE, bool DENSE, bool XL>
 static void launch_mode(const TravArgs& A, int grid, cudaStream_t st) {
     if (A.order >= 1) {
-        if (A.debug) k_trav<MODE, true, true, DENSE><<<grid, kTravThreads, 0, st>>>(A);
-        else k_trav<MODE, false, true, DENSE><<<grid, kTravThreads, 0, st>>>(A);
+        if (A.debug) k_trav<MODE, true, true, DENSE, XL><<<grid, kTravThreads, 0, st>>>(A);
+        else k_trav<MODE, false, true, DENSE, XL><<<grid, kTravThreads, 0, st>>>(A);
     } else {
-        if (A.debug) k_trav<MODE, true, false, DENSE><<<grid, kTravThreads, 0, st>>>(A);
-        else k_trav<MODE, false, false, DENSE><<<grid, kTravThreads, 0, st>>>(A);
+        if (A.debug) k_trav<MODE, true, false, DENSE, XL><<<grid, kTravThreads, 0, st>>>(A);
+        else k_trav<MODE, false, false, DENSE, XL><<<grid, kTravThreads, 0, st>>>(A);
     }
 }
+
+static bool leaf_xl(const TravArgs& A) { return A.ns_levels < kMaxDepth || A.stream; }
 
 void launch_traverse_internal(const TravArgs& args, int level, int grid, cudaStream_t st) {
     TravArgs A = args;
     A.level = level;
-    launch_mode<MODE_INTERNAL, false>(A, grid, st);
+    launch_mode<MODE_INTERNAL, false, false>(A, grid, st);
 }
 
 void launch_traverse_leaves(const TravArgs& args, const int grid[2], cudaStream_t st) {
-    launch_mode<MODE_LEAF, false>(args, grid[0], st);
-    launch_mode<MODE_LEAF, true>(args, grid[1], st);
+    if (leaf_xl(args)) {
+        launch_mode<MODE_LEAF, false, true>(args, grid[0], st);
+        launch_mode<MODE_LEAF, true, true>(args, grid[1], st);
+    } else {
+        launch_mode<MODE_LEAF, false, false>(args, grid[0], st);
+        launch_mode<MODE_LEAF, true, false>(args, grid[1], st);
+    }
 }
 
 int traverse_threads() { return kTravThreads; }
-const void* traverse_kernel_ptr(int order, int dense) {
-    if (order) {
-        return dense ? (const void*)k_trav<MODE_LEAF, false, true, true>
-                     : (const void*)k_trav<MODE_LEAF, false, true, false>;
+const void* traverse_kernel_ptr(int order, int dense, int xl) {
+    if (xl) {
+        if (order) {
+            return dense ? (const void*)k_trav<MODE_LEAF, false, true, true, true>
+                         : (const void*)k_trav<MODE_LEAF, false, true, false, true>;
+        }
+        return dense ? (const void*)k_trav<MODE_LEAF, false, false, true, true>
+                     : (const void*)k_trav<MODE_LEAF, false, false, false, true>;
     }
-    return dense ? (const void*)k_trav<MODE_LEAF, false, false, true>
-                 : (const void*)k_trav<MODE_LEAF, false, false, false>;
+    if (order) {
+        return dense ? (const void*)k_trav<MODE_LEAF, false, true, true, false>
+                     : (const void*)k_trav<MODE_LEAF, false, true, false, false>;
+    }
+    return dense ? (const void*)k_trav<MODE_LEAF, false, false, true, false>
+                 : (const void*)k_trav<MODE_LEAF, false, false, false, false>;
 }
 const void* traverse_internal_kernel_ptr(int order) {
-    return order ? (const void*)k_trav<MODE_INTERNAL, false, true, false>
-                 : (const void*)k_trav<MODE_INTERNAL, false, false, false>;
+    return order ? (const void*)k_trav<MODE_INTERNAL, false, true, false, false>
+                 : (const void*)k_trav<MODE_INTERNAL, false, false, false, false>;
 }
 
 }  // namespace psg

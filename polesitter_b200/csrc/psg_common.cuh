@@ -76,7 +76,7 @@ struct Status {
     uint32_t dense_work;                   // ... and taken by k_dense_p2p
     uint32_t max_leaf;                     // particles in the fullest leaf
     uint32_t heavy_work;                   // groups taken by k_heavy_leaf
-    uint32_t pad_heavy;
+    uint32_t ns_fail;                      // bit k: level k's near lists did not fit
 };
 
 // P2P sources spilled from the traversal: chunk c holds cnt[c] source-leaf

@@ -29,6 +29,7 @@ extern "C" {
 #define PSG_ERR_P2P_OVERFLOW 0x10u /* P2P chunk store too small: regrow, rerun */
 #define PSG_ERR_DENSE_OVERFLOW 0x20u /* full-leaf record list too small: regrow, rerun */
 #define PSG_ERR_HEAVY_OVERFLOW 0x40u /* shallow-leaf records or frontier too small */
+#define PSG_ERR_CHAIN_ORDER 0x80u   /* an order-1 group without near lists (host bug) */
 
 /* debug statistics slots (Status.stat) */
 #define PSG_STAT_MAC 0
@@ -122,6 +123,10 @@ int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n
 #define PSG_OPT_JUDGE 8          /* 1: sampled FP64 judge in closure mode 1 too */
 #define PSG_OPT_HEAVY_DEPTH 9    /* leaves this shallow walk block-parallel (-1: from theta) */
 #define PSG_OPT_LEAF_CAP 10      /* split nodes holding more particles than this (1..256) */
+#define PSG_OPT_NEAR_LEVELS 11   /* store near lists for node depths <= this at most (2..10) */
+#define PSG_OPT_STREAM 12        /* 1: sum P2P in the leaf pass, never spill it */
+#define PSG_OPT_SHRINK_STORES 13 /* 1: shrink the growable traversal stores now */
+#define PSG_OPT_SORT_SPIN 14     /* > 0: sort look-back polls, first tile publishing late */
 #define PSG_MAX_LEAF_CAP 256
 
 /* the learned far-field closure (k_closure.cu) */

@@ -28,7 +28,7 @@ struct SortBuffers {
 };
 int sort_tile_size();
 void launch_sort(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* status,
-                 cudaStream_t st);
+                 cudaStream_t st, int spin_limit = 0);
 void launch_gather(const uint32_t* perm, const float* x, const float* y, const float* z,
                    const float* m, const uint32_t* id, size_t n, float4* xyzm, uint32_t* ids,
                    int grid, cudaStream_t st);
@@ -47,7 +47,7 @@ void launch_upward(TreeView tv, const Status* status, const float4* xyzm, int gr
 // (polesitter.h:1050-1146, :1224-1254, :1258-1494)
 struct TravArgs;
 int traverse_threads();
-const void* traverse_kernel_ptr(int order, int dense);
+const void* traverse_kernel_ptr(int order, int dense, int xl);
 const void* traverse_internal_kernel_ptr(int order);
 void launch_traverse_internal(const TravArgs& A, int level, int grid, cudaStream_t st);
 void launch_traverse_leaves(const TravArgs& A, const int grid[2], cudaStream_t st);
@@ -87,7 +87,8 @@ void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const 
 // the judge's FP64 direct sum on a sample (runs beside the tree build and
 // traversal on its own stream) and its decision (after the traversal)
 void launch_judge_direct(const float4* xyzm, size_t n, uint32_t* tg, int s, double* f64,
-                         uint32_t tick, int blocks, cudaStream_t st);
+                         uint32_t tick, int blocks, cudaStream_t st, double* part,
+                         size_t part_doubles);
 void launch_judge_decide(const uint32_t* tg, int s, const double* f64, const float* fx,
                          const float* fy, const float* fz, const float4* dF, int allow,
                          JudgeOut* out, cudaStream_t st);
@@ -104,8 +105,13 @@ void launch_mlp_adam(float* p, float* m, float* v, const float* g, int n, float 
                      float beta2, float eps, float bc1, float bc2, cudaStream_t st);
 
 // k_direct.cu -- FP64 direct-sum forces for sampled targets (tests/accuracy.c:42-72)
+// part: partial sums of the source splits (summed in split order, so the
+// result does not depend on scheduling); as many splits as part_doubles
+// holds, at most those that fill about `blocks` blocks
+size_t direct_f64_part_doubles(size_t n, size_t n_targets, int blocks);
 void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, size_t n_targets,
-                       double* out /*[n_targets][3]*/, int blocks, cudaStream_t st);
+                       double* out /*[n_targets][3]*/, int blocks, cudaStream_t st,
+                       double* part, size_t part_doubles);
 
 }  // namespace psg
 
@@ -133,5 +139,8 @@ struct TravArgs {
     int heavy_depth;    // leaf children of nodes above this depth go to k_heavy_leaf
     uint32_t* heavy_frontier;  // per block: 2 x heavy_fcap candidate slots
     uint32_t heavy_fcap;
+    int ns_levels;      // near lists exist for nodes of depth <= ns_levels; deeper
+                        // groups walk their ancestor chain (k_traverse.cu)
+    int stream;         // 1: P2P summed in the leaf pass as sources are found, no spill
 };
 }  // namespace psg

@@ -70,6 +70,8 @@ struct ClosureState {
     int have_weights;
     uint32_t* judge_tg;  // judge sample (sorted indices)
     double* judge_f64;   // FP64 direct forces of the sample
+    double* judge_part;  // ... their partial sums per source split
+    size_t judge_part_n;
     JudgeOut* d_judge;
     JudgeOut* h_judge;
     uint32_t tick;       // ticks run in closure mode (varies the judge sample)
@@ -83,7 +85,8 @@ struct State {
     uint32_t magic;
     int device;
     int sms;
-    int trav_grid[2][2];   // leaf-pass grid [closure order 0 / 1][sparse / dense variant]
+    int trav_grid[2][2][2];  // leaf-pass grid [closure order 0 / 1][sparse / dense variant]
+                             // [plain / chain + stream variant]
     int trav_int_grid[2];
     size_t max_particles;
     float theta;
@@ -107,6 +110,12 @@ struct State {
     cudaStream_t aux;      // k_heavy_leaf, beside the leaf pass
     cudaEvent_t ev_levels, ev_heavy;
     int heavy_depth;       // option; < 0: derived from theta
+    int ns_levels;         // near lists are stored for node depths <= this (kMaxDepth: all);
+                           // lowered when they do not fit, deeper groups walk their chains
+    int stream_p2p;        // P2P summed in the leaf pass as found (no spill store)
+    int force_ns_levels;   // option: store near lists for depths <= this at most
+    int force_stream;      // option: always stream the P2P
+    int sort_spin_limit;   // look-back polls before the sort gives up (option; 0: default)
     uint32_t leaf_cap;     // option: nodes holding more particles are split (1: the reference)
     double grid_scale;     // traversal grids x this (ensemble autotuner); 0: 1
     int kahan;
@@ -131,6 +140,13 @@ struct State {
     int attempts;   // traversal runs of the last tick (> 1: a capacity regrow)
 };
 
+// the near-list levels and the P2P mode start over when what they depend
+// on (theta, leaf capacity, expansion order, store sizes) changes
+static void reset_near_levels(State* s) {
+    s->ns_levels = kMaxDepth;
+    s->stream_p2p = 0;
+}
+
 static int grid_for(const State* s, size_t n, int per_block_items) {
     size_t want = (n + per_block_items - 1) / per_block_items;
     size_t cap = (size_t)s->sms * 8;
@@ -141,6 +157,7 @@ static int grid_for(const State* s, size_t n, int per_block_items) {
 static int alloc_ns(State* s, unsigned long long cap) {
     if (s->ns) cudaFree(s->ns);
     s->ns = nullptr;
+    s->ns_cap = 0;
     PSG_ALLOC(s->ns, cap * sizeof(uint32_t));
     s->ns_cap = cap;
     return PSG_OK;
@@ -152,6 +169,7 @@ static int alloc_p2p(State* s, uint32_t chunks) {
         if (p) cudaFree(p);
     s->p2p.src = s->p2p.next = s->p2p.cnt = nullptr;
     s->p2p.mask = nullptr;
+    s->p2p.cap_chunks = 0;
     PSG_ALLOC(s->p2p.src, (size_t)chunks * kP2PChunk * 4);
     PSG_ALLOC(s->p2p.mask, (size_t)chunks * kP2PChunk);
     PSG_ALLOC(s->p2p.next, (size_t)chunks * 4);
@@ -163,6 +181,7 @@ static int alloc_p2p(State* s, uint32_t chunks) {
 static int alloc_dense(State* s, uint32_t cap) {
     if (s->dense_rec) cudaFree(s->dense_rec);
     s->dense_rec = nullptr;
+    s->dense_cap = 0;
     PSG_ALLOC(s->dense_rec, (size_t)cap * sizeof(uint4));
     s->dense_cap = cap;
     return PSG_OK;
@@ -223,7 +242,7 @@ static void free_state(State* s) {
                   s->d_status, s->dense_rec, s->heavy_frontier, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
                   s->tk_vmir[0], s->tk_vmir[1], s->tk_vmir[2], s->cl.lg0, s->cl.lg1,
                   s->cl.leaf_of, s->cl.dF, s->cl.params, s->cl.packed, s->cl.judge_tg,
-                  s->cl.judge_f64, s->cl.d_judge};
+                  s->cl.judge_f64, s->cl.judge_part, s->cl.d_judge};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->h_status) cudaFreeHost(s->h_status);
@@ -308,6 +327,8 @@ static int init_state(State* s, size_t maxp, float theta) {
     r = alloc_heavy(s, (uint32_t)(n / 4 + 4096));
     if (r != PSG_OK) return r;
     s->heavy_depth = -1;
+    s->ns_levels = kMaxDepth;
+    s->force_ns_levels = kMaxDepth;
     s->leaf_cap = 1;
     PSG_CHECK(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
     PSG_CHECK(cudaEventCreateWithFlags(&s->ev_levels, cudaEventDisableTiming));
@@ -315,9 +336,11 @@ static int init_state(State* s, size_t maxp, float theta) {
     for (int o = 0; o < 2; ++o) {
         int bps = 0;
         for (int dn = 0; dn < 2; ++dn) {
-            PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &bps, traverse_kernel_ptr(o, dn), traverse_threads(), 0));
-            s->trav_grid[o][dn] = s->sms * (bps > 0 ? bps : 1);
+            for (int xl = 0; xl < 2; ++xl) {
+                PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &bps, traverse_kernel_ptr(o, dn, xl), traverse_threads(), 0));
+                s->trav_grid[o][dn][xl] = s->sms * (bps > 0 ? bps : 1);
+            }
         }
         PSG_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &bps, traverse_internal_kernel_ptr(o), traverse_threads(), 0));
@@ -340,6 +363,8 @@ static int closure_alloc(State* s) {
     PSG_ALLOC(c.packed, sizeof(MlpPacked));
     PSG_ALLOC(c.judge_tg, kJudgeSamples * 4);
     PSG_ALLOC(c.judge_f64, kJudgeSamples * 3 * sizeof(double));
+    c.judge_part_n = direct_f64_part_doubles(n, kJudgeSamples, s->sms * 2);
+    PSG_ALLOC(c.judge_part, c.judge_part_n * sizeof(double));
     PSG_ALLOC(c.d_judge, sizeof(JudgeOut));
     PSG_CHECK(cudaMallocHost((void**)&c.h_judge, sizeof(JudgeOut)));
     std::memset(c.h_judge, 0, sizeof(JudgeOut));
@@ -360,6 +385,16 @@ static int heavy_depth_for(const State* s) {
     return d < 2 ? 2 : d;
 }
 
+// Depth of the deepest nodes whose near lists this traversal stores.  The
+// shallow-leaf walk reads the lists of depths < heavy_depth, so they always
+// exist; the order-1 expansion needs every level's (its chain groups would
+// need each ancestor's own gradient).
+static int near_levels(const State* s) {
+    if (s->order >= 1) return kMaxDepth;
+    int k = std::min(s->ns_levels, s->force_ns_levels);
+    return std::max(k, std::max(2, heavy_depth_for(s) - 1));
+}
+
 static void record(State* s, int ph) {
     if (s->timing) cudaEventRecord(s->ev[ph], s->stream);
 }
@@ -373,6 +408,7 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     PSG_CHECK(cudaMemsetAsync(&s->d_status->p2p_chunks, 0, 4, s->stream));
     PSG_CHECK(cudaMemsetAsync(&s->d_status->dense_count, 0, 8, s->stream));
     PSG_CHECK(cudaMemsetAsync(&s->d_status->heavy_work, 0, 4, s->stream));
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->ns_fail, 0, 4, s->stream));
     TravArgs A;
     A.tv = s->tv;
     A.p2p = s->p2p;
@@ -397,12 +433,14 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     A.heavy_depth = heavy_depth_for(s);
     A.heavy_frontier = s->heavy_frontier;
     A.heavy_fcap = s->heavy_fcap;
+    A.ns_levels = near_levels(s);
+    A.stream = (s->stream_p2p || s->force_stream) ? 1 : 0;
     const double gs = s->grid_scale > 0.0 ? s->grid_scale : 1.0;
     auto scaled = [&](int g) {
         const int v = (int)(g * gs);
         return v < 1 ? 1 : v;
     };
-    for (int k = 2; k <= kMaxDepth; ++k)
+    for (int k = 2; k <= A.ns_levels; ++k)
         launch_traverse_internal(A, k, scaled(s->trav_int_grid[o]), s->stream);
     record(s, PH_TRAV);
     // shallow leaves on the aux stream, beside the leaf pass; the leaf
@@ -412,7 +450,8 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     launch_heavy_leaf(A, scaled(s->heavy_slots), s->aux);
     PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
     launch_leaf_start(s->d_status, A.heavy_depth, o, s->stream);
-    const int lg[2] = {scaled(s->trav_grid[o][0]), scaled(s->trav_grid[o][1])};
+    const int xl = (A.ns_levels < kMaxDepth || A.stream) ? 1 : 0;
+    const int lg[2] = {scaled(s->trav_grid[o][0][xl]), scaled(s->trav_grid[o][1][xl])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
     // full-leaf records: 12 blocks per SM, fewer for a small system (whose
@@ -426,15 +465,75 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     return PSG_OK;
 }
 
-// grows every store whose capacity bit is set in err (x2 of what the run
-// asked for), after a traversal run read back its status
+// bytes a growing store may take: what the device has free plus what the
+// store holds now (freed before the new one is allocated), less 1/16 of the
+// device for everything else
+static unsigned long long store_budget(unsigned long long held) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return held;
+    }
+    const unsigned long long avail = (unsigned long long)fr + held, margin = tot / 16;
+    return avail > margin ? avail - margin : 0ull;
+}
+
+// a store of another size, or the old one back when the device refuses
+static bool try_alloc_ns(State* s, unsigned long long cap) {
+    const unsigned long long old = s->ns_cap;
+    if (alloc_ns(s, cap) == PSG_OK) return true;
+    cudaGetLastError();
+    alloc_ns(s, old);
+    return false;
+}
+
+static bool try_alloc_p2p(State* s, uint32_t chunks) {
+    const uint32_t old = s->p2p.cap_chunks;
+    if (alloc_p2p(s, chunks) == PSG_OK) return true;
+    cudaGetLastError();
+    alloc_p2p(s, old);
+    return false;
+}
+
+// After a traversal run read back its status, makes room for every store
+// that ran out, for the rerun and later ticks:
+//  * near lists: grown to twice what the run reserved while the device has
+//    the memory and 32-bit offsets reach; past that (order 0), they stop at
+//    the level before the first that did not fit, the groups below walk
+//    their ancestor chains, and the P2P is streamed, so no store grows with
+//    theta any more;
+//  * P2P chunks: grown likewise, else the P2P is streamed;
+//  * full-leaf records and shallow-leaf frontiers: grown.
+// PSG_EOOM when nothing can give.
 static int regrow(State* s, uint32_t err) {
     if (err & PSG_ERR_NS_OVERFLOW) {
-        unsigned long long need = s->h_status->ns_used[0];
-        need = 2 * need + 1024;
-        if (need >= 0xFFFFFFF0ull) need = 0xFFFFFFF0ull;
-        int r = alloc_ns(s, need);
-        if (r != PSG_OK) return r;
+        const unsigned long long used = s->h_status->ns_used[0];
+        const uint32_t fail = s->h_status->ns_fail;
+        const int kf = fail ? __builtin_ctz(fail) : kMaxDepth;
+        const unsigned long long limit =
+            std::min(0xFFFFFFF0ull, store_budget(s->ns_cap * 4) / 4);
+        const unsigned long long want = 2 * used + (1ull << 20);
+        const int floor_k = std::max(2, heavy_depth_for(s) - 1);
+        bool done = false;
+        if (want <= limit) {
+            done = try_alloc_ns(s, want);
+        } else if (s->ns_cap < limit && used + (1ull << 20) <= limit) {
+            // what the run reserved fits, twice that does not: the largest
+            // store, and the levels below show whether it is enough
+            done = try_alloc_ns(s, limit);
+        }
+        if (!done && s->order == 0 && kf - 1 >= floor_k) {
+            s->ns_levels = kf - 1;
+            s->stream_p2p = 1;
+            done = true;
+        }
+        if (!done && s->order >= 1 && limit > s->ns_cap) done = try_alloc_ns(s, limit);
+        if (!done) {
+            std::snprintf(g_err, sizeof(g_err),
+                          "near lists need %llu entries at level %d; the device holds %llu",
+                          want, kf, limit);
+            return PSG_EOOM;
+        }
     }
     if (err & PSG_ERR_HEAVY_OVERFLOW) {
         unsigned long long cap = 2ull * s->heavy_fcap;
@@ -450,11 +549,13 @@ static int regrow(State* s, uint32_t err) {
         if (r != PSG_OK) return r;
     }
     if (err & PSG_ERR_P2P_OVERFLOW) {
-        unsigned long long need = s->h_status->p2p_chunks;
-        need = 2 * need + 1024;
-        if (need > 0x7FFFFFFFull) need = 0x7FFFFFFFull;
-        int r = alloc_p2p(s, (uint32_t)need);
-        if (r != PSG_OK) return r;
+        // the chunk counter is 32-bit: below the capacity it has wrapped
+        const unsigned long long used = s->h_status->p2p_chunks;
+        const unsigned long long need = used < s->p2p.cap_chunks ? ~0ull : 2 * used + 1024;
+        const unsigned long long per = kP2PChunk * 5 + 8;
+        const unsigned long long limit =
+            std::min(0x7FFFFFFFull, store_budget(s->p2p.cap_chunks * per) / per);
+        if (!(need <= limit && try_alloc_p2p(s, (uint32_t)need))) s->stream_p2p = 1;
     }
     return PSG_OK;
 }
@@ -483,7 +584,7 @@ static int run_traversal(State* s, const float4* xyzm, float* fx, float* fy, flo
         PSG_CHECK(cudaMemsetAsync(&s->d_status->stat[0], 0, sizeof(s->d_status->stat), s->stream));
         if (s->timing) cudaEventRecord(s->ev[PH_UP], s->stream);
     }
-    note("traversal capacity regrow", cudaErrorMemoryAllocation);
+    std::snprintf(g_err, sizeof(g_err), "traversal stores still too small after 6 runs");
     return PSG_EOOM;
 }
 
@@ -549,7 +650,7 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     record(s, PH_BEGIN);
     PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
     const int g = grid_for(s, n, 1024);
-    launch_sort(s->sort, d.codes, n, g, s->d_status, st);
+    launch_sort(s->sort, d.codes, n, g, s->d_status, st, s->sort_spin_limit);
     record(s, PH_SORT);
     launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
     launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
@@ -564,7 +665,7 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
         PSG_CHECK(cudaEventRecord(cj.ev_sorted, st));
         PSG_CHECK(cudaStreamWaitEvent(cj.side, cj.ev_sorted, 0));
         launch_judge_direct(s->xyzm, n, cj.judge_tg, smp, cj.judge_f64, cj.tick, s->sms * 2,
-                            cj.side);
+                            cj.side, cj.judge_part, cj.judge_part_n);
         PSG_CHECK(cudaEventRecord(cj.ev_judge, cj.side));
     }
     const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
@@ -600,10 +701,12 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
             return r;
         }
     }
-    if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_HEAVY_OVERFLOW)) {
+    if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_HEAVY_OVERFLOW |
+               PSG_ERR_CHAIN_ORDER)) {
         if (judge) cudaStreamSynchronize(cj.side);
         const bool nodes = (err & PSG_ERR_NODES) &&
-                           !(err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_HEAVY_OVERFLOW));
+                           !(err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_HEAVY_OVERFLOW |
+                                    PSG_ERR_CHAIN_ORDER));
         std::snprintf(g_err, sizeof(g_err), nodes ? "morton codes not sorted/30-bit (0x%x)"
                                                   : "device status error 0x%x", err);
         return nodes ? PSG_EINVAL : PSG_EDEVICE;
@@ -651,6 +754,8 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     s->stats[11] = (unsigned long long)s->attempts;
     s->stats[12] = s->h_status->max_leaf;
     s->stats[13] = s->h_status->dense_count;
+    s->stats[14] = (unsigned long long)near_levels(s);
+    s->stats[15] = (s->stream_p2p || s->force_stream) ? 1ull : 0ull;
     if (s->timing) {
         cudaEventSynchronize(s->ev[PH_CLOSURE]);
         const int order[7] = {PH_BEGIN, PH_SORT, PH_GATHER, PH_TREE, PH_UP, PH_TRAV, PH_DENSE};
@@ -982,7 +1087,7 @@ static int check_systems(Ensemble* e, const DevArrays& a) {
     for (size_t k = 0; k < e->nsys; ++k) {
         State* s = e->sys[k];
         const uint32_t err = s->h_status->err;
-        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES)) {
+        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_CHAIN_ORDER)) {
             std::snprintf(g_err, sizeof(g_err), "ensemble system %zu: device status 0x%x", k, err);
             return (err & PSG_ERR_NODES) ? PSG_EINVAL : PSG_EDEVICE;
         }
@@ -1133,6 +1238,12 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
     const size_t kSample = 1024;
     PSG_ALLOC(d_tg, kSample * 4);
     PSG_ALLOC(d_f64, kSample * 3 * sizeof(double));
+    size_t maxn = 1;
+    for (size_t k = 0; k < e->nsys; ++k) maxn = std::max(maxn, e->count[k]);
+    const int dsms = e->sys[0]->sms * 8;
+    const size_t part_n = direct_f64_part_doubles(maxn, kSample, dsms);
+    double* d_part = nullptr;
+    PSG_ALLOC(d_part, part_n * sizeof(double));
     std::vector<uint32_t> tg(kSample);
     std::vector<double> f64(kSample * 3);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1161,7 +1272,7 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
         const size_t ns = n < kSample ? n : kSample;
         for (size_t i = 0; i < ns; ++i) tg[i] = (uint32_t)(i * n / ns);
         PSG_CHECK(cudaMemcpyAsync(d_tg, tg.data(), ns * 4, cudaMemcpyHostToDevice, s->stream));
-        launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, s->sms * 8, s->stream);
+        launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, dsms, s->stream, d_part, part_n);
         PSG_CHECK(cudaMemcpyAsync(f64.data(), d_f64, ns * 3 * sizeof(double),
                                   cudaMemcpyDeviceToHost, s->stream));
         std::vector<float> hf[3] = {std::vector<float>(n), std::vector<float>(n),
@@ -1262,6 +1373,7 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
     cudaEventDestroy(e1);
     cudaFree(d_tg);
     cudaFree(d_f64);
+    cudaFree(d_part);
     if (r == PSG_OK) {
         for (size_t k = 0; k < e->nsys; ++k) {
             e->sys[k]->theta = chosen[k];
@@ -1355,7 +1467,10 @@ int psg_set_option(void* mem, int key, double value) {
     if (!s || s->magic != psg::kMagic) return PSG_EINVAL;
     switch (key) {
         case PSG_OPT_DEBUG: s->debug = value != 0.0; return PSG_OK;
-        case PSG_OPT_THETA: s->theta = value > 0.0 ? (float)value : 1.0f; return PSG_OK;
+        case PSG_OPT_THETA:
+            s->theta = value > 0.0 ? (float)value : 1.0f;
+            psg::reset_near_levels(s);
+            return PSG_OK;
         case PSG_OPT_MORTON_VARIANT:
             if (value < 0 || value > 2) return PSG_EINVAL;
             s->morton_variant = (int)value;
@@ -1372,6 +1487,7 @@ int psg_set_option(void* mem, int key, double value) {
             }
             s->cl.mode = mode;
             s->order = mode >= 1 ? 1 : 0;
+            psg::reset_near_levels(s);
             return PSG_OK;
         }
         case PSG_OPT_JUDGE: s->cl.judge = value != 0.0; return PSG_OK;
@@ -1383,6 +1499,27 @@ int psg_set_option(void* mem, int key, double value) {
             if (value < 1 || value > PSG_MAX_LEAF_CAP || (double)(int)value != value)
                 return PSG_EINVAL;
             s->leaf_cap = (uint32_t)value;
+            psg::reset_near_levels(s);
+            return PSG_OK;
+        case PSG_OPT_NEAR_LEVELS:
+            if (value < 2 || value > psg::kMaxDepth || (double)(int)value != value)
+                return PSG_EINVAL;
+            s->force_ns_levels = (int)value;
+            return PSG_OK;
+        case PSG_OPT_STREAM: s->force_stream = value != 0.0; return PSG_OK;
+        case PSG_OPT_SHRINK_STORES: {
+            if (value != 1.0) return PSG_EINVAL;
+            PSG_CHECK(cudaSetDevice(s->device));
+            PSG_CHECK(cudaStreamSynchronize(s->stream));
+            int r = psg::alloc_ns(s, 1024);
+            if (r == PSG_OK) r = psg::alloc_p2p(s, 64);
+            if (r == PSG_OK) r = psg::alloc_dense(s, 64);
+            psg::reset_near_levels(s);
+            return r;
+        }
+        case PSG_OPT_SORT_SPIN:
+            if (value < 0 || value > (1 << 22) || (double)(int)value != value) return PSG_EINVAL;
+            s->sort_spin_limit = (int)value;
             return PSG_OK;
         default: return PSG_EINVAL;
     }
@@ -1484,10 +1621,14 @@ int psg_direct_f64(void* mem, const psg_arrays_t* a, const uint32_t* targets, si
         PSG_CHECK(cudaMemcpyAsync(dt, targets, n_t * 4, cudaMemcpyHostToDevice, st));
     }
     if (ho) PSG_ALLOC(dout, n_t * 3 * sizeof(double));
-    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, s->sms * 8, st);
+    const size_t part_n = psg::direct_f64_part_doubles(n, n_t, s->sms * 8);
+    double* part = nullptr;
+    PSG_ALLOC(part, part_n * sizeof(double));
+    psg::launch_direct_f64(s->xyzm, n, dt, n_t, dout, s->sms * 8, st, part, part_n);
     PSG_CHECK(cudaGetLastError());
     if (ho) PSG_CHECK(cudaMemcpyAsync(out, dout, n_t * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     PSG_CHECK(cudaStreamSynchronize(st));
+    cudaFree(part);
     if (ht) cudaFree(dt);
     if (ho) cudaFree(dout);
     return PSG_OK;
