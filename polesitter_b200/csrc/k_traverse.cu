@@ -987,59 +987,39 @@ __global__ void __launch_bounds__(kTravThreads,
 
 // L2P + P2P of the full leaves recorded by the leaf pass.  A warp takes one
 // record (a run of leaves, up to 32 of their particles, the group's source
-// chain) at a time from a shared counter; T lanes own the record's target
-// particles (T the smallest power of two >= their count) and the 32 / T
-// slices of lanes split the sources, so a record with few targets still
-// keeps the warp busy; the slices' sums are added at the end.
-//
-// Sources go through the warp in tiles of 32 particles: a chunk's entries
-// (source leaves that serve at least one leaf of the record) are laid end to
-// end by a prefix sum of their particle counts, lane j finds the entry of
-// particle b + j by a binary search over those sums, loads it (coalesced
-// within a leaf) with the entry's child mask into the warp's shared tile,
-// and every lane then runs its target against the tile's particles from
-// shared memory.  When every entry of a chunk serves every leaf of the run,
-// the per-pair mask test is dropped.  A record with at most 4 targets (8 or
-// more slices) skips the staging: each slice walks whole source leaves from
-// global memory, as the tile's binary search would cost more than its reuse
-// saves.  Sources are summed in chain order, so the result does not depend
-// on scheduling.
-struct DenseTile {
-    float4 p[32];
-    uint32_t m[32];
-};
+// chain) at a time from a shared counter.  The chain's entries (source
+// leaves) are split by the leaves of the record they serve:
+//  * an entry that serves every leaf of the record is summed by all lanes:
+//    T lanes own the record's target particles (T the smallest power of two
+//    >= their count) and the 32 / T slices of lanes split the entry's
+//    particles;
+//  * an entry that serves only some of its leaves is summed per leaf q, in
+//    another walk of the chain, with the lanes dealt over q's targets alone
+//    (T_q lanes, 32 / T_q slices),
+// so no lane computes a pair its target does not want.  Sources are read
+// straight from the sorted particles: a slice's lanes read the same
+// address, the slices read adjacent ones, two particles per step into two
+// accumulator chains.  The per-leaf sums reach the target's lane through
+// shared memory (a target belongs to one leaf, so its slot is written once).
+// Sums are taken in chain order, so the result does not depend on
+// scheduling.
 
-// one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
-// a source counts only if its child mask holds the target's leaf q.  Plain
-// sums alternate between two accumulator sets (independent FMA chains),
-// added at the end of the tile.
-template <bool MASKED, bool KAHAN>
-__device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, uint32_t S,
-                                           uint32_t nt, uint32_t q, float4 t, float& ax,
-                                           float& ay, float& az, float& cx, float& cy, float& cz,
-                                           uint32_t& used) {
+// target t against the particles first + slice, first + slice + S, ... <
+// first + cnt (polesitter.h:1424-1444, rsqrt), optionally Kahan-compensated
+template <bool KAHAN>
+__device__ __forceinline__ void walk_leaf(const float4* __restrict__ xyzm, uint32_t first,
+                                          uint32_t cnt, uint32_t slice, uint32_t S, float4 t,
+                                          float& ax, float& ay, float& az, float& cx,
+                                          float& cy, float& cz) {
     if constexpr (KAHAN) {
-        for (uint32_t j = j0; j < nt; j += S) {
-            const float4 p = tile.p[j];
-            float w = p.w;
-            if (MASKED) {
-                const bool on = (tile.m[j] >> q) & 1u;
-                w = on ? w : 0.f;
-                used += on ? 1u : 0u;
-            } else {
-                ++used;
-            }
-            float fx, fy, fz;
+        for (uint32_t j = slice; j < cnt; j += S) {
+            const float4 p = xyzm[first + j];
             const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
-            const float inv = rsqrtf(r2);
-            const float f = w * (inv * inv * inv);
-            fx = __fmul_rn(dx, f);
-            fy = __fmul_rn(dy, f);
-            fz = __fmul_rn(dz, f);
-            const float yx = __fsub_rn(fx, cx);
-            const float yy = __fsub_rn(fy, cy);
-            const float yz = __fsub_rn(fz, cz);
+            const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 0.1f))));
+            const float f = p.w * (inv * inv * inv);
+            const float yx = __fsub_rn(__fmul_rn(dx, f), cx);
+            const float yy = __fsub_rn(__fmul_rn(dy, f), cy);
+            const float yz = __fsub_rn(__fmul_rn(dz, f), cz);
             const float tx = __fadd_rn(ax, yx);
             const float ty = __fadd_rn(ay, yy);
             const float tz = __fadd_rn(az, yz);
@@ -1052,24 +1032,14 @@ __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, u
         }
     } else {
         float ex = 0.f, ey = 0.f, ez = 0.f;
-        uint32_t j = j0;
-#pragma unroll 2
-        for (; j + S < nt; j += 2 * S) {
-            const float4 p0 = tile.p[j], p1 = tile.p[j + S];
-            float w0 = p0.w, w1 = p1.w;
-            if (MASKED) {
-                const bool on0 = (tile.m[j] >> q) & 1u, on1 = (tile.m[j + S] >> q) & 1u;
-                w0 = on0 ? w0 : 0.f;
-                w1 = on1 ? w1 : 0.f;
-                used += (on0 ? 1u : 0u) + (on1 ? 1u : 0u);
-            } else {
-                used += 2;
-            }
+        uint32_t j = slice;
+        for (; j + S < cnt; j += 2 * S) {
+            const float4 p0 = xyzm[first + j], p1 = xyzm[first + j + S];
             const float dx0 = p0.x - t.x, dy0 = p0.y - t.y, dz0 = p0.z - t.z;
             const float dx1 = p1.x - t.x, dy1 = p1.y - t.y, dz1 = p1.z - t.z;
             const float i0 = rsqrtf(fmaf(dx0, dx0, fmaf(dy0, dy0, fmaf(dz0, dz0, 0.1f))));
             const float i1 = rsqrtf(fmaf(dx1, dx1, fmaf(dy1, dy1, fmaf(dz1, dz1, 0.1f))));
-            const float f0 = w0 * (i0 * i0 * i0), f1 = w1 * (i1 * i1 * i1);
+            const float f0 = p0.w * (i0 * i0 * i0), f1 = p1.w * (i1 * i1 * i1);
             ax = fmaf(dx0, f0, ax);
             ay = fmaf(dy0, f0, ay);
             az = fmaf(dz0, f0, az);
@@ -1077,19 +1047,11 @@ __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, u
             ey = fmaf(dy1, f1, ey);
             ez = fmaf(dz1, f1, ez);
         }
-        if (j < nt) {
-            const float4 p = tile.p[j];
-            float w = p.w;
-            if (MASKED) {
-                const bool on = (tile.m[j] >> q) & 1u;
-                w = on ? w : 0.f;
-                used += on ? 1u : 0u;
-            } else {
-                ++used;
-            }
+        if (j < cnt) {
+            const float4 p = xyzm[first + j];
             const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
             const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 0.1f))));
-            const float f = w * (inv * inv * inv);
+            const float f = p.w * (inv * inv * inv);
             ax = fmaf(dx, f, ax);
             ay = fmaf(dy, f, ay);
             az = fmaf(dz, f, az);
@@ -1102,11 +1064,12 @@ __device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, u
 
 template <bool DEBUG, bool GRAD, bool KAHAN>
 __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
-    __shared__ DenseTile tiles[kTravWarps];
-    DenseTile& tile = tiles[threadIdx.x >> 5];
+    __shared__ float4 s_part[kTravWarps][32];  // per-leaf sums of the record's targets
+    float4* part = s_part[threadIdx.x >> 5];
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_DENSE_OVERFLOW)) return;
     const TreeView& tv = A.tv;
+    const float4* __restrict__ xyzm = A.xyzm;
     const uint32_t lane = lane_id();
     const uint32_t total = min(status->dense_count, A.dense_cap);
     if (total == 0) return;
@@ -1117,13 +1080,13 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         r = __shfl_sync(0xFFFFFFFFu, r, 0);
         if (r >= total) break;
         const uint4 rec = A.dense_rec[r];
-        const uint32_t fc = rec.x, run = rec.w >> 8, cnt_t = rec.w & 0xFFu;
+        const uint32_t fc = rec.x, run = rec.w >> 8, cnt_t = rec.w & 0xFFu, first = rec.z;
         uint32_t T = 1;
         while (T < cnt_t) T <<= 1;
         const uint32_t S = 32u / T;
         const uint32_t tl = lane & (T - 1u), slice = lane / T;
         const bool active = tl < cnt_t;
-        const uint32_t i = rec.z + (active ? tl : 0u);
+        const uint32_t i = first + (active ? tl : 0u);
         // this lane's leaf: the child of the run whose particles hold i
         uint32_t q = __ffs(run) - 1;
         for (uint32_t m = run; m; m &= m - 1) {
@@ -1131,61 +1094,79 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
             if (tv.info[fc + qq].x <= i) q = qq;
         }
         const uint32_t u = fc + q;
-        const float4 t = A.xyzm[i];
+        const float4 t = xyzm[i];
+        part[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-        uint32_t used = 0;
+        uint32_t used = 0, partial_q = 0;
+        // pass 1: the entries that serve every leaf of the record
         for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
             const uint32_t cnt = A.p2p.cnt[c];
-            if (S >= 8u) {
-                // few targets: each slice walks whole source leaves of the
-                // chunk from global memory (no staging)
-                for (uint32_t k = slice; k < cnt; k += S) {
-                    if (!((A.p2p.mask[(size_t)c * kP2PChunk + k] >> q) & 1u)) continue;
-                    const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + k]];
-                    p2p_range(A.xyzm, make_uint2(si.x, si.y), t, KAHAN, bx, by, bz, cx, cy, cz);
-                    used += si.y;
-                }
-                continue;
-            }
-            uint32_t es = 0, en = 0, em = 0;
+            uint32_t em = 0, es = 0, en = 0;
             if (lane < cnt) {
                 em = A.p2p.mask[(size_t)c * kP2PChunk + lane] & run;
-                if (em) {
+                if (em == run) {
                     const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
                     es = si.x;
                     en = si.y;
                 }
             }
-            const uint32_t incl = warp_incl_scan(en);
-            const uint32_t ptot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-            const bool masked = __ballot_sync(0xFFFFFFFFu, en && em != run) != 0u;
-            for (uint32_t b = 0; b < ptot; b += 32) {
-                // lane j: flat source particle b + j -> entry e (incl[e-1] <= f < incl[e])
-                const uint32_t f = b + lane;
-                uint32_t e = 0;
-#pragma unroll
-                for (uint32_t step = 16; step > 0; step >>= 1) {
-                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, e + step - 1);
-                    if (v <= f) e += step;
-                }
-                const uint32_t e_start = __shfl_sync(0xFFFFFFFFu, es, e);
-                const uint32_t e_excl = __shfl_sync(0xFFFFFFFFu, incl - en, e);
-                const uint32_t e_mask = __shfl_sync(0xFFFFFFFFu, em, e);
-                __syncwarp();
-                if (f < ptot) {
-                    tile.p[lane] = A.xyzm[e_start + (f - e_excl)];
-                    tile.m[lane] = e_mask;
-                }
-                __syncwarp();
-                const uint32_t nt = min(32u, ptot - b);
-                if (masked)
-                    dense_tile<true, KAHAN>(tile, slice, S, nt, q, t, bx, by, bz, cx, cy, cz, used);
-                else
-                    dense_tile<false, KAHAN>(tile, slice, S, nt, q, t, bx, by, bz, cx, cy, cz,
-                                             used);
+            partial_q |= __reduce_or_sync(0xFFFFFFFFu, em != run ? em : 0u);
+            for (uint32_t full = __ballot_sync(0xFFFFFFFFu, em == run); full; full &= full - 1) {
+                const uint32_t e = __ffs(full) - 1;
+                const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
+                const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
+                walk_leaf<KAHAN>(xyzm, s0, n0, slice, S, t, bx, by, bz, cx, cy, cz);
+                if (DEBUG) used += n0;
             }
         }
-        if (DEBUG) inter += active ? used : 0u;
+        // pass 2: per leaf of the record, the entries that serve it but not
+        // every leaf of the record
+        for (uint32_t m = partial_q; m; m &= m - 1) {
+            const uint32_t qq = __ffs(m) - 1;
+            const uint4 ci = tv.info[fc + qq];
+            const uint32_t lo = max(ci.x, first), hi = min(ci.x + ci.y, first + cnt_t);
+            if (hi <= lo) continue;
+            const uint32_t nq = hi - lo;
+            uint32_t Tq = 1;
+            while (Tq < nq) Tq <<= 1;
+            const uint32_t Sq = 32u / Tq, tq = lane & (Tq - 1u), sq = lane / Tq;
+            const bool actq = tq < nq;
+            const uint32_t iq = lo + (actq ? tq : 0u);
+            const float4 tp = xyzm[iq];
+            float px = 0.f, py = 0.f, pz = 0.f, kx = 0.f, ky = 0.f, kz = 0.f;
+            uint32_t usedq = 0;
+            for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
+                const uint32_t cnt = A.p2p.cnt[c];
+                uint32_t em = 0, es = 0, en = 0;
+                if (lane < cnt) em = A.p2p.mask[(size_t)c * kP2PChunk + lane] & run;
+                const bool mine = em != run && ((em >> qq) & 1u);
+                if (mine) {
+                    const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
+                    es = si.x;
+                    en = si.y;
+                }
+                for (uint32_t pm = __ballot_sync(0xFFFFFFFFu, mine); pm; pm &= pm - 1) {
+                    const uint32_t e = __ffs(pm) - 1;
+                    const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
+                    const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
+                    walk_leaf<KAHAN>(xyzm, s0, n0, sq, Sq, tp, px, py, pz, kx, ky, kz);
+                    if (DEBUG) usedq += n0;
+                }
+            }
+            px -= kx;
+            py -= ky;
+            pz -= kz;
+            for (uint32_t o = Tq; o < 32u; o <<= 1) {
+                px += __shfl_xor_sync(0xFFFFFFFFu, px, o);
+                py += __shfl_xor_sync(0xFFFFFFFFu, py, o);
+                pz += __shfl_xor_sync(0xFFFFFFFFu, pz, o);
+            }
+            if (actq && sq == 0) part[iq - first] = make_float4(px, py, pz, 0.f);
+            if (DEBUG) inter += (actq && sq == 0) ? usedq : 0u;
+        }
+        __syncwarp();
+        if (DEBUG) inter += (active && slice == 0) ? used : 0u;
         // sum the slices' partial sums (fixed order)
         bx -= cx;
         by -= cy;
@@ -1196,6 +1177,10 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
             bz += __shfl_xor_sync(0xFFFFFFFFu, bz, o);
         }
         if (active && slice == 0) {
+            const float4 pp = part[tl];
+            bx += pp.x;
+            by += pp.y;
+            bz += pp.z;
             const float4 L = tv.lt[u];
             float lx = L.y, ly = L.z, lz = L.w;
             if constexpr (GRAD) {
@@ -1212,6 +1197,7 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
             A.fy[i] = (float)(mm * ((double)ly + (double)by));
             A.fz[i] = (float)(mm * ((double)lz + (double)bz));
         }
+        __syncwarp();
     }
     if (DEBUG) {
         inter = warp_sum(inter);
