@@ -70,10 +70,12 @@ __global__ void __launch_bounds__(256) k_sort_scan(const uint32_t* __restrict__ 
     }
 }
 
+// One stable pass on the 8-bit digit (key >> shift) & 0xFF; offs: the
+// pass's 256 global digit starts.
 __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int pass,
-    const uint32_t* __restrict__ offs /*[4][256]*/, uint32_t* lookback /*[tiles][256]*/,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int shift,
+    const uint32_t* __restrict__ offs /*[256]*/, uint32_t* lookback /*[tiles][256]*/,
     uint32_t* ticket, Status* status, int spin_limit, int late) {
     __shared__ uint32_t s_wcnt[kSortWarps][256];
     __shared__ uint32_t s_keys[kSortTile];
@@ -84,7 +86,6 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
     __shared__ uint32_t s_tile;
 
     const int t = threadIdx.x, w = t >> 5, l = t & 31;
-    const int shift = pass * 8;
     if (t == 0) s_tile = atomicAdd(ticket, 1u);
     for (int i = t; i < kSortWarps * 256; i += kSortThreads) (&s_wcnt[0][0])[i] = 0;
     __syncthreads();
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(
         }
         atomicExch(my, kFlagInc | (prefix + total));
     }
-    s_glob[t] = offs[pass * 256 + t] + prefix;
+    s_glob[t] = offs[t] + prefix;
     // tile-local digit starts: exclusive scan of totals over digits
     uint32_t inc = warp_incl_scan(total);
     if (l == 31) s_wsum[w] = inc;
@@ -243,7 +244,8 @@ void launch_sort(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* st
     uint32_t* kouts[4] = {b.key_b, b.key_a, b.key_b, codes};
     uint32_t* vouts[4] = {b.val_b, b.val_a, b.val_b, b.val_a};
     for (int p = 0; p < 4; ++p) {
-        k_sort_pass<<<tiles, kSortThreads, 0, st>>>(kin, vin, kouts[p], vouts[p], n, p, b.offs,
+        k_sort_pass<<<tiles, kSortThreads, 0, st>>>(kin, vin, kouts[p], vouts[p], n, 8 * p,
+                                                   b.offs + 256 * p,
                                                    b.lookback + (size_t)p * tiles * 256,
                                                    status->sort_tiles + p, status, limit,
                                                    spin_limit > 0 && p == 0 ? 1 : 0);
@@ -251,6 +253,80 @@ void launch_sort(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* st
         vin = vouts[p];
     }
     b.perm = b.val_a;
+}
+
+// the system of the particle at each position after the code passes
+__global__ void __launch_bounds__(256) k_sort_sys_keys(const uint32_t* __restrict__ perm,
+                                                       const uint32_t* __restrict__ part_sys,
+                                                       size_t n, uint32_t* __restrict__ out) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t j = perm[i];
+        out[i] = j < n ? part_sys[j] : 0u;  // j >= n only after a sort error (raised)
+    }
+}
+
+// codes in the final order, from the unsorted codes
+__global__ void __launch_bounds__(256) k_sort_gather_codes(const uint32_t* __restrict__ perm,
+                                                           const uint32_t* __restrict__ codes,
+                                                           size_t n, uint32_t* __restrict__ out) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t j = perm[i];
+        out[i] = j < n ? codes[j] : 0u;
+    }
+}
+
+// Many systems in one array, system k at [sys_off[k], sys_off[k+1]): every
+// system's codes sorted stably within its own range, in one set of passes.
+// The four code passes sort all particles by code; then stable passes on the
+// system index (its low byte, then its high byte when there are more than
+// 256 systems) put each system back in its range with its code order and
+// ties kept -- the order each system's own sort gives.  The digit starts of
+// the system passes come from the system sizes (sys_offs, host-computed,
+// [passes][256]).
+void launch_sort_forest(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* status,
+                        cudaStream_t st, const uint32_t* part_sys, int sys_passes,
+                        const uint32_t* sys_offs) {
+    const int tiles = (int)((n + kSortTile - 1) / kSortTile);
+    const int passes = 4 + sys_passes;
+    cudaMemsetAsync(b.hist, 0, 4 * 256 * sizeof(uint32_t), st);
+    cudaMemsetAsync(b.lookback, 0, (size_t)passes * tiles * 256 * sizeof(uint32_t), st);
+    cudaMemsetAsync(status->sort_tiles, 0, sizeof(status->sort_tiles), st);
+    k_sort_hist<<<grid, 256, 0, st>>>(codes, n, b.hist);
+    k_sort_scan<<<1, 256, 0, st>>>(b.hist, b.offs);
+    // code passes: codes -> b -> a -> b -> a (the input codes stay as they are)
+    const uint32_t* kin = codes;
+    const uint32_t* vin = nullptr;
+    uint32_t* kouts[4] = {b.key_b, b.key_a, b.key_b, b.key_a};
+    uint32_t* vouts[4] = {b.val_b, b.val_a, b.val_b, b.val_a};
+    for (int p = 0; p < 4; ++p) {
+        k_sort_pass<<<tiles, kSortThreads, 0, st>>>(kin, vin, kouts[p], vouts[p], n, 8 * p,
+                                                   b.offs + 256 * p,
+                                                   b.lookback + (size_t)p * tiles * 256,
+                                                   status->sort_tiles + p, status, kSpinLimit,
+                                                   0);
+        kin = kouts[p];
+        vin = vouts[p];
+    }
+    // system passes on (system index, permutation)
+    k_sort_sys_keys<<<grid, 256, 0, st>>>(b.val_a, part_sys, n, b.key_b);
+    uint32_t* sk[2] = {b.key_b, b.key_a};
+    uint32_t* sv[2] = {b.val_a, b.val_b};
+    for (int q = 0; q < sys_passes; ++q) {
+        const int p = 4 + q;
+        k_sort_pass<<<tiles, kSortThreads, 0, st>>>(sk[q & 1], sv[q & 1], sk[(q + 1) & 1],
+                                                   sv[(q + 1) & 1], n, 8 * q,
+                                                   sys_offs + 256 * q,
+                                                   b.lookback + (size_t)p * tiles * 256,
+                                                   status->sort_tiles + p, status, kSpinLimit,
+                                                   0);
+    }
+    b.perm = sv[sys_passes & 1];
+    // the codes in that order (key_b is free again: the system keys it held
+    // were consumed, or it received the discarded keys of the last pass)
+    k_sort_gather_codes<<<grid, 256, 0, st>>>(b.perm, codes, n, b.key_b);
+    cudaMemcpyAsync(codes, b.key_b, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
 }
 
 void launch_gather(const uint32_t* perm, const float* x, const float* y, const float* z,

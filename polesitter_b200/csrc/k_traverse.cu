@@ -484,7 +484,10 @@ __global__ void __launch_bounds__(kTravThreads,
     const TreeView& tv = A.tv;
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
-    if (MODE == MODE_LEAF && ((status->max_leaf >= kDenseSwitch) != DENSE)) return;
+    // the variant for this tree (batched systems: each group takes its
+    // system's variant, so a system sums exactly as it does alone)
+    if (MODE == MODE_LEAF && !tv.part_sys && ((status->max_leaf >= kDenseSwitch) != DENSE))
+        return;
     // a shallower level's near lists did not fit: this level's are void
     if (MODE == MODE_INTERNAL && (status->ns_fail & ((1u << A.level) - 1u))) return;
     const float theta2 = __fmul_rn(A.theta, A.theta);
@@ -552,6 +555,17 @@ __global__ void __launch_bounds__(kTravThreads,
             const uint32_t nc = plink >> 28;
             if (nc == 0) continue;
             const uint32_t fc = plink & kLinkMask;
+            // batched systems: the group's own system, theta and root; its
+            // shallow leaves belong to k_heavy_leaf
+            uint32_t gsys = 0;
+            float th2 = theta2;
+            if (tv.part_sys) {
+                gsys = tv.part_sys[tv.info[pid].x];
+                th2 = tv.sys_theta2[gsys];
+                if (MODE == MODE_LEAF && ((int)dp < tv.sys_heavy[gsys] ||
+                                          ((tv.sys_maxleaf[gsys] >= kDenseSwitch) != DENSE)))
+                    continue;
+            }
             uint32_t cl = 0;
             if (lane < nc) {
                 sm.cgeo[lane] = tv.geo[fc + lane];
@@ -674,7 +688,7 @@ __global__ void __launch_bounds__(kTravThreads,
                 uint32_t tot;
                 if (root_pending) {
                     if (lane == 0) {
-                        sm.cand_node[0] = 0;  // the root
+                        sm.cand_node[0] = gsys;  // the (system's) root
                         sm.cand_mask[0] = (uint8_t)tgt_mask;
                         if constexpr (MODE == MODE_LEAF && XL) sm.cand_lvl[0] = 0;
                     }
@@ -773,7 +787,7 @@ __global__ void __launch_bounds__(kTravThreads,
                         float dx, dy, dz, d2;
                         const bool act = (smask >> q) & 1u;
                         const bool sep = mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z,
-                                                       sg.w, theta2, dx, dy, dz, d2) && act;
+                                                       sg.w, th2, dx, dy, dz, d2) && act;
                         // branch-free: every lane evaluates, only separated pairs add
                         float fx, fy, fz;
                         if constexpr (GRAD) {
@@ -830,7 +844,7 @@ __global__ void __launch_bounds__(kTravThreads,
                                 const float4 cg = sm.chain_geo[slvl - 1];
                                 float dx, dy, dz, d2;
                                 if (mac_separated(cg.x, cg.y, cg.z, cg.w, sg.x, sg.y, sg.z, sg.w,
-                                                  theta2, dx, dy, dz, d2)) {
+                                                  th2, dx, dy, dz, d2)) {
                                     float fx, fy, fz;
                                     m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
                                     cacc0 += fx;
@@ -1263,6 +1277,8 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
     uint32_t* fb = fa + A.heavy_fcap;
     uint32_t* const fp = fa + 2 * (size_t)A.heavy_fcap;  // P2P sources of a multi-particle leaf
     uint32_t leaves = 0, pid = 0, dp = 0, fc = 0;  // current group's leaf children
+    uint32_t gsys = 0;                              // ... its system (batched systems)
+    float th2 = theta2;
     for (;;) {
         if (leaves == 0) {
             // next group with leaf children
@@ -1275,6 +1291,12 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
             for (int d = 1; d < A.heavy_depth && d < kMaxDepth; ++d)
                 if (g >= cum[d]) dp = d;
             pid = tv.lvl_base[dp] + (g - cum[dp]);
+            if (tv.part_sys) {
+                // batched systems: only the groups shallow for their own system
+                gsys = tv.part_sys[tv.info[pid].x];
+                if ((int)dp >= tv.sys_heavy[gsys]) continue;
+                th2 = tv.sys_theta2[gsys];
+            }
             const uint32_t plink = tv.link[pid];
             fc = plink & kLinkMask;
             for (uint32_t q = 0; q < (plink >> 28); ++q)
@@ -1291,7 +1313,7 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
         // initial candidates: cand(p)
         uint32_t F = 0;
         if (dp <= 1) {
-            if (tid == 0) fa[0] = 0;  // the root
+            if (tid == 0) fa[0] = gsys;  // the (system's) root
             F = 1;
         } else {
             const uint32_t* nsl = A.ns + tv.ns_off[pid];
@@ -1329,7 +1351,7 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
                     sn = fa[i];
                     const float4 sg = tv.geo[sn];
                     float dx, dy, dz, d2;
-                    if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w, theta2, dx,
+                    if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w, th2, dx,
                                       dy, dz, d2)) {
                         const float4 mp = tv.mp[sn];
                         float fx, fy, fz;

@@ -115,12 +115,48 @@ __device__ __forceinline__ void thread_flags(const uint32_t* __restrict__ codes,
     }
 }
 
+// Many systems in one array: the same rules inside each system's range,
+// with its own leaf capacity; a system's first position starts its root (a
+// depth-0 node, node k of level 0) and no run crosses a system boundary.
+__device__ __forceinline__ void thread_flags_forest(const uint32_t* __restrict__ codes, size_t n,
+                                                    size_t p0, const TreeView& tv,
+                                                    uint32_t (&f)[kTreePer]) {
+#pragma unroll 1
+    for (int q = 0; q < kTreePer; ++q) {
+        const size_t i = p0 + q;
+        if (i >= n) {
+            f[q] = 0u;
+            continue;
+        }
+        const uint32_t k = tv.part_sys[i];
+        const size_t lo = tv.sys_off[k], hi = tv.sys_off[k + 1];
+        const uint32_t cap = tv.sys_cap[k];
+        const bool first = i == lo;
+        const int cpl_i = first ? -1 : cpl2(codes[i - 1], codes[i]);
+        int w;
+        if (cap <= 1u) {
+            const int cnext = i + 1 < hi ? cpl2(codes[i], codes[i + 1]) : -1;
+            w = max(cpl_i, cnext);
+        } else {
+            w = hi - lo >= 2 ? 0 : -1;
+            const size_t jlo = i >= lo + cap ? i - cap : lo;
+            if (hi >= lo + cap + 1) {
+                const size_t jhi = min(i, hi - 1 - cap);
+                for (size_t j = jlo; j <= jhi; ++j) w = max(w, cpl2(codes[j], codes[j + cap]));
+            }
+        }
+        f[q] = node_flags(cpl_i, w, first);
+    }
+}
+
 __global__ void __launch_bounds__(kTreeThreads) k_tree_count(const uint32_t* __restrict__ codes,
                                                             size_t n, uint32_t cap,
-                                                            uint32_t* __restrict__ tile_cnt) {
+                                                            uint32_t* __restrict__ tile_cnt,
+                                                            const TreeView tv) {
     const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
     uint32_t f[kTreePer];
-    thread_flags(codes, n, p0, cap, f);
+    if (tv.part_sys) thread_flags_forest(codes, n, p0, tv, f);
+    else thread_flags(codes, n, p0, cap, f);
     unsigned long long lo = 0, hi = 0;
 #pragma unroll
     for (int q = 0; q < kTreePer; ++q) add_flags(lo, hi, f[q]);
@@ -172,7 +208,7 @@ __global__ void __launch_bounds__(1024) k_tree_scan(uint32_t* __restrict__ tile_
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        status->lvl_count[0] = 1;
+        status->lvl_count[0] = tv.part_sys ? tv.nsys : 1u;
         status->lvl_count[kLevels] = 0;
     }
 }
@@ -227,7 +263,9 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
     }
     const size_t p0 = (size_t)blockIdx.x * kTreeTile + (size_t)threadIdx.x * kTreePer;
     uint32_t f[kTreePer];
-    thread_flags(codes, n, p0, cap, f);
+    const bool forest = tv.part_sys != nullptr;
+    if (forest) thread_flags_forest(codes, n, p0, tv, f);
+    else thread_flags(codes, n, p0, cap, f);
     unsigned long long lo = 0, hi = 0;
 #pragma unroll
     for (int q = 0; q < kTreePer; ++q) add_flags(lo, hi, f[q]);
@@ -263,7 +301,7 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
         rank[d] = tv.lvl_base[d] + s_off[d] + get_cnt(elo, ehi, d);
     rank[kMaxDepth + 1] = 0;
 
-    if (p0 == 0) {  // root
+    if (p0 == 0 && !forest) {  // root
         tv.geo[0] = make_float4(cx, cy, cz, hw);
         tv.info[0] = make_uint4(0u, (uint32_t)n, tv.lvl_base[1], pack_flags(0, 0, 0));
         tv.parent[0] = kNone;
@@ -275,16 +313,36 @@ __global__ void __launch_bounds__(kTreeThreads) k_tree_emit(const uint32_t* __re
     for (int q = 0; q < kTreePer; ++q) {
         const size_t i = p0 + q;
         const uint32_t fq = f[q];
+        uint32_t sys = 0;
+        if (forest && i < n) {
+            // this position's system: its root box (README.md:76-78) and, at
+            // its first position, its root node
+            sys = tv.part_sys[i];
+            const float* bb = tv.sys_bbox + 4 * sys;
+            hw = __fdiv_rn(bb[2], 2.0f);
+            cx = cy = cz = __fadd_rn(bb[0], hw);
+            const uint32_t lo_s = tv.sys_off[sys];
+            if (i == lo_s) {
+                tv.geo[sys] = make_float4(cx, cy, cz, hw);
+                tv.info[sys] = make_uint4(lo_s, tv.sys_off[sys + 1] - lo_s, rank[1],
+                                          pack_flags(0, 0, 0));
+                tv.parent[sys] = kNone;
+                tv.cbase[sys] = rank[1];
+                tv.arrive[sys] = 0;
+                tv.lt[sys] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
         if (fq) {
             const uint32_t code = codes[i];
+            const size_t run_n = forest ? tv.sys_off[sys + 1] : n;
 #pragma unroll 1
             for (int d = 1; d <= kMaxDepth; ++d) {
                 if (!((fq >> (d - 1)) & 1u)) continue;
                 const uint32_t id = rank[d];
                 if (id - tv.lvl_base[d] >= status->lvl_count[d]) continue;  // capacity guard
-                const size_t end = run_end(codes, n, i, d);
+                const size_t end = run_end(codes, run_n, i, d);
                 const uint32_t cnt = (uint32_t)(end - i);
-                uint32_t par = 0;
+                uint32_t par = forest ? sys : 0u;
                 if (d > 1) par = rank[d - 1] + ((fq >> (d - 2)) & 1u) - 1u;
                 const uint32_t cb = d < kMaxDepth ? rank[d + 1] : 0u;
                 tv.geo[id] = node_centre(code, d, cx, cy, cz, hw);
@@ -328,6 +386,9 @@ __global__ void __launch_bounds__(256) k_tree_link(TreeView tv, const Status* st
         tv.link[id] = nch ? ((inf.z & kLinkMask) | (nch << 28)) : 0u;
         tv.lt[id] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (nch == 0 && inf.y > max_leaf) max_leaf = inf.y;
+        // batched systems: each system picks its own leaf-pass variant
+        if (nch == 0 && tv.part_sys && inf.y >= 32u)
+            atomicMax(&tv.sys_maxleaf[tv.part_sys[inf.x]], inf.y);
     }
     max_leaf = __reduce_max_sync(0xFFFFFFFFu, max_leaf);
     if (lane_id() == 0 && max_leaf) atomicMax(&const_cast<Status*>(status)->max_leaf, max_leaf);
@@ -373,7 +434,7 @@ void launch_tree(const uint32_t* codes, size_t n, uint32_t* tile_buf, TreeView t
                  Status* status, float cx, float cy, float cz, float hw, int grid,
                  cudaStream_t st, const float* bbox, uint32_t leaf_cap) {
     const int tiles = (int)((n + kTreeTile - 1) / kTreeTile);
-    k_tree_count<<<tiles, kTreeThreads, 0, st>>>(codes, n, leaf_cap, tile_buf);
+    k_tree_count<<<tiles, kTreeThreads, 0, st>>>(codes, n, leaf_cap, tile_buf, tv);
     k_tree_scan<<<1, 1024, 0, st>>>(tile_buf, tiles, tv, status);
     k_tree_emit<<<tiles, kTreeThreads, 0, st>>>(codes, n, tile_buf, tv, status, cx, cy, cz, hw,
                                                 bbox, leaf_cap);

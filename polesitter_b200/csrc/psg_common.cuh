@@ -56,6 +56,17 @@ struct TreeView {
     uint32_t* dbg_p2p;     // per node P2P leaf-pair count (debug)
     float4* lg0;           // closure order 1: field gradient xx, yy, zz, xy
     float2* lg1;           //                  and xz, yz (null when unused)
+    // many independent systems in one tree pass (the batched ensemble): the
+    // particles of system k are [sys_off[k], sys_off[k + 1]), its root is
+    // node k of level 0.  part_sys == null: one system, root node 0.
+    const uint32_t* part_sys;   // system of each particle position
+    const uint32_t* sys_off;    // [nsys + 1]
+    const uint32_t* sys_cap;    // leaf capacity per system
+    const float* sys_bbox;      // (min, max, range, 1023 / range) per system
+    const float* sys_theta2;    // theta * theta (rounded) per system
+    const int32_t* sys_heavy;   // shallow-leaf depth per system
+    uint32_t* sys_maxleaf;      // particles in each system's fullest leaf (this tick)
+    uint32_t nsys;
     uint32_t lvl_base[kLevels + 1];
     uint32_t lvl_cap[kLevels + 1];
 };
@@ -71,7 +82,7 @@ struct Status {
     unsigned long long stat[16];           // debug totals (see PSG_STAT_*)
     uint32_t max_stack;                    // deepest DFS stack seen (debug)
     uint32_t p2p_chunks;                   // P2P chunks used this tick
-    uint32_t sort_tiles[4];                // onesweep tile tickets
+    uint32_t sort_tiles[6];                // onesweep tile tickets (code + system passes)
     uint32_t dense_count;                  // full-leaf P2P records written
     uint32_t dense_work;                   // ... and taken by k_dense_p2p
     uint32_t max_leaf;                     // particles in the fullest leaf

@@ -14,6 +14,13 @@ struct P2PStore;
 // k_prepare.cu -- bbox + Morton codes (polesitter.h:1911-2170)
 void launch_prepare(const float* x, const float* y, const float* z, size_t n, float2* partial,
                     int grid, uint32_t* codes, float* bbox_out, int variant, cudaStream_t st);
+// many systems in one array: block b covers particles [blk[b].y, blk[b].z) of
+// system blk[b].x, the blocks of system k are [sys_blk[k], sys_blk[k + 1]);
+// sys_bbox receives (min, max, range, 1023 / range) per system
+void launch_prepare_forest(const float* x, const float* y, const float* z, const uint4* blk,
+                           int nblk, const uint32_t* sys_blk, const uint32_t* sys_off,
+                           float2* partial, uint32_t* codes, float* sys_bbox, int variant,
+                           cudaStream_t st);
 
 // k_sort.cu -- stable LSD radix sort + gather (polesitter.h:1588-1693)
 struct SortBuffers {
@@ -29,6 +36,12 @@ struct SortBuffers {
 int sort_tile_size();
 void launch_sort(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* status,
                  cudaStream_t st, int spin_limit = 0);
+// many systems in one array: each sorted within its range (sys_passes stable
+// passes on the system index after the code passes; lookback sized for 4 +
+// sys_passes passes)
+void launch_sort_forest(SortBuffers& b, uint32_t* codes, size_t n, int grid, Status* status,
+                        cudaStream_t st, const uint32_t* part_sys, int sys_passes,
+                        const uint32_t* sys_offs);
 void launch_gather(const uint32_t* perm, const float* x, const float* y, const float* z,
                    const float* m, const uint32_t* id, size_t n, float4* xyzm, uint32_t* ids,
                    int grid, cudaStream_t st);
@@ -75,6 +88,13 @@ struct TickState {
 };
 void launch_tick_reset_ids(uint32_t* id, size_t n, int grid, cudaStream_t st);
 void launch_tick_euler(const TickState& t, size_t n, float dt, int grid, cudaStream_t st);
+// many systems in one array (system k at [sys_off[k], sys_off[k + 1]))
+void launch_forest_reset_ids(uint32_t* id, size_t n, const uint32_t* part_sys,
+                             const uint32_t* sys_off, int grid, cudaStream_t st);
+void launch_forest_euler(const TickState& t, size_t n, float dt, const uint32_t* part_sys,
+                         const uint32_t* sys_off, int grid, cudaStream_t st);
+void launch_forest_single_forces(const uint32_t* sys_off, uint32_t nsys, float* fx, float* fy,
+                                 float* fz, cudaStream_t st);
 
 // k_closure.cu -- the learned far-field closure (no counterpart in the reference)
 struct MlpPacked;

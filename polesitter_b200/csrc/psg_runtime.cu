@@ -110,6 +110,7 @@ struct State {
     cudaStream_t aux;      // k_heavy_leaf, beside the leaf pass
     cudaEvent_t ev_levels, ev_heavy;
     int heavy_depth;       // option; < 0: derived from theta
+    int forest_heavy;      // many systems: the deepest of their shallow-leaf depths
     int ns_levels;         // near lists are stored for node depths <= this (kMaxDepth: all);
                            // lowered when they do not fit, deeper groups walk their chains
     int stream_p2p;        // P2P summed in the leaf pass as found (no spill store)
@@ -264,7 +265,10 @@ static void free_state(State* s) {
     s->magic = 0;
 }
 
-static int init_state(State* s, size_t maxp, float theta) {
+// lvl_caps (optional): node capacity of each level, for a tree pass over
+// many systems; sort_passes: radix passes the look-back flags must serve
+static int init_state(State* s, size_t maxp, float theta, const uint32_t* lvl_caps = nullptr,
+                      int sort_passes = 4) {
     std::memset(s, 0, sizeof(State));
     PSG_CHECK(cudaGetDevice(&s->device));
     PSG_CHECK(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device));
@@ -283,7 +287,7 @@ static int init_state(State* s, size_t maxp, float theta) {
     PSG_ALLOC(s->sort.hist, 4 * 256 * 4);
     PSG_ALLOC(s->sort.offs, 4 * 256 * 4);
     const size_t stiles = (n + sort_tile_size() - 1) / sort_tile_size();
-    PSG_ALLOC(s->sort.lookback, 4 * stiles * 256 * 4);
+    PSG_ALLOC(s->sort.lookback, (size_t)sort_passes * stiles * 256 * 4);
     const size_t ttiles = (n + tree_tile_size() - 1) / tree_tile_size();
     PSG_ALLOC(s->tree_tiles, ttiles * kMaxDepth * 4);
     // level capacities: min(8^d, n) nodes at depth d
@@ -292,6 +296,7 @@ static int init_state(State* s, size_t maxp, float theta) {
         unsigned long long cap8 = 1ull << (3 * d);
         uint32_t cap = (uint32_t)(cap8 < n ? cap8 : n);
         if (d == 0) cap = 1;
+        if (lvl_caps) cap = lvl_caps[d];
         s->tv.lvl_base[d] = base;
         s->tv.lvl_cap[d] = cap;
         base += cap;
@@ -378,11 +383,16 @@ static int closure_alloc(State* s) {
 // at depth d (half width H / 2^d of the root's H) stays unseparated from the
 // sources within about theta H / 2^(d-1), a large part of the tree once
 // 2^d <= 4 theta.
-static int heavy_depth_for(const State* s) {
-    if (s->heavy_depth >= 0) return s->heavy_depth > 5 ? 5 : s->heavy_depth;
+static int heavy_depth_of(float theta) {
     int d = 0;
-    while (d < 5 && (float)(2 << d) <= 4.0f * s->theta) ++d;
+    while (d < 5 && (float)(2 << d) <= 4.0f * theta) ++d;
     return d < 2 ? 2 : d;
+}
+
+static int heavy_depth_for(const State* s) {
+    if (s->tv.part_sys) return s->forest_heavy;  // many systems: the deepest of theirs
+    if (s->heavy_depth >= 0) return s->heavy_depth > 5 ? 5 : s->heavy_depth;
+    return heavy_depth_of(s->theta);
 }
 
 // Depth of the deepest nodes whose near lists this traversal stores.  The
@@ -449,7 +459,9 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
     launch_heavy_leaf(A, scaled(s->heavy_slots), s->aux);
     PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
-    launch_leaf_start(s->d_status, A.heavy_depth, o, s->stream);
+    // one system: the leaf pass starts past the shallow groups; many: each
+    // group checks its own system's depth
+    launch_leaf_start(s->d_status, s->tv.part_sys ? 0 : A.heavy_depth, o, s->stream);
     const int xl = (A.ns_levels < kMaxDepth || A.stream) ? 1 : 0;
     const int lg[2] = {scaled(s->trav_grid[o][0][xl]), scaled(s->trav_grid[o][1][xl])};
     launch_traverse_leaves(A, lg, s->stream);
@@ -916,38 +928,66 @@ static int prepare(const psg_arrays_t* a, float* out_min, float* out_max, float*
     return PSG_OK;
 }
 
-// ---- batched ensemble: many independent systems per tick in CUDA graphs ----
+// ---- batched ensemble: many independent systems in one tree pass ----------
 //
-// Every system keeps its own context (tree, stores, streams).  One tick of
-// all systems is two CUDA graphs captured once and replayed: the forces
-// graph forks one branch per system (ids reset, prepare with the root taken
-// on the device, sort, tree, upward, traversal, status copy) and joins them;
-// the step graph does each system's velocity permutation + Euler.  Between
-// the two the host reads every system's status once: a store that ran out is
-// regrown and that system's traversal rerun directly, and both graphs are
-// captured again with the new buffers.
+// All systems share one set of device buffers: their particles are the
+// caller's concatenated arrays (system k at [off_k, off_k + N_k)), and every
+// phase of the tick is one launch over all of them -- the segmented bounding
+// box and Morton codes, the radix sort (four code passes, then stable passes
+// on the system index, so each system ends sorted within its range), the
+// tree build (a system's first position starts its root, node k of level 0;
+// no run crosses a system boundary), the level-synchronous upward pass, and
+// the persistent traversal kernels, whose work queues run over the groups of
+// every system with each group's own theta, root, leaf-pass variant and
+// shallow-leaf depth.  Per system the arithmetic is exactly that of its own
+// tick, so the results equal each system's ps_b200_run_ticks bit for bit.
+// One tick is two CUDA graphs captured once and replayed (forces; velocity
+// permutation + Euler); between them the host reads the one status block and
+// regrows a store that ran out (then that traversal is rerun and the graphs
+// are captured again).
 
 constexpr uint32_t kEnsMagic = 0x50534745u;  // "PSGE"
+constexpr uint32_t kForestBlock = 1024;      // particles per prepare block
 
 struct Ensemble {
     uint32_t magic = 0;
     int device = 0;
     size_t nsys = 0, total = 0;
     std::vector<size_t> count, offset;
-    std::vector<State*> sys;
-    std::vector<cudaEvent_t> join;
-    cudaEvent_t fork = nullptr;
-    cudaStream_t root = nullptr;
+    std::vector<float> theta;       // per system
+    std::vector<uint32_t> cap;      // leaf capacity per system
+    State* fs = nullptr;            // the device state of all systems together
+    // per-system tables (device)
+    uint32_t* part_sys = nullptr;   // system of each particle position
+    uint32_t* sys_off = nullptr;    // [nsys + 1]
+    uint32_t* sys_cap = nullptr;
+    float* sys_theta2 = nullptr;
+    int32_t* sys_heavy = nullptr;
+    float* sys_bbox = nullptr;      // [nsys][4]
+    uint32_t* sys_maxleaf = nullptr;
+    uint32_t* sys_sort_offs = nullptr;  // digit starts of the system sort passes
+    int sys_passes = 1;
+    uint4* blk = nullptr;           // prepare blocks: (system, first, end)
+    uint32_t* sys_blk = nullptr;    // [nsys + 1]
+    float2* partial = nullptr;
+    int nblk = 0;
+    float* vtmp = nullptr;          // 3 x total velocity scratch
     cudaGraphExec_t g_force = nullptr, g_step = nullptr;
     bool dirty = true;
-    DevArrays cap{};          // arrays the graphs were captured with
+    DevArrays cap_arr{};            // arrays the graphs were captured with
     float* cap_v[3] = {nullptr, nullptr, nullptr};
     float cap_dt = 0.f;
-    float* vtmp = nullptr;    // 3 x total velocity scratch
     double grid_scale = 1.0;
     int variant = PSG_MORTON_AVX2;
     std::vector<uint32_t> leaf_ladder{1u, 16u, 32u, 64u};  // leaf capacities the autotuner tries
 };
+
+static DevArrays slice(const DevArrays& a, size_t off) {
+    DevArrays d = a;
+    d.x += off; d.y += off; d.z += off; d.m += off;
+    d.fx += off; d.fy += off; d.fz += off; d.id += off; d.codes += off;
+    return d;
+}
 
 static int ensure_tick_scratch(State* s) {
     if (s->tk_bbox) return PSG_OK;
@@ -959,57 +999,26 @@ static int ensure_tick_scratch(State* s) {
     return PSG_OK;
 }
 
-static DevArrays slice(const DevArrays& a, size_t off) {
-    DevArrays d = a;
-    d.x += off; d.y += off; d.z += off; d.m += off;
-    d.fx += off; d.fy += off; d.fz += off; d.id += off; d.codes += off;
-    return d;
-}
-
-// one system's forces for a tick, enqueued on s->stream without any host
-// synchronisation (capturable)
-static int enqueue_system_forces(State* s, const DevArrays& d, size_t n, int variant) {
-    cudaStream_t st = s->stream;
-    const int g = grid_for(s, n, 1024);
-    int gp = (int)((n + 1023) / 1024);
-    if (gp > s->tk_grid) gp = s->tk_grid;
-    launch_tick_reset_ids(d.id, n, g, st);
-    launch_prepare(d.x, d.y, d.z, n, s->tk_partial, gp, d.codes, s->tk_bbox, variant, st);
-    PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
-    launch_sort(s->sort, d.codes, n, g, s->d_status, st);
-    launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
-    launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
-    const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
-    launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, 0.f, 0.f, 0.f, 0.f, gt, st,
-                s->tk_bbox, s->leaf_cap);
-    launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
-    if (n > 1) {
-        s->trav_n = n;
-        int r = enqueue_traversal(s, s->xyzm, d.fx, d.fy, d.fz);
-        if (r != PSG_OK) return r;
-    } else {
-        PSG_CHECK(cudaMemsetAsync(d.fx, 0, 4, st));
-        PSG_CHECK(cudaMemsetAsync(d.fy, 0, 4, st));
-        PSG_CHECK(cudaMemsetAsync(d.fz, 0, 4, st));
+// theta, theta^2 (rounded as the MAC rounds it), shallow-leaf depth and leaf
+// capacity of every system to the device tables
+static int upload_systems(Ensemble* e) {
+    std::vector<float> th2(e->nsys);
+    std::vector<int32_t> hv(e->nsys);
+    int hmax = 2;
+    for (size_t k = 0; k < e->nsys; ++k) {
+        const float t = e->theta[k];
+        th2[k] = t * t;
+        hv[k] = heavy_depth_of(t);
+        hmax = std::max(hmax, (int)hv[k]);
     }
-    PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status), cudaMemcpyDeviceToHost,
-                              st));
-    return PSG_OK;
-}
-
-// one system's velocity permutation through ids + semi-implicit Euler
-static int enqueue_system_step(State* s, const DevArrays& d, float* const v[3], float* vt,
-                               size_t n, float dt) {
-    cudaStream_t st = s->stream;
-    TickState ts;
-    ts.id = d.id;
-    ts.vx_in = v[0]; ts.vy_in = v[1]; ts.vz_in = v[2];
-    ts.vx_out = vt; ts.vy_out = vt + n; ts.vz_out = vt + 2 * n;
-    ts.x = d.x; ts.y = d.y; ts.z = d.z; ts.m = d.m;
-    ts.fx = d.fx; ts.fy = d.fy; ts.fz = d.fz;
-    launch_tick_euler(ts, n, dt, grid_for(s, n, 1024), st);
-    for (int c = 0; c < 3; ++c)
-        PSG_CHECK(cudaMemcpyAsync(v[c], vt + c * n, n * 4, cudaMemcpyDeviceToDevice, st));
+    PSG_CHECK(cudaMemcpy(e->sys_theta2, th2.data(), e->nsys * 4, cudaMemcpyHostToDevice));
+    PSG_CHECK(cudaMemcpy(e->sys_heavy, hv.data(), e->nsys * 4, cudaMemcpyHostToDevice));
+    PSG_CHECK(cudaMemcpy(e->sys_cap, e->cap.data(), e->nsys * 4, cudaMemcpyHostToDevice));
+    if (hmax != e->fs->forest_heavy) e->dirty = true;  // a launch parameter changes
+    e->fs->forest_heavy = hmax;
+    // the stores' near-list depth and P2P mode start over with the settings
+    e->fs->ns_levels = kMaxDepth;
+    e->fs->stream_p2p = 0;
     return PSG_OK;
 }
 
@@ -1020,32 +1029,59 @@ static void drop_graphs(Ensemble* e) {
     e->dirty = true;
 }
 
-// capture one graph: a branch per system, forked from and joined into root
+// one tick's forces of all systems, enqueued on the forest stream without
+// any host synchronisation (capturable)
+static int enqueue_forest_forces(Ensemble* e, const DevArrays& d) {
+    State* s = e->fs;
+    cudaStream_t st = s->stream;
+    const size_t n = e->total;
+    const int g = grid_for(s, n, 1024);
+    launch_forest_reset_ids(d.id, n, e->part_sys, e->sys_off, g, st);
+    launch_prepare_forest(d.x, d.y, d.z, e->blk, e->nblk, e->sys_blk, e->sys_off, e->partial,
+                          d.codes, e->sys_bbox, e->variant, st);
+    PSG_CHECK(cudaMemsetAsync(s->d_status, 0, sizeof(Status), st));
+    PSG_CHECK(cudaMemsetAsync(e->sys_maxleaf, 0, e->nsys * 4, st));
+    launch_sort_forest(s->sort, d.codes, n, g, s->d_status, st, e->part_sys, e->sys_passes,
+                       e->sys_sort_offs);
+    launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
+    launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
+    const int gt = (int)((s->tv.lvl_base[kLevels] + 255) / 256);
+    launch_tree(d.codes, n, s->tree_tiles, s->tv, s->d_status, 0.f, 0.f, 0.f, 0.f, gt, st,
+                nullptr, 1);
+    launch_upward(s->tv, s->d_status, s->xyzm, gt, st);
+    s->trav_n = n;
+    int r = enqueue_traversal(s, s->xyzm, d.fx, d.fy, d.fz);
+    if (r != PSG_OK) return r;
+    launch_forest_single_forces(e->sys_off, (uint32_t)e->nsys, d.fx, d.fy, d.fz, st);
+    PSG_CHECK(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(Status), cudaMemcpyDeviceToHost,
+                              st));
+    return PSG_OK;
+}
+
+// every system's velocity permutation through its ids + semi-implicit Euler
+static int enqueue_forest_step(Ensemble* e, const DevArrays& d, float* const v[3], float dt) {
+    State* s = e->fs;
+    cudaStream_t st = s->stream;
+    const size_t n = e->total;
+    TickState ts;
+    ts.id = d.id;
+    ts.vx_in = v[0]; ts.vy_in = v[1]; ts.vz_in = v[2];
+    ts.vx_out = e->vtmp; ts.vy_out = e->vtmp + n; ts.vz_out = e->vtmp + 2 * n;
+    ts.x = d.x; ts.y = d.y; ts.z = d.z; ts.m = d.m;
+    ts.fx = d.fx; ts.fy = d.fy; ts.fz = d.fz;
+    launch_forest_euler(ts, n, dt, e->part_sys, e->sys_off, grid_for(s, n, 1024), st);
+    for (int c = 0; c < 3; ++c)
+        PSG_CHECK(cudaMemcpyAsync(v[c], e->vtmp + c * n, n * 4, cudaMemcpyDeviceToDevice, st));
+    return PSG_OK;
+}
+
 static int capture(Ensemble* e, bool forces, const DevArrays& a, float* const v[3], float dt,
                    cudaGraphExec_t* out) {
-    PSG_CHECK(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
-    int r = PSG_OK;
-    if (cudaEventRecord(e->fork, e->root) != cudaSuccess) r = PSG_EDEVICE;
-    for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
-        State* s = e->sys[k];
-        if (cudaStreamWaitEvent(s->stream, e->fork, 0) != cudaSuccess) {
-            r = PSG_EDEVICE;
-            break;
-        }
-        const DevArrays d = slice(a, e->offset[k]);
-        if (forces) {
-            r = enqueue_system_forces(s, d, e->count[k], e->variant);
-        } else {
-            float* vk[3] = {v[0] + e->offset[k], v[1] + e->offset[k], v[2] + e->offset[k]};
-            r = enqueue_system_step(s, d, vk, e->vtmp + 3 * e->offset[k], e->count[k], dt);
-        }
-        if (r != PSG_OK) break;
-        if (cudaEventRecord(e->join[k], s->stream) != cudaSuccess ||
-            cudaStreamWaitEvent(e->root, e->join[k], 0) != cudaSuccess)
-            r = PSG_EDEVICE;
-    }
+    cudaStream_t st = e->fs->stream;
+    PSG_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int r = forces ? enqueue_forest_forces(e, a) : enqueue_forest_step(e, a, v, dt);
     cudaGraph_t graph = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(e->root, &graph);
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     if (r == PSG_OK && ce != cudaSuccess) {
         note("cudaStreamEndCapture", ce);
         r = PSG_EDEVICE;
@@ -1062,19 +1098,19 @@ static int capture(Ensemble* e, bool forces, const DevArrays& a, float* const v[
 }
 
 static int ensure_graphs(Ensemble* e, const DevArrays& a, float* const v[3], float dt) {
-    const bool same = !e->dirty && std::memcmp(&e->cap, &a, sizeof(DevArrays)) == 0 &&
+    const bool same = !e->dirty && std::memcmp(&e->cap_arr, &a, sizeof(DevArrays)) == 0 &&
                       e->cap_v[0] == v[0] && e->cap_v[1] == v[1] && e->cap_v[2] == v[2] &&
                       e->cap_dt == dt;
     if (same) return PSG_OK;
     drop_graphs(e);
-    for (State* s : e->sys) s->grid_scale = e->grid_scale;
+    e->fs->grid_scale = e->grid_scale;
     int r = capture(e, true, a, v, dt, &e->g_force);
     if (r == PSG_OK) r = capture(e, false, a, v, dt, &e->g_step);
     if (r != PSG_OK) {
         drop_graphs(e);
         return r;
     }
-    e->cap = a;
+    e->cap_arr = a;
     for (int c = 0; c < 3; ++c) e->cap_v[c] = v[c];
     e->cap_dt = dt;
     e->dirty = false;
@@ -1082,26 +1118,28 @@ static int ensure_graphs(Ensemble* e, const DevArrays& a, float* const v[3], flo
 }
 
 // after a forces replay: fatal status -> error; capacity bits -> regrow and
-// rerun that system's traversal, and capture again before the next tick
-static int check_systems(Ensemble* e, const DevArrays& a) {
-    for (size_t k = 0; k < e->nsys; ++k) {
-        State* s = e->sys[k];
-        const uint32_t err = s->h_status->err;
-        if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_CHAIN_ORDER)) {
-            std::snprintf(g_err, sizeof(g_err), "ensemble system %zu: device status 0x%x", k, err);
-            return (err & PSG_ERR_NODES) ? PSG_EINVAL : PSG_EDEVICE;
+// rerun the traversal, and capture again before the next tick
+static int check_forest(Ensemble* e, const DevArrays& a) {
+    State* s = e->fs;
+    const uint32_t err = s->h_status->err;
+    if (err & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_CHAIN_ORDER)) {
+        std::snprintf(g_err, sizeof(g_err), "ensemble: device status 0x%x", err);
+        return (err & PSG_ERR_NODES) ? PSG_EINVAL : PSG_EDEVICE;
+    }
+    if (err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW | PSG_ERR_DENSE_OVERFLOW |
+               PSG_ERR_HEAVY_OVERFLOW)) {
+        int r = regrow(s, err);
+        if (r != PSG_OK) return r;
+        PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, s->stream));
+        uint32_t err2 = 0;
+        r = run_traversal(s, s->xyzm, a.fx, a.fy, a.fz, &err2);
+        if (r != PSG_OK) return r;
+        if (err2 & (PSG_ERR_SORT_SPIN | PSG_ERR_STACK | PSG_ERR_NODES | PSG_ERR_CHAIN_ORDER |
+                    PSG_ERR_HEAVY_OVERFLOW)) {
+            std::snprintf(g_err, sizeof(g_err), "ensemble: device status 0x%x", err2);
+            return PSG_EDEVICE;
         }
-        if (err & (PSG_ERR_NS_OVERFLOW | PSG_ERR_P2P_OVERFLOW | PSG_ERR_DENSE_OVERFLOW |
-                   PSG_ERR_HEAVY_OVERFLOW)) {
-            int r = regrow(s, err);
-            if (r != PSG_OK) return r;
-            PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, s->stream));
-            const DevArrays d = slice(a, e->offset[k]);
-            uint32_t err2 = 0;
-            r = run_traversal(s, s->xyzm, d.fx, d.fy, d.fz, &err2);
-            if (r != PSG_OK) return r;
-            e->dirty = true;
-        }
+        e->dirty = true;
     }
     return PSG_OK;
 }
@@ -1126,19 +1164,18 @@ static int ens_map(Ensemble* e, const psg_arrays_t* a, DevArrays& d) {
 }
 
 static void free_ensemble(Ensemble* e) {
-    if (e->root) cudaStreamSynchronize(e->root);
+    if (e->fs && e->fs->stream) cudaStreamSynchronize(e->fs->stream);
     drop_graphs(e);
-    for (State* s : e->sys) {
-        if (s) {
-            free_state(s);
-            delete s;
-        }
+    if (e->fs) {
+        if (e->fs->magic == kMagic) free_state(e->fs);
+        delete e->fs;
+        e->fs = nullptr;
     }
-    for (cudaEvent_t ev : e->join)
-        if (ev) cudaEventDestroy(ev);
-    if (e->fork) cudaEventDestroy(e->fork);
-    if (e->root) cudaStreamDestroy(e->root);
-    if (e->vtmp) cudaFree(e->vtmp);
+    void* ps[] = {e->part_sys, e->sys_off, e->sys_cap, e->sys_theta2, e->sys_heavy,
+                  e->sys_bbox, e->sys_maxleaf, e->sys_sort_offs, e->blk, e->sys_blk,
+                  e->partial, e->vtmp};
+    for (void* p : ps)
+        if (p) cudaFree(p);
     e->magic = 0;
 }
 
@@ -1153,22 +1190,87 @@ static int ens_create(Ensemble* e, const size_t* counts, size_t nsys, const floa
         off += counts[k];
     }
     e->total = off;
-    PSG_CHECK(cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking));
-    PSG_CHECK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
-    e->join.assign(nsys, nullptr);
-    e->sys.assign(nsys, nullptr);
-    for (size_t k = 0; k < nsys; ++k) {
-        PSG_CHECK(cudaEventCreateWithFlags(&e->join[k], cudaEventDisableTiming));
-        State* s = new (std::nothrow) State;
-        if (!s) return PSG_EALLOC;
-        e->sys[k] = s;
-        const float th = theta && theta[k] > 0.f ? theta[k] : 2.0f;
-        int r = init_state(s, counts[k], th);
-        if (r != PSG_OK) return r;
-        r = ensure_tick_scratch(s);
-        if (r != PSG_OK) return r;
+    if (off >= 0xFFFFFFF0ull || nsys > 65536) {
+        std::snprintf(g_err, sizeof(g_err), "ensemble: at most 65,536 systems and 2^32 particles");
+        return PSG_EINVAL;
     }
-    PSG_ALLOC(e->vtmp, 3 * (e->total ? e->total : 1) * sizeof(float));
+    e->theta.resize(nsys);
+    for (size_t k = 0; k < nsys; ++k) e->theta[k] = theta && theta[k] > 0.f ? theta[k] : 2.0f;
+    e->cap.assign(nsys, 1u);
+    // level capacities: the sum over systems of min(8^d, N_k); level 0 holds
+    // the roots
+    uint32_t caps[kLevels];
+    for (int d = 0; d <= kMaxDepth; ++d) {
+        unsigned long long c = 0;
+        for (size_t k = 0; k < nsys; ++k)
+            c += d == 0 ? 1ull : std::min<unsigned long long>(1ull << (3 * d), counts[k]);
+        if (c >= 0xFFFFFFF0ull) return PSG_EINVAL;
+        caps[d] = (uint32_t)c;
+    }
+    e->sys_passes = nsys > 256 ? 2 : 1;
+    e->fs = new (std::nothrow) State;
+    if (!e->fs) return PSG_EALLOC;
+    int r = init_state(e->fs, e->total, 2.0f, caps, 4 + e->sys_passes);
+    if (r != PSG_OK) return r;
+    r = ensure_tick_scratch(e->fs);
+    if (r != PSG_OK) return r;
+    // per-system tables
+    std::vector<uint32_t> psys(e->total), soff(nsys + 1), sblk(nsys + 1);
+    std::vector<uint4> blk;
+    for (size_t k = 0; k < nsys; ++k) {
+        soff[k] = (uint32_t)e->offset[k];
+        sblk[k] = (uint32_t)blk.size();
+        for (size_t i = 0; i < counts[k]; ++i) psys[e->offset[k] + i] = (uint32_t)k;
+        for (size_t b = 0; b < counts[k]; b += kForestBlock)
+            blk.push_back(make_uint4((uint32_t)k, (uint32_t)(e->offset[k] + b),
+                                     (uint32_t)(e->offset[k] + std::min<size_t>(b + kForestBlock,
+                                                                               counts[k])),
+                                     0u));
+    }
+    soff[nsys] = (uint32_t)e->total;
+    sblk[nsys] = (uint32_t)blk.size();
+    e->nblk = (int)blk.size();
+    // digit starts of the system passes: the systems are contiguous, so a
+    // digit's start is where its first system starts (low byte pass: systems
+    // grouped by their low byte)
+    std::vector<uint32_t> so(256 * e->sys_passes, 0u);
+    for (int q = 0; q < e->sys_passes; ++q) {
+        std::vector<unsigned long long> hist(256, 0ull);
+        for (size_t k = 0; k < nsys; ++k) hist[(k >> (8 * q)) & 0xFFu] += counts[k];
+        unsigned long long run = 0;
+        for (int dgt = 0; dgt < 256; ++dgt) {
+            so[256 * q + dgt] = (uint32_t)run;
+            run += hist[dgt];
+        }
+    }
+    PSG_ALLOC(e->part_sys, e->total * 4);
+    PSG_ALLOC(e->sys_off, (nsys + 1) * 4);
+    PSG_ALLOC(e->sys_cap, nsys * 4);
+    PSG_ALLOC(e->sys_theta2, nsys * 4);
+    PSG_ALLOC(e->sys_heavy, nsys * 4);
+    PSG_ALLOC(e->sys_bbox, nsys * 16);
+    PSG_ALLOC(e->sys_maxleaf, nsys * 4);
+    PSG_ALLOC(e->sys_sort_offs, so.size() * 4);
+    PSG_ALLOC(e->blk, blk.size() * sizeof(uint4));
+    PSG_ALLOC(e->sys_blk, (nsys + 1) * 4);
+    PSG_ALLOC(e->partial, blk.size() * sizeof(float2));
+    PSG_ALLOC(e->vtmp, 3 * e->total * sizeof(float));
+    PSG_CHECK(cudaMemcpy(e->part_sys, psys.data(), e->total * 4, cudaMemcpyHostToDevice));
+    PSG_CHECK(cudaMemcpy(e->sys_off, soff.data(), (nsys + 1) * 4, cudaMemcpyHostToDevice));
+    PSG_CHECK(cudaMemcpy(e->sys_sort_offs, so.data(), so.size() * 4, cudaMemcpyHostToDevice));
+    PSG_CHECK(cudaMemcpy(e->blk, blk.data(), blk.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    PSG_CHECK(cudaMemcpy(e->sys_blk, sblk.data(), (nsys + 1) * 4, cudaMemcpyHostToDevice));
+    TreeView& tv = e->fs->tv;
+    tv.part_sys = e->part_sys;
+    tv.sys_off = e->sys_off;
+    tv.sys_cap = e->sys_cap;
+    tv.sys_bbox = e->sys_bbox;
+    tv.sys_theta2 = e->sys_theta2;
+    tv.sys_heavy = e->sys_heavy;
+    tv.sys_maxleaf = e->sys_maxleaf;
+    tv.nsys = (uint32_t)nsys;
+    r = upload_systems(e);
+    if (r != PSG_OK) return r;
     e->magic = kEnsMagic;
     return PSG_OK;
 }
@@ -1185,32 +1287,36 @@ static int ens_run(Ensemble* e, const psg_arrays_t* a, float* const v[3], float 
         }
     }
     PSG_CHECK(cudaSetDevice(e->device));
+    cudaStream_t st = e->fs->stream;
     for (uint32_t t = 0; t < ticks; ++t) {
         r = ensure_graphs(e, d, v, dt);
         if (r != PSG_OK) return r;
-        PSG_CHECK(cudaGraphLaunch(e->g_force, e->root));
-        PSG_CHECK(cudaStreamSynchronize(e->root));
-        r = check_systems(e, d);
+        PSG_CHECK(cudaGraphLaunch(e->g_force, st));
+        PSG_CHECK(cudaStreamSynchronize(st));
+        r = check_forest(e, d);
         if (r != PSG_OK) return r;
-        PSG_CHECK(cudaGraphLaunch(e->g_step, e->root));
+        PSG_CHECK(cudaGraphLaunch(e->g_step, st));
     }
-    PSG_CHECK(cudaStreamSynchronize(e->root));
+    PSG_CHECK(cudaStreamSynchronize(st));
     return PSG_OK;
 }
 
-// Autotuner.  theta: per size class (the systems with the same floor(log2 N)),
-// the smallest theta of a ladder whose median relative force error against
-// an FP64 direct sum on up to 1024 particles of the class's first system is
-// at most `target`.  Launch shape: the traversal grids' scale, among
-// {1, 1/2, 1/4} of the single-system persistent grids, by the time of one
-// forces replay of the whole ensemble.  Works on copies; the caller's arrays
-// are left as they are.
+// Autotuner.  Per size class (the systems with the same floor(log2 N)) and
+// per leaf capacity of its ladder: the smallest theta of {1, 1.5, 2, 3, 4, 6,
+// 8} whose median relative force error against an FP64 direct sum on up to
+// 1024 particles of the class's first system is at most `target` (a tick of
+// that system alone).  Then, class by class from the one holding the most
+// particles: the leaf capacity (with its theta) whose whole-ensemble forces
+// replay is fastest, among those that met the target.  Last, the traversal
+// grids' scale among {1, 1/2, 1/4} by the same replay time.  Works on copies;
+// the caller's arrays are left as they are.
 static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float* theta_out,
                         double* scale_out) {
     DevArrays d;
     int r = ens_map(e, a, d);
     if (r != PSG_OK) return r;
     PSG_CHECK(cudaSetDevice(e->device));
+    cudaStream_t st = e->fs->stream;
     const size_t T = e->total;
     float* buf = nullptr;  // scratch copy: x y z m fx fy fz (7 T floats), id, codes
     PSG_ALLOC(buf, (size_t)9 * T * 4 + 16);
@@ -1220,201 +1326,194 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
     c.id = (uint32_t*)(buf + 7 * T); c.codes = (uint32_t*)(buf + 8 * T);
     c.any_host = false;
     auto restore = [&]() -> int {
-        PSG_CHECK(cudaMemcpyAsync(c.x, d.x, T * 4, cudaMemcpyDeviceToDevice, e->root));
-        PSG_CHECK(cudaMemcpyAsync(c.y, d.y, T * 4, cudaMemcpyDeviceToDevice, e->root));
-        PSG_CHECK(cudaMemcpyAsync(c.z, d.z, T * 4, cudaMemcpyDeviceToDevice, e->root));
-        PSG_CHECK(cudaMemcpyAsync(c.m, d.m, T * 4, cudaMemcpyDeviceToDevice, e->root));
-        PSG_CHECK(cudaStreamSynchronize(e->root));
+        PSG_CHECK(cudaMemcpyAsync(c.x, d.x, T * 4, cudaMemcpyDeviceToDevice, st));
+        PSG_CHECK(cudaMemcpyAsync(c.y, d.y, T * 4, cudaMemcpyDeviceToDevice, st));
+        PSG_CHECK(cudaMemcpyAsync(c.z, d.z, T * 4, cudaMemcpyDeviceToDevice, st));
+        PSG_CHECK(cudaMemcpyAsync(c.m, d.m, T * 4, cudaMemcpyDeviceToDevice, st));
+        PSG_CHECK(cudaStreamSynchronize(st));
         return PSG_OK;
     };
     static const float ladder[] = {1.0f, 1.5f, 2.0f, 3.0f, 4.0f, 6.0f, 8.0f};
     const int nl = (int)(sizeof(ladder) / sizeof(ladder[0]));
     std::vector<int> cls(e->nsys);
-    for (size_t k = 0; k < e->nsys; ++k) cls[k] = (int)std::floor(std::log2((double)e->count[k] + 1));
-    std::vector<float> chosen(e->nsys, 0.f);
-    std::vector<uint32_t> chosen_cap(e->nsys, 1u);
+    for (size_t k = 0; k < e->nsys; ++k)
+        cls[k] = (int)std::floor(std::log2((double)e->count[k] + 1));
+    std::vector<int> classes;  // distinct classes, by the particles they hold (most first)
+    std::vector<size_t> rep;   // the first system of each class
+    {
+        std::vector<std::pair<unsigned long long, int>> held;
+        for (size_t k = 0; k < e->nsys; ++k) {
+            auto it = std::find(classes.begin(), classes.end(), cls[k]);
+            if (it == classes.end()) {
+                classes.push_back(cls[k]);
+                rep.push_back(k);
+                held.push_back({0ull, (int)classes.size() - 1});
+                it = classes.end() - 1;
+            }
+            held[it - classes.begin()].first += e->count[k];
+        }
+        std::sort(held.begin(), held.end(), [](auto& x, auto& y) { return x.first > y.first; });
+        std::vector<int> c2;
+        std::vector<size_t> r2;
+        for (auto& h : held) {
+            c2.push_back(classes[h.second]);
+            r2.push_back(rep[h.second]);
+        }
+        classes = c2;
+        rep = r2;
+    }
+    const size_t ncls = classes.size(), nlc = e->leaf_ladder.size();
+    std::vector<std::vector<float>> th(nlc, std::vector<float>(ncls, ladder[nl - 1]));
+    std::vector<std::vector<bool>> met(nlc, std::vector<bool>(ncls, false));
+    const size_t kSample = 1024;
     uint32_t* d_tg = nullptr;
     double* d_f64 = nullptr;
-    const size_t kSample = 1024;
     PSG_ALLOC(d_tg, kSample * 4);
     PSG_ALLOC(d_f64, kSample * 3 * sizeof(double));
     size_t maxn = 1;
     for (size_t k = 0; k < e->nsys; ++k) maxn = std::max(maxn, e->count[k]);
-    const int dsms = e->sys[0]->sms * 8;
+    const int dsms = e->fs->sms * 8;
     const size_t part_n = direct_f64_part_doubles(maxn, kSample, dsms);
     double* d_part = nullptr;
     PSG_ALLOC(d_part, part_n * sizeof(double));
     std::vector<uint32_t> tg(kSample);
     std::vector<double> f64(kSample * 3);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    PSG_CHECK(cudaEventCreate(&e0));
-    PSG_CHECK(cudaEventCreate(&e1));
-    // one tick of system k from the saved state at its current theta and
-    // leaf capacity; *ms = its device time
-    auto one_tick = [&](State* s, const DevArrays& ck, size_t n, float* ms) -> int {
-        int rr = restore();
-        if (rr != PSG_OK) return rr;
-        PSG_CHECK(cudaEventRecord(e0, s->stream));
-        launch_tick_reset_ids(ck.id, n, grid_for(s, n, 1024), s->stream);
-        int gp = (int)((n + 1023) / 1024);
-        if (gp > s->tk_grid) gp = s->tk_grid;
-        launch_prepare(ck.x, ck.y, ck.z, n, s->tk_partial, gp, ck.codes, s->tk_bbox,
-                       e->variant, s->stream);
-        rr = tick_core(s, ck, n, 0.f, 0.f, 0.f, 0.f, s->tk_bbox);
-        if (rr != PSG_OK) return rr;
-        PSG_CHECK(cudaEventRecord(e1, s->stream));
-        PSG_CHECK(cudaEventSynchronize(e1));
-        PSG_CHECK(cudaEventElapsedTime(ms, e0, e1));
-        return PSG_OK;
-    };
-    // median relative force error of that tick on kSample particles
-    auto median_error = [&](State* s, const DevArrays& ck, size_t n, double* med) -> int {
-        const size_t ns = n < kSample ? n : kSample;
-        for (size_t i = 0; i < ns; ++i) tg[i] = (uint32_t)(i * n / ns);
-        PSG_CHECK(cudaMemcpyAsync(d_tg, tg.data(), ns * 4, cudaMemcpyHostToDevice, s->stream));
-        launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, dsms, s->stream, d_part, part_n);
-        PSG_CHECK(cudaMemcpyAsync(f64.data(), d_f64, ns * 3 * sizeof(double),
-                                  cudaMemcpyDeviceToHost, s->stream));
-        std::vector<float> hf[3] = {std::vector<float>(n), std::vector<float>(n),
-                                    std::vector<float>(n)};
-        PSG_CHECK(cudaMemcpyAsync(hf[0].data(), ck.fx, n * 4, cudaMemcpyDeviceToHost, s->stream));
-        PSG_CHECK(cudaMemcpyAsync(hf[1].data(), ck.fy, n * 4, cudaMemcpyDeviceToHost, s->stream));
-        PSG_CHECK(cudaMemcpyAsync(hf[2].data(), ck.fz, n * 4, cudaMemcpyDeviceToHost, s->stream));
-        PSG_CHECK(cudaStreamSynchronize(s->stream));
-        std::vector<double> rel(ns);
-        for (size_t i = 0; i < ns; ++i) {
-            const double gx = f64[3 * i], gy = f64[3 * i + 1], gz = f64[3 * i + 2];
-            const double ex = hf[0][tg[i]] - gx, ey = hf[1][tg[i]] - gy, ez = hf[2][tg[i]] - gz;
-            const double nr = std::sqrt(gx * gx + gy * gy + gz * gz);
-            rel[i] = nr > 0 ? std::sqrt(ex * ex + ey * ey + ez * ez) / nr : 0.0;
-        }
-        std::nth_element(rel.begin(), rel.begin() + ns / 2, rel.end());
-        *med = rel[ns / 2];
-        return PSG_OK;
-    };
-    // per leaf capacity of the ladder and size class: the smallest theta
-    // meeting the target (none meets it: the largest), from the class's
-    // first system
-    const size_t nl_cap = e->leaf_ladder.size();
-    std::vector<std::vector<float>> th_cap(nl_cap, std::vector<float>(e->nsys, ladder[nl - 1]));
-    std::vector<bool> all_met(nl_cap, true);
-    for (size_t ci = 0; ci < nl_cap && r == PSG_OK; ++ci) {
-        const uint32_t cap = e->leaf_ladder[ci];
-        std::vector<bool> done(e->nsys, false);
-        for (size_t k = 0; k < e->nsys && r == PSG_OK; ++k) {
-            if (done[k]) continue;
-            State* s = e->sys[k];
-            const size_t n = e->count[k];
-            const DevArrays ck = slice(c, e->offset[k]);
-            s->leaf_cap = cap;
-            float pick = ladder[nl - 1];
-            bool met = false;
-            for (int li = 0; li < nl && r == PSG_OK; ++li) {
-                float ms = 0.f;
-                double err = 0.0;
-                s->theta = ladder[li];
-                if ((r = one_tick(s, ck, n, &ms)) != PSG_OK) break;
-                if ((r = median_error(s, ck, n, &err)) != PSG_OK) break;
-                if (err <= (double)target) {
-                    pick = ladder[li];
-                    met = true;
+    // theta per (leaf capacity, class): ticks of the class's first system alone
+    for (size_t ci = 0; ci < ncls && r == PSG_OK; ++ci) {
+        const size_t k = rep[ci], n = e->count[k];
+        State* s = new (std::nothrow) State;
+        if (!s) { r = PSG_EALLOC; break; }
+        r = init_state(s, n, 2.0f);
+        if (r == PSG_OK) r = ensure_tick_scratch(s);
+        const DevArrays ck = slice(c, e->offset[k]);
+        for (size_t li = 0; li < nlc && r == PSG_OK; ++li) {
+            s->leaf_cap = e->leaf_ladder[li];
+            for (int ti = 0; ti < nl && r == PSG_OK; ++ti) {
+                s->theta = ladder[ti];
+                reset_near_levels(s);
+                if ((r = restore()) != PSG_OK) break;
+                launch_tick_reset_ids(ck.id, n, grid_for(s, n, 1024), s->stream);
+                int gp = (int)((n + 1023) / 1024);
+                if (gp > s->tk_grid) gp = s->tk_grid;
+                launch_prepare(ck.x, ck.y, ck.z, n, s->tk_partial, gp, ck.codes, s->tk_bbox,
+                               e->variant, s->stream);
+                if ((r = tick_core(s, ck, n, 0.f, 0.f, 0.f, 0.f, s->tk_bbox)) != PSG_OK) break;
+                const size_t ns = n < kSample ? n : kSample;
+                for (size_t i = 0; i < ns; ++i) tg[i] = (uint32_t)(i * n / ns);
+                PSG_CHECK(cudaMemcpyAsync(d_tg, tg.data(), ns * 4, cudaMemcpyHostToDevice,
+                                          s->stream));
+                launch_direct_f64(s->xyzm, n, d_tg, ns, d_f64, dsms, s->stream, d_part, part_n);
+                PSG_CHECK(cudaMemcpyAsync(f64.data(), d_f64, ns * 3 * sizeof(double),
+                                          cudaMemcpyDeviceToHost, s->stream));
+                std::vector<float> hf[3] = {std::vector<float>(n), std::vector<float>(n),
+                                            std::vector<float>(n)};
+                PSG_CHECK(cudaMemcpyAsync(hf[0].data(), ck.fx, n * 4, cudaMemcpyDeviceToHost,
+                                          s->stream));
+                PSG_CHECK(cudaMemcpyAsync(hf[1].data(), ck.fy, n * 4, cudaMemcpyDeviceToHost,
+                                          s->stream));
+                PSG_CHECK(cudaMemcpyAsync(hf[2].data(), ck.fz, n * 4, cudaMemcpyDeviceToHost,
+                                          s->stream));
+                PSG_CHECK(cudaStreamSynchronize(s->stream));
+                std::vector<double> rel(ns);
+                for (size_t i = 0; i < ns; ++i) {
+                    const double gx = f64[3 * i], gy = f64[3 * i + 1], gz = f64[3 * i + 2];
+                    const double ex = hf[0][tg[i]] - gx, ey = hf[1][tg[i]] - gy,
+                                 ez = hf[2][tg[i]] - gz;
+                    const double nr = std::sqrt(gx * gx + gy * gy + gz * gz);
+                    rel[i] = nr > 0 ? std::sqrt(ex * ex + ey * ey + ez * ez) / nr : 0.0;
+                }
+                std::nth_element(rel.begin(), rel.begin() + ns / 2, rel.end());
+                if (rel[ns / 2] <= (double)target) {
+                    th[li][ci] = ladder[ti];
+                    met[li][ci] = true;
                     break;
                 }
             }
-            if (!met) all_met[ci] = false;
-            for (size_t j = 0; j < e->nsys; ++j) {
-                if (cls[j] == cls[k]) {
-                    th_cap[ci][j] = pick;
-                    done[j] = true;
-                }
-            }
         }
+        if (s->magic == kMagic) free_state(s);
+        delete s;
     }
-    // then one leaf capacity for the whole ensemble: the fastest forces replay
-    // among those whose every class met the target (none did: the first)
-    size_t best_ci = 0;
-    if (r == PSG_OK && nl_cap > 1) {
-        float* vdummy[3] = {c.fx, c.fy, c.fz};
-        double best = 1e300;
-        for (size_t ci = 0; ci < nl_cap && r == PSG_OK; ++ci) {
-            if (!all_met[ci] && all_met[best_ci]) continue;
-            for (size_t k = 0; k < e->nsys; ++k) {
-                e->sys[k]->theta = th_cap[ci][k];
-                e->sys[k]->leaf_cap = e->leaf_ladder[ci];
-            }
-            e->dirty = true;
-            float ms = 0.f;
-            for (int rep = 0; rep < 2 && r == PSG_OK; ++rep) {  // the first replay grows stores
-                if ((r = restore()) != PSG_OK) break;
-                if ((r = ensure_graphs(e, c, vdummy, 0.f)) != PSG_OK) break;
-                PSG_CHECK(cudaEventRecord(e0, e->root));
-                PSG_CHECK(cudaGraphLaunch(e->g_force, e->root));
-                PSG_CHECK(cudaEventRecord(e1, e->root));
-                PSG_CHECK(cudaStreamSynchronize(e->root));
-                if ((r = check_systems(e, c)) != PSG_OK) break;
-                cudaEventElapsedTime(&ms, e0, e1);
-            }
-            if (r != PSG_OK) break;
-            const bool eligible = all_met[ci] || !all_met[best_ci];
-            if (eligible && (ms < best || (all_met[ci] && !all_met[best_ci]))) {
-                best = ms;
-                best_ci = ci;
-            }
-        }
-        drop_graphs(e);
-    }
-    if (nl_cap > 0) {
-        for (size_t k = 0; k < e->nsys; ++k) {
-            chosen[k] = th_cap[best_ci][k];
-            chosen_cap[k] = e->leaf_ladder[best_ci];
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     cudaFree(d_tg);
     cudaFree(d_f64);
     cudaFree(d_part);
-    if (r == PSG_OK) {
-        for (size_t k = 0; k < e->nsys; ++k) {
-            e->sys[k]->theta = chosen[k];
-            e->sys[k]->leaf_cap = chosen_cap[k];
+    // one forces replay of the copies with the current settings: its time
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    PSG_CHECK(cudaEventCreate(&t0));
+    PSG_CHECK(cudaEventCreate(&t1));
+    float* vdummy[3] = {c.fx, c.fy, c.fz};
+    auto replay = [&](float* ms) -> int {
+        int rr = PSG_OK;
+        for (int rep2 = 0; rep2 < 2 && rr == PSG_OK; ++rep2) {  // the first grows stores
+            if ((rr = restore()) != PSG_OK) break;
+            if ((rr = ensure_graphs(e, c, vdummy, 0.f)) != PSG_OK) break;
+            PSG_CHECK(cudaEventRecord(t0, st));
+            PSG_CHECK(cudaGraphLaunch(e->g_force, st));
+            PSG_CHECK(cudaEventRecord(t1, st));
+            PSG_CHECK(cudaStreamSynchronize(st));
+            if ((rr = check_forest(e, c)) != PSG_OK) break;
+            cudaEventElapsedTime(ms, t0, t1);
         }
-        // launch shape: one forces replay of the copies per grid scale
-        static const double scales[] = {1.0, 0.5, 0.25};
-        float* vdummy[3] = {c.fx, c.fy, c.fz};
+        return rr;
+    };
+    auto set_class = [&](size_t ci, size_t li) {
+        for (size_t k = 0; k < e->nsys; ++k) {
+            if (cls[k] != classes[ci]) continue;
+            e->cap[k] = e->leaf_ladder[li];
+            e->theta[k] = th[li][ci];
+        }
+    };
+    // start from each class's first leaf capacity that met the target
+    std::vector<size_t> pick(ncls, 0);
+    for (size_t ci = 0; ci < ncls; ++ci)
+        for (size_t li = 0; li < nlc; ++li)
+            if (met[li][ci]) {
+                pick[ci] = li;
+                break;
+            }
+    for (size_t ci = 0; ci < ncls; ++ci) set_class(ci, pick[ci]);
+    if (r == PSG_OK) r = upload_systems(e);
+    // then class by class the fastest whole replay
+    for (size_t ci = 0; ci < ncls && r == PSG_OK && nlc > 1; ++ci) {
         double best = 1e300;
-        double best_scale = 1.0;
-        cudaEvent_t t0, t1;
-        PSG_CHECK(cudaEventCreate(&t0));
-        PSG_CHECK(cudaEventCreate(&t1));
+        size_t best_li = pick[ci];
+        for (size_t li = 0; li < nlc && r == PSG_OK; ++li) {
+            if (!met[li][ci] && met[pick[ci]][ci]) continue;
+            set_class(ci, li);
+            if ((r = upload_systems(e)) != PSG_OK) break;
+            e->dirty = true;
+            float ms = 0.f;
+            if ((r = replay(&ms)) != PSG_OK) break;
+            if (ms < best) {
+                best = ms;
+                best_li = li;
+            }
+        }
+        pick[ci] = best_li;
+        set_class(ci, best_li);
+        if (r == PSG_OK) r = upload_systems(e);
+    }
+    // launch shape: the traversal grids' scale
+    if (r == PSG_OK) {
+        static const double scales[] = {1.0, 0.5, 0.25};
+        double best = 1e300, best_scale = 1.0;
         for (double sc : scales) {
             e->grid_scale = sc;
             e->dirty = true;
-            for (int rep = 0; rep < 2 && r == PSG_OK; ++rep) {  // the first replay grows stores
-                if ((r = restore()) != PSG_OK) break;
-                if ((r = ensure_graphs(e, c, vdummy, 0.f)) != PSG_OK) break;
-                PSG_CHECK(cudaEventRecord(t0, e->root));
-                PSG_CHECK(cudaGraphLaunch(e->g_force, e->root));
-                PSG_CHECK(cudaEventRecord(t1, e->root));
-                PSG_CHECK(cudaStreamSynchronize(e->root));
-                if ((r = check_systems(e, c)) != PSG_OK) break;
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, t0, t1);
-                if (rep == 1 && ms < best) {
-                    best = ms;
-                    best_scale = sc;
-                }
+            float ms = 0.f;
+            if ((r = replay(&ms)) != PSG_OK) break;
+            if (ms < best) {
+                best = ms;
+                best_scale = sc;
             }
-            if (r != PSG_OK) break;
         }
-        cudaEventDestroy(t0);
-        cudaEventDestroy(t1);
         e->grid_scale = best_scale;
         drop_graphs(e);
         if (scale_out) *scale_out = best_scale;
         if (theta_out)
-            for (size_t k = 0; k < e->nsys; ++k) theta_out[k] = chosen[k];
+            for (size_t k = 0; k < e->nsys; ++k) theta_out[k] = e->theta[k];
     }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
     cudaFree(buf);
     return r;
 }
@@ -1679,14 +1778,14 @@ int psg_ensemble_autotune(void* h, const psg_arrays_t* a, float target, float* t
 int psg_ensemble_systems(void* h, float* theta_out, size_t n) {
     psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
     if (!e || e->magic != psg::kEnsMagic || !theta_out || n != e->nsys) return PSG_EINVAL;
-    for (size_t k = 0; k < n; ++k) theta_out[k] = e->sys[k]->theta;
+    for (size_t k = 0; k < n; ++k) theta_out[k] = e->theta[k];
     return PSG_OK;
 }
 
 int psg_ensemble_leaf_caps(void* h, uint32_t* cap_out, size_t n) {
     psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
     if (!e || e->magic != psg::kEnsMagic || !cap_out || n != e->nsys) return PSG_EINVAL;
-    for (size_t k = 0; k < n; ++k) cap_out[k] = e->sys[k]->leaf_cap;
+    for (size_t k = 0; k < n; ++k) cap_out[k] = e->cap[k];
     return PSG_OK;
 }
 
@@ -1700,9 +1799,10 @@ int psg_ensemble_set_leaf_caps(void* h, const uint32_t* caps, size_t n, int ladd
         return PSG_OK;
     }
     if (n != e->nsys) return PSG_EINVAL;
-    for (size_t k = 0; k < n; ++k) e->sys[k]->leaf_cap = caps[k];
+    PSG_CHECK(cudaSetDevice(e->device));
+    for (size_t k = 0; k < n; ++k) e->cap[k] = caps[k];
     e->dirty = true;
-    return PSG_OK;
+    return psg::upload_systems(e);
 }
 
 // ---- learned closure ----------------------------------------------------------
