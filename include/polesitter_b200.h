@@ -185,15 +185,17 @@ ps_result_t ps_b200_closure_train(ps_context_t* ctx, const float* x, const float
 
 /* ---- batched ensemble (no counterpart in the reference) ----------------
  *
- * Many independent systems advanced together: each keeps its own context,
- * and one tick of all of them is two CUDA graphs captured once and replayed
- * (forces: a branch per system -- ids reset, prepare, sort, tree, upward,
- * traversal; step: each system's velocity permutation + semi-implicit Euler,
- * as in ps_b200_run_ticks).  The systems' particles are one concatenated set
- * of DEVICE arrays: system k holds counts[k] particles from the sum of the
- * counts before it, its ids are local (0 .. counts[k]-1) and, like its
- * positions, come back sorted within its range.  Results equal running each
- * system through ps_b200_run_ticks with its own theta and leaf capacity. */
+ * Many independent systems advanced together: every phase of a tick -- ids
+ * reset, prepare, sort, tree build, upward pass, traversal, velocity
+ * permutation + semi-implicit Euler as in ps_b200_run_ticks -- is one launch
+ * over all systems (each system sorted and built within its own range, each
+ * traversal group with its own system's theta and root), and one tick is two
+ * CUDA graphs captured once and replayed.  The systems' particles are one
+ * concatenated set of DEVICE arrays: system k holds counts[k] particles from
+ * the sum of the counts before it, its ids are local (0 .. counts[k]-1) and,
+ * like its positions, come back sorted within its range.  Results equal
+ * running each system through ps_b200_run_ticks with its own theta and leaf
+ * capacity, bit for bit.  At most 65,536 systems. */
 typedef struct ps_b200_ensemble ps_b200_ensemble_t;
 
 /* theta per system (NULL: 2.0 for all) */
@@ -204,14 +206,14 @@ ps_result_t ps_b200_ensemble_create(ps_b200_ensemble_t** out, const size_t* coun
  * not changed): per leaf capacity of the ladder (default {1, 16, 32, 64})
  * and size class (systems with equal floor(log2 N)), the smallest theta of
  * {1, 1.5, 2, 3, 4, 6, 8} whose median relative force error against an FP64
- * direct sum (1024 sampled particles of the class's first system) is at
- * most target_median_error (none: 8); then one leaf capacity for all
- * systems, the one whose forces replay of the whole ensemble is fastest
- * among those where every class met the target; then the traversal grids'
- * scale among {1, 1/2, 1/4} of one system's persistent grids, by the same
- * replay time.  theta_out (n_systems) and
- * grid_scale_out receive the choice (either may be NULL);
- * ps_b200_ensemble_leaf_caps reads the leaf capacities. */
+ * direct sum (1024 sampled particles of the class's first system, ticked
+ * alone) is at most target_median_error (none: 8); then, class by class from
+ * the one holding the most particles, the leaf capacity (with its theta)
+ * whose forces replay of the whole ensemble is fastest among those that met
+ * the target; then the traversal grids' scale among {1, 1/2, 1/4}, by the
+ * same replay time.  theta_out (n_systems) and grid_scale_out receive the
+ * choice (either may be NULL); ps_b200_ensemble_leaf_caps reads the leaf
+ * capacities. */
 ps_result_t ps_b200_ensemble_autotune(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
                                       uint32_t* morton_codes, float target_median_error,
                                       float* theta_out, double* grid_scale_out);

@@ -365,10 +365,10 @@ class Context:
 
 
 class Ensemble:
-    """Many independent systems advanced together (ps_b200_ensemble_*): one
-    context per system, each tick two replayed CUDA graphs.  Arrays are
-    concatenated device arrays (torch CUDA tensors), system k at offsets
-    sum(counts[:k])."""
+    """Many independent systems advanced together (ps_b200_ensemble_*): every
+    phase of a tick is one launch over all systems, each tick two replayed
+    CUDA graphs.  Arrays are concatenated device arrays (torch CUDA tensors),
+    system k at offsets sum(counts[:k])."""
 
     def __init__(self, counts, theta=None):
         import numpy as np
