@@ -127,6 +127,7 @@ static size_t direct_splits(size_t n, size_t n_targets, int blocks, size_t part_
 }
 
 size_t direct_f64_part_doubles(size_t n, size_t n_targets, int blocks) {
+    if (n_targets == 0 || n == 0) return 1;
     size_t chunk = 0;
     return direct_splits(n, n_targets, blocks, ~(size_t)0 / 2, &chunk) * n_targets * 3;
 }

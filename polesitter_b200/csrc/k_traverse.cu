@@ -484,6 +484,10 @@ __global__ void __launch_bounds__(kTravThreads,
     const TreeView& tv = A.tv;
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN)) return;
+    // a run whose near lists ran out is void (the host grows them and runs
+    // again): the internal levels below the one that failed did not run, so
+    // their lists must not be read
+    if (MODE == MODE_LEAF && (status->err & PSG_ERR_NS_OVERFLOW)) return;
     // the variant for this tree (batched systems: each group takes its
     // system's variant, so a system sums exactly as it does alone)
     if (MODE == MODE_LEAF && !tv.part_sys && ((status->max_leaf >= kDenseSwitch) != DENSE))
@@ -709,9 +713,12 @@ __global__ void __launch_bounds__(kTravThreads,
                     tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
                     const uint32_t ex = inc - c;
                     const bool lf = (link >> 28) == 0;
+                    // a chain group's candidates are first tested against its
+                    // ancestor a_{K+1} alone (level 1, no children)
+                    const uint8_t cmk = (uint8_t)((XL && nchain) ? 0u : tgt_mask);
                     for (uint32_t i = 0; i < c; ++i) {
                         sm.cand_node[ex + i] = lf ? s0 : (link & kLinkMask) + i;
-                        sm.cand_mask[ex + i] = (uint8_t)tgt_mask;
+                        sm.cand_mask[ex + i] = cmk;
                         if constexpr (MODE == MODE_LEAF && XL)
                             sm.cand_lvl[ex + i] = nchain ? 1 : 0;
                     }
@@ -1010,13 +1017,147 @@ __global__ void __launch_bounds__(kTravThreads,
 //  * an entry that serves only some of its leaves is summed per leaf q, in
 //    another walk of the chain, with the lanes dealt over q's targets alone
 //    (T_q lanes, 32 / T_q slices),
-// so no lane computes a pair its target does not want.  Sources are read
-// straight from the sorted particles: a slice's lanes read the same
-// address, the slices read adjacent ones, two particles per step into two
-// accumulator chains.  The per-leaf sums reach the target's lane through
+// so no lane computes a pair its target does not want.  A chunk's taken
+// entries go through the warp's shared tile (sum_tiles); with 8 or more
+// slices (4 or fewer targets) the slices instead walk whole source leaves
+// from global memory (walk_leaf), as the tile's search would cost more than
+// its reuse saves.  The per-leaf sums reach the target's lane through
 // shared memory (a target belongs to one leaf, so its slot is written once).
 // Sums are taken in chain order, so the result does not depend on
 // scheduling.
+
+struct DenseTile {
+    float4 p[32];
+    uint32_t m[32];
+};
+
+// one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
+// a source counts only if its child mask holds the target's leaf q.  Plain
+// sums alternate between two accumulator sets (independent FMA chains),
+// added at the end of the tile.
+template <bool MASKED, bool KAHAN>
+__device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, uint32_t S,
+                                           uint32_t nt, uint32_t q, float4 t, float& ax,
+                                           float& ay, float& az, float& cx, float& cy, float& cz,
+                                           uint32_t& used) {
+    if constexpr (KAHAN) {
+        for (uint32_t j = j0; j < nt; j += S) {
+            const float4 p = tile.p[j];
+            float w = p.w;
+            if (MASKED) {
+                const bool on = (tile.m[j] >> q) & 1u;
+                w = on ? w : 0.f;
+                used += on ? 1u : 0u;
+            } else {
+                ++used;
+            }
+            float fx, fy, fz;
+            const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
+            const float inv = rsqrtf(r2);
+            const float f = w * (inv * inv * inv);
+            fx = __fmul_rn(dx, f);
+            fy = __fmul_rn(dy, f);
+            fz = __fmul_rn(dz, f);
+            const float yx = __fsub_rn(fx, cx);
+            const float yy = __fsub_rn(fy, cy);
+            const float yz = __fsub_rn(fz, cz);
+            const float tx = __fadd_rn(ax, yx);
+            const float ty = __fadd_rn(ay, yy);
+            const float tz = __fadd_rn(az, yz);
+            cx = __fsub_rn(__fsub_rn(tx, ax), yx);
+            cy = __fsub_rn(__fsub_rn(ty, ay), yy);
+            cz = __fsub_rn(__fsub_rn(tz, az), yz);
+            ax = tx;
+            ay = ty;
+            az = tz;
+        }
+    } else {
+        float ex = 0.f, ey = 0.f, ez = 0.f;
+        uint32_t j = j0;
+#pragma unroll 2
+        for (; j + S < nt; j += 2 * S) {
+            const float4 p0 = tile.p[j], p1 = tile.p[j + S];
+            float w0 = p0.w, w1 = p1.w;
+            if (MASKED) {
+                const bool on0 = (tile.m[j] >> q) & 1u, on1 = (tile.m[j + S] >> q) & 1u;
+                w0 = on0 ? w0 : 0.f;
+                w1 = on1 ? w1 : 0.f;
+                used += (on0 ? 1u : 0u) + (on1 ? 1u : 0u);
+            } else {
+                used += 2;
+            }
+            const float dx0 = p0.x - t.x, dy0 = p0.y - t.y, dz0 = p0.z - t.z;
+            const float dx1 = p1.x - t.x, dy1 = p1.y - t.y, dz1 = p1.z - t.z;
+            const float i0 = rsqrtf(fmaf(dx0, dx0, fmaf(dy0, dy0, fmaf(dz0, dz0, 0.1f))));
+            const float i1 = rsqrtf(fmaf(dx1, dx1, fmaf(dy1, dy1, fmaf(dz1, dz1, 0.1f))));
+            const float f0 = w0 * (i0 * i0 * i0), f1 = w1 * (i1 * i1 * i1);
+            ax = fmaf(dx0, f0, ax);
+            ay = fmaf(dy0, f0, ay);
+            az = fmaf(dz0, f0, az);
+            ex = fmaf(dx1, f1, ex);
+            ey = fmaf(dy1, f1, ey);
+            ez = fmaf(dz1, f1, ez);
+        }
+        if (j < nt) {
+            const float4 p = tile.p[j];
+            float w = p.w;
+            if (MASKED) {
+                const bool on = (tile.m[j] >> q) & 1u;
+                w = on ? w : 0.f;
+                used += on ? 1u : 0u;
+            } else {
+                ++used;
+            }
+            const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
+            const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 0.1f))));
+            const float f = w * (inv * inv * inv);
+            ax = fmaf(dx, f, ax);
+            ay = fmaf(dy, f, ay);
+            az = fmaf(dz, f, az);
+        }
+        ax += ex;
+        ay += ey;
+        az += ez;
+    }
+}
+
+
+// The particles of the chunk entries the lanes hold (entry start es, count
+// en; en = 0 for an entry not taken) against target t: laid end to end by a
+// warp prefix sum, they pass through the warp's shared tile 32 at a time --
+// lane j finds the entry of flat particle b + j by a binary search over the
+// prefix sums and stages it (coalesced within a leaf) -- and every lane runs
+// its target against the tile's particles j = slice, slice + S, ...
+// Returns the particles summed (the same on every lane).
+template <bool KAHAN>
+__device__ __forceinline__ uint32_t sum_tiles(DenseTile& tile, const float4* __restrict__ xyzm,
+                                              uint32_t es, uint32_t en, uint32_t slice,
+                                              uint32_t S, float4 t, float& ax, float& ay,
+                                              float& az, float& cx, float& cy, float& cz) {
+    const uint32_t lane = lane_id();
+    const uint32_t incl = warp_incl_scan(en);
+    const uint32_t ptot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t used = 0;
+    for (uint32_t b = 0; b < ptot; b += 32) {
+        const uint32_t f = b + lane;
+        uint32_t e = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+            const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, e + step - 1);
+            if (v <= f) e += step;
+        }
+        const uint32_t e_start = __shfl_sync(0xFFFFFFFFu, es, e);
+        const uint32_t e_excl = __shfl_sync(0xFFFFFFFFu, incl - en, e);
+        __syncwarp();
+        if (f < ptot) tile.p[lane] = xyzm[e_start + (f - e_excl)];
+        __syncwarp();
+        const uint32_t nt = min(32u, ptot - b);
+        dense_tile<false, KAHAN>(tile, slice, S, nt, 0u, t, ax, ay, az, cx, cy, cz, used);
+    }
+    __syncwarp();
+    return ptot;
+}
 
 // target t against the particles first + slice, first + slice + S, ... <
 // first + cnt (polesitter.h:1424-1444, rsqrt), optionally Kahan-compensated
@@ -1079,7 +1220,9 @@ __device__ __forceinline__ void walk_leaf(const float4* __restrict__ xyzm, uint3
 template <bool DEBUG, bool GRAD, bool KAHAN>
 __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
     __shared__ float4 s_part[kTravWarps][32];  // per-leaf sums of the record's targets
+    __shared__ DenseTile tiles[kTravWarps];
     float4* part = s_part[threadIdx.x >> 5];
+    DenseTile& tile = tiles[threadIdx.x >> 5];
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_DENSE_OVERFLOW)) return;
     const TreeView& tv = A.tv;
@@ -1126,12 +1269,19 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
                 }
             }
             partial_q |= __reduce_or_sync(0xFFFFFFFFu, em != run ? em : 0u);
-            for (uint32_t full = __ballot_sync(0xFFFFFFFFu, em == run); full; full &= full - 1) {
-                const uint32_t e = __ffs(full) - 1;
-                const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
-                const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
-                walk_leaf<KAHAN>(xyzm, s0, n0, slice, S, t, bx, by, bz, cx, cy, cz);
-                if (DEBUG) used += n0;
+            if (S >= 8u) {
+                for (uint32_t full = __ballot_sync(0xFFFFFFFFu, em == run); full;
+                     full &= full - 1) {
+                    const uint32_t e = __ffs(full) - 1;
+                    const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
+                    const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
+                    walk_leaf<KAHAN>(xyzm, s0, n0, slice, S, t, bx, by, bz, cx, cy, cz);
+                    if (DEBUG) used += n0;
+                }
+            } else {
+                const uint32_t got =
+                    sum_tiles<KAHAN>(tile, xyzm, es, en, slice, S, t, bx, by, bz, cx, cy, cz);
+                if (DEBUG) used += got;
             }
         }
         // pass 2: per leaf of the record, the entries that serve it but not
@@ -1160,12 +1310,18 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
                     es = si.x;
                     en = si.y;
                 }
-                for (uint32_t pm = __ballot_sync(0xFFFFFFFFu, mine); pm; pm &= pm - 1) {
-                    const uint32_t e = __ffs(pm) - 1;
-                    const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
-                    const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
-                    walk_leaf<KAHAN>(xyzm, s0, n0, sq, Sq, tp, px, py, pz, kx, ky, kz);
-                    if (DEBUG) usedq += n0;
+                if (Sq >= 8u) {
+                    for (uint32_t pm = __ballot_sync(0xFFFFFFFFu, mine); pm; pm &= pm - 1) {
+                        const uint32_t e = __ffs(pm) - 1;
+                        const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
+                        const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
+                        walk_leaf<KAHAN>(xyzm, s0, n0, sq, Sq, tp, px, py, pz, kx, ky, kz);
+                        if (DEBUG) usedq += n0;
+                    }
+                } else if (__any_sync(0xFFFFFFFFu, mine)) {
+                    const uint32_t got = sum_tiles<KAHAN>(tile, xyzm, es, en, sq, Sq, tp, px, py,
+                                                          pz, kx, ky, kz);
+                    if (DEBUG) usedq += got;
                 }
             }
             px -= kx;
@@ -1261,7 +1417,10 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
     __shared__ float2 s_g1;
     __shared__ unsigned long long s_cnt[kHeavyWarps][3];
     Status* status = A.status;
-    if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_HEAVY_OVERFLOW)) return;
+    // (a run whose near lists ran out is void: see k_trav)
+    if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_HEAVY_OVERFLOW |
+                       PSG_ERR_NS_OVERFLOW))
+        return;
     const TreeView& tv = A.tv;
     // work items: the leaf children of the nodes at depths 0 .. heavy_depth-1
     uint32_t cum[kMaxDepth + 1];
