@@ -1017,6 +1017,8 @@ static int upload_systems(Ensemble* e) {
     if (hmax != e->fs->forest_heavy) e->dirty = true;  // a launch parameter changes
     e->fs->forest_heavy = hmax;
     // the stores' near-list depth and P2P mode start over with the settings
+    // (both are launch parameters of the captured graphs)
+    if (e->fs->ns_levels != kMaxDepth || e->fs->stream_p2p) e->dirty = true;
     e->fs->ns_levels = kMaxDepth;
     e->fs->stream_p2p = 0;
     return PSG_OK;
