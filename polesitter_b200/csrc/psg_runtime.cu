@@ -61,6 +61,7 @@ struct Mirror {
 struct ClosureState {
     int mode;            // 0 off (the reference), 1 order-1 local, 2 order-1 + MLP
     int judge;           // run the sampled FP64 judge in mode 1 too
+    int judge_bps;       // blocks per SM of the judge's FP64 direct sum (1..8)
     float4* lg0;         // per node: field gradient xx yy zz xy
     float2* lg1;         //           xz yz
     uint32_t* leaf_of;   // per sorted particle: its leaf
@@ -368,7 +369,8 @@ static int closure_alloc(State* s) {
     PSG_ALLOC(c.packed, sizeof(MlpPacked));
     PSG_ALLOC(c.judge_tg, kJudgeSamples * 4);
     PSG_ALLOC(c.judge_f64, kJudgeSamples * 3 * sizeof(double));
-    c.judge_part_n = direct_f64_part_doubles(n, kJudgeSamples, s->sms * 2);
+    c.judge_part_n = direct_f64_part_doubles(n, kJudgeSamples, s->sms * 8);
+    if (c.judge_bps == 0) c.judge_bps = 2;
     PSG_ALLOC(c.judge_part, c.judge_part_n * sizeof(double));
     PSG_ALLOC(c.d_judge, sizeof(JudgeOut));
     PSG_CHECK(cudaMallocHost((void**)&c.h_judge, sizeof(JudgeOut)));
@@ -676,7 +678,8 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     if (judge) {
         PSG_CHECK(cudaEventRecord(cj.ev_sorted, st));
         PSG_CHECK(cudaStreamWaitEvent(cj.side, cj.ev_sorted, 0));
-        launch_judge_direct(s->xyzm, n, cj.judge_tg, smp, cj.judge_f64, cj.tick, s->sms * 2,
+        launch_judge_direct(s->xyzm, n, cj.judge_tg, smp, cj.judge_f64, cj.tick,
+                            s->sms * cj.judge_bps,
                             cj.side, cj.judge_part, cj.judge_part_n);
         PSG_CHECK(cudaEventRecord(cj.ev_judge, cj.side));
     }
@@ -1592,6 +1595,10 @@ int psg_set_option(void* mem, int key, double value) {
             return PSG_OK;
         }
         case PSG_OPT_JUDGE: s->cl.judge = value != 0.0; return PSG_OK;
+        case PSG_OPT_JUDGE_BLOCKS:
+            if (value < 1 || value > 8 || (double)(int)value != value) return PSG_EINVAL;
+            s->cl.judge_bps = (int)value;
+            return PSG_OK;
         case PSG_OPT_HEAVY_DEPTH:
             if (value > 5) return PSG_EINVAL;
             s->heavy_depth = value < 0 ? -1 : (int)value;
