@@ -47,7 +47,7 @@ size_t ps_b200_context_size(void);
                                         tile of the first pass publishes ~200 us late; the
                                         tick then returns PS_EDEVICE; 0 (default) restores
                                         the normal limit */
-#define PS_B200_OPT_JUDGE_BLOCKS 15  /* blocks per SM (1..8, default 2) of the closure judge's
+#define PS_B200_OPT_JUDGE_BLOCKS 15  /* blocks per SM (1..8, default 4) of the closure judge's
                                         FP64 direct sum, which runs beside the tree build and
                                         traversal: more take a larger share of the SMs */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);

@@ -370,7 +370,7 @@ static int closure_alloc(State* s) {
     PSG_ALLOC(c.judge_tg, kJudgeSamples * 4);
     PSG_ALLOC(c.judge_f64, kJudgeSamples * 3 * sizeof(double));
     c.judge_part_n = direct_f64_part_doubles(n, kJudgeSamples, s->sms * 8);
-    if (c.judge_bps == 0) c.judge_bps = 2;
+    if (c.judge_bps == 0) c.judge_bps = 4;
     PSG_ALLOC(c.judge_part, c.judge_part_n * sizeof(double));
     PSG_ALLOC(c.d_judge, sizeof(JudgeOut));
     PSG_CHECK(cudaMallocHost((void**)&c.h_judge, sizeof(JudgeOut)));
@@ -468,13 +468,15 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     const int lg[2] = {scaled(s->trav_grid[o][0][xl]), scaled(s->trav_grid[o][1][xl])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
+    // the shallow-leaf walk hands its multi-particle leaves' P2P to the
+    // full-leaf kernel too
+    PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     // full-leaf records: 12 blocks per SM, fewer for a small system (whose
     // records, if any, are few), so an ensemble of small systems does not
     // launch thousands of idle blocks each
     const size_t dense_blocks =
         std::min<size_t>((size_t)s->sms * 12, std::max<size_t>(4, s->trav_n / 64));
     launch_dense_p2p(A, scaled((int)dense_blocks), s->stream);
-    PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     record(s, PH_END);
     return PSG_OK;
 }
