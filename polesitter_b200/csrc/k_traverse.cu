@@ -1419,7 +1419,6 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
     __shared__ float4 s_g[2];  // multi-particle leaf: field gradient (xx yy zz xy), local field
     __shared__ float2 s_g1;
     __shared__ unsigned long long s_cnt[kHeavyWarps][3];
-    __shared__ uint32_t s_c0, s_r0;  // a multi-particle leaf's chunks and records
     Status* status = A.status;
     // (a run whose near lists ran out is void: see k_trav)
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_HEAVY_OVERFLOW |
@@ -1546,10 +1545,7 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
                                           cx, cy, cz);
                             }
                             ++n_p2p;
-                            // (a multi-particle leaf's pairs are counted where
-                            // they are summed: k_dense_p2p, unless streamed)
-                            if (!multi || A.stream)
-                                n_inter += (unsigned long long)si.y * ui.y;
+                            n_inter += (unsigned long long)si.y * ui.y;
                         }
                     }
                 }
@@ -1657,45 +1653,8 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
             }
         }
         __syncthreads();
-        if (multi && !A.stream) {
-            // the leaf's P2P + L2P go to k_dense_p2p: its source list as a
-            // chain of chunks (list order, read back to front) serving this
-            // one leaf, and records of up to 32 of its particles
-            const uint32_t q = u - fc;
-            const uint32_t nch = (np2p + kP2PChunk - 1) / kP2PChunk;
-            const uint32_t nrec = (ui.y + kDenseChunk - 1) / kDenseChunk;
-            if (tid == 0) {
-                s_c0 = nch ? atomicAdd(&status->p2p_chunks, nch) : 0u;
-                s_r0 = atomicAdd(&status->dense_count, nrec);
-            }
-            __syncthreads();
-            const uint32_t c0 = s_c0, r0 = s_r0;
-            const bool cok = (unsigned long long)c0 + nch <= A.p2p.cap_chunks;
-            if (cok) {
-                for (uint32_t e = tid; e < np2p; e += kHeavyThreads) {
-                    const size_t slot = (size_t)(c0 + e / kP2PChunk) * kP2PChunk + e % kP2PChunk;
-                    A.p2p.src[slot] = fp[e];
-                    A.p2p.mask[slot] = (uint8_t)(1u << q);
-                }
-                for (uint32_t k = tid; k < nch; k += kHeavyThreads) {
-                    A.p2p.next[c0 + k] = k ? c0 + k - 1 : kNone;
-                    A.p2p.cnt[c0 + k] = min((uint32_t)kP2PChunk, np2p - k * kP2PChunk);
-                }
-            } else if (tid == 0) {
-                set_err(status, PSG_ERR_P2P_OVERFLOW);
-            }
-            const uint32_t head = (cok && nch) ? c0 + nch - 1 : kNone;
-            for (uint32_t k = tid; k < nrec; k += kHeavyThreads) {
-                if (r0 + k < A.dense_cap)
-                    A.dense_rec[r0 + k] = make_uint4(
-                        fc, head, ui.x + k * kDenseChunk,
-                        min(kDenseChunk, ui.y - k * kDenseChunk) | ((1u << q) << 8));
-            }
-            if (tid == 0 && r0 + nrec > A.dense_cap) set_err(status, PSG_ERR_DENSE_OVERFLOW);
-            __syncthreads();
-        } else if (multi) {
-            // streamed P2P (no chunk store): P2P + L2P per particle over the
-            // listed sources, fixed-order sums
+        if (multi) {
+            // P2P + L2P per particle over the listed sources, fixed-order sums
             const float4 L = s_g[1];
             for (uint32_t k = 0; k < ui.y; ++k) {
                 const float4 tk = A.xyzm[ui.x + k];

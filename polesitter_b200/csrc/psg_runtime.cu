@@ -468,15 +468,13 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     const int lg[2] = {scaled(s->trav_grid[o][0][xl]), scaled(s->trav_grid[o][1][xl])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
-    // the shallow-leaf walk hands its multi-particle leaves' P2P to the
-    // full-leaf kernel too
-    PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     // full-leaf records: 12 blocks per SM, fewer for a small system (whose
     // records, if any, are few), so an ensemble of small systems does not
     // launch thousands of idle blocks each
     const size_t dense_blocks =
         std::min<size_t>((size_t)s->sms * 12, std::max<size_t>(4, s->trav_n / 64));
     launch_dense_p2p(A, scaled((int)dense_blocks), s->stream);
+    PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     record(s, PH_END);
     return PSG_OK;
 }
@@ -1221,6 +1219,15 @@ static int ens_create(Ensemble* e, const size_t* counts, size_t nsys, const floa
     if (r != PSG_OK) return r;
     r = ensure_tick_scratch(e->fs);
     if (r != PSG_OK) return r;
+    // the shallow-leaf walk serves the shallow groups of every system: more
+    // blocks, each frontier sized for the largest system
+    {
+        size_t maxn = 1;
+        for (size_t k = 0; k < nsys; ++k) maxn = std::max(maxn, counts[k]);
+        e->fs->heavy_slots = e->fs->sms * 2;
+        r = alloc_heavy(e->fs, (uint32_t)(maxn / 4 + 4096));
+        if (r != PSG_OK) return r;
+    }
     // per-system tables
     std::vector<uint32_t> psys(e->total), soff(nsys + 1), sblk(nsys + 1);
     std::vector<uint4> blk;
