@@ -14,12 +14,12 @@ timed step.
 the learned closure's snapshot family (an equal-mass Plummer sphere plus 32
 sub-clumps holding 30% of the mass, seeded), theta = 6.25, leaf capacity 16,
 closure mode 2: the order-1 local expansion, the shipped MLP correction and
-the per-tick FP64 judge on 4096 sampled particles.  Beside it, the plain GPU FMM (the
-reference's far field, mode 0) on the same snapshot over a range of theta
-(on the reference's tree, and on leaf capacity 16), each with its median
-relative force error: the plain method's ticks/s at
-the closure's error bound (<= 1e-3) is bounded by the fastest plain setting
-that still misses it.
+the per-tick FP64 judge on 4096 sampled particles.  Beside it, the metric
+itself: each method's ticks/s at the closure's error bound (median relative
+force error <= 1e-3 against the FP64 direct sum) on the same snapshot -- the
+plain GPU FMM (the reference's far field, mode 0) on the reference's tree and
+on larger leaves, and the order-1 expansion without the network (mode 1) --
+each at the first theta of its ladder that meets the bound.
 --workload plain: the reference's plain tick on an N = 1,048,576 Plummer
 sphere at theta = 2 (the configuration the parity tests pin).
 

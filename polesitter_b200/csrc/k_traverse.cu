@@ -1141,8 +1141,9 @@ __device__ __forceinline__ uint32_t sum_tiles(DenseTile& tile, const float4* __r
     const uint32_t lane = lane_id();
     const uint32_t incl = warp_incl_scan(en);
     const uint32_t ptot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    uint32_t used = 0;
-    for (uint32_t b = 0; b < ptot; b += 32) {
+    const uint32_t excl = incl - en;
+    // lane j's particle of the tile starting at flat index b (warp-collective)
+    auto fetch = [&](uint32_t b) -> float4 {
         const uint32_t f = b + lane;
         uint32_t e = 0;
 #pragma unroll
@@ -1151,10 +1152,17 @@ __device__ __forceinline__ uint32_t sum_tiles(DenseTile& tile, const float4* __r
             if (v <= f) e += step;
         }
         const uint32_t e_start = __shfl_sync(0xFFFFFFFFu, es, e);
-        const uint32_t e_excl = __shfl_sync(0xFFFFFFFFu, incl - en, e);
+        const uint32_t e_excl = __shfl_sync(0xFFFFFFFFu, excl, e);
+        return f < ptot ? xyzm[e_start + (f - e_excl)] : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    uint32_t used = 0;
+    float4 pcur = ptot ? fetch(0u) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t b = 0; b < ptot; b += 32) {
         __syncwarp();
-        if (f < ptot) tile.p[lane] = xyzm[e_start + (f - e_excl)];
+        tile.p[lane] = pcur;
         __syncwarp();
+        // the next tile's particle is in flight while this tile is summed
+        if (b + 32 < ptot) pcur = fetch(b + 32);
         const uint32_t nt = min(32u, ptot - b);
         dense_tile<false, KAHAN>(tile, slice, S, nt, 0u, t, ax, ay, az, cx, cy, cz, used);
     }
@@ -1220,6 +1228,24 @@ __device__ __forceinline__ void walk_leaf(const float4* __restrict__ xyzm, uint3
     }
 }
 
+// a spilled chunk as one lane sees it: the chunk's entry count and link,
+// and the lane's entry (its source leaf and child mask; slots past the count
+// hold stale values and are not used)
+struct ChunkHead {
+    uint32_t cnt, next, src, mask;
+};
+
+__device__ __forceinline__ ChunkHead load_chunk(const P2PStore& st, uint32_t c, uint32_t lane) {
+    ChunkHead h{0u, kNone, 0u, 0u};
+    if (c != kNone) {
+        h.cnt = st.cnt[c];
+        h.next = st.next[c];
+        h.src = st.src[(size_t)c * kP2PChunk + lane];
+        h.mask = st.mask[(size_t)c * kP2PChunk + lane];
+    }
+    return h;
+}
+
 template <bool DEBUG, bool GRAD, bool KAHAN>
 __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
     __shared__ float4 s_part[kTravWarps][32];  // per-leaf sums of the record's targets
@@ -1259,18 +1285,22 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         __syncwarp();
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
         uint32_t used = 0, partial_q = 0;
-        // pass 1: the entries that serve every leaf of the record
-        for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
-            const uint32_t cnt = A.p2p.cnt[c];
+        // pass 1: the entries that serve every leaf of the record; the next
+        // chunk's header and entries are loaded while a chunk is summed
+        ChunkHead h = load_chunk(A.p2p, rec.y, lane);
+        for (uint32_t c = rec.y; c != kNone;) {
+            const uint32_t cnt = h.cnt;
             uint32_t em = 0, es = 0, en = 0;
             if (lane < cnt) {
-                em = A.p2p.mask[(size_t)c * kP2PChunk + lane] & run;
+                em = h.mask & run;
                 if (em == run) {
-                    const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
+                    const uint4 si = tv.info[h.src];
                     es = si.x;
                     en = si.y;
                 }
             }
+            c = h.next;
+            h = load_chunk(A.p2p, c, lane);
             partial_q |= __reduce_or_sync(0xFFFFFFFFu, em != run ? em : 0u);
             if (S >= 8u) {
                 for (uint32_t full = __ballot_sync(0xFFFFFFFFu, em == run); full;
@@ -1303,16 +1333,19 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
             const float4 tp = xyzm[iq];
             float px = 0.f, py = 0.f, pz = 0.f, kx = 0.f, ky = 0.f, kz = 0.f;
             uint32_t usedq = 0;
-            for (uint32_t c = rec.y; c != kNone; c = A.p2p.next[c]) {
-                const uint32_t cnt = A.p2p.cnt[c];
+            ChunkHead hq = load_chunk(A.p2p, rec.y, lane);
+            for (uint32_t c = rec.y; c != kNone;) {
+                const uint32_t cnt = hq.cnt;
                 uint32_t em = 0, es = 0, en = 0;
-                if (lane < cnt) em = A.p2p.mask[(size_t)c * kP2PChunk + lane] & run;
+                if (lane < cnt) em = hq.mask & run;
                 const bool mine = em != run && ((em >> qq) & 1u);
                 if (mine) {
-                    const uint4 si = tv.info[A.p2p.src[(size_t)c * kP2PChunk + lane]];
+                    const uint4 si = tv.info[hq.src];
                     es = si.x;
                     en = si.y;
                 }
+                c = hq.next;
+                hq = load_chunk(A.p2p, c, lane);
                 if (Sq >= 8u) {
                     for (uint32_t pm = __ballot_sync(0xFFFFFFFFu, mine); pm; pm &= pm - 1) {
                         const uint32_t e = __ffs(pm) - 1;

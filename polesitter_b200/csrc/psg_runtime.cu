@@ -384,8 +384,13 @@ static int closure_alloc(State* s) {
 // Leaves at most this deep are walked block-parallel by k_heavy_leaf: a leaf
 // at depth d (half width H / 2^d of the root's H) stays unseparated from the
 // sources within about theta H / 2^(d-1), a large part of the tree once
-// 2^d <= 4 theta.
-static int heavy_depth_of(float theta) {
+// 2^d <= 4 theta.  That only costs a warp long in a large system: below
+// kHeavyMinParticles, where a walk over the whole tree is still short (and
+// shallow leaves are most leaves), the leaf pass takes every leaf.
+constexpr size_t kHeavyMinParticles = 131072;
+
+static int heavy_depth_of(float theta, size_t n) {
+    if (n < kHeavyMinParticles) return 0;
     int d = 0;
     while (d < 5 && (float)(2 << d) <= 4.0f * theta) ++d;
     return d < 2 ? 2 : d;
@@ -394,7 +399,7 @@ static int heavy_depth_of(float theta) {
 static int heavy_depth_for(const State* s) {
     if (s->tv.part_sys) return s->forest_heavy;  // many systems: the deepest of theirs
     if (s->heavy_depth >= 0) return s->heavy_depth > 5 ? 5 : s->heavy_depth;
-    return heavy_depth_of(s->theta);
+    return heavy_depth_of(s->theta, s->trav_n);
 }
 
 // Depth of the deepest nodes whose near lists this traversal stores.  The
@@ -1007,11 +1012,11 @@ static int ensure_tick_scratch(State* s) {
 static int upload_systems(Ensemble* e) {
     std::vector<float> th2(e->nsys);
     std::vector<int32_t> hv(e->nsys);
-    int hmax = 2;
+    int hmax = 0;
     for (size_t k = 0; k < e->nsys; ++k) {
         const float t = e->theta[k];
         th2[k] = t * t;
-        hv[k] = heavy_depth_of(t);
+        hv[k] = heavy_depth_of(t, e->count[k]);
         hmax = std::max(hmax, (int)hv[k]);
     }
     PSG_CHECK(cudaMemcpy(e->sys_theta2, th2.data(), e->nsys * 4, cudaMemcpyHostToDevice));
