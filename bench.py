@@ -628,11 +628,12 @@ def tick_loop(P, torch, dev):
 def ensemble_run(P, torch, dev):
     """The batched ensemble: 256 independent systems, N log-uniform in
     [1024, 262144], half uniform cubes and half Plummer spheres (a in
-    [0.5, 2]); theta per size class and the traversal grid scale from the
-    autotuner (target median force error 3e-2; leaf capacity per class from
-    {1, 16, 32, 64}); 50 ticks of semi-implicit
-    Euler, dt=1e-3, each tick two replayed CUDA graphs.  Beside it, the same
-    systems advanced one after the other through ps_b200_run_ticks."""
+    [0.5, 2]); theta and leaf capacity (from {1, 16, 32, 64}) per size class,
+    the expansion order (0 or 1) and the traversal grid scale from the
+    autotuner (target median force error 3e-2); 50 ticks of semi-implicit
+    Euler, dt=1e-3, each tick two replayed CUDA graphs of one launch per phase
+    over all systems.  Beside it, the same systems advanced one after the
+    other through ps_b200_run_ticks."""
     from polesitter_b200 import workloads as W
     nsys, ticks, target = 256, 50, 3e-2
     counts, p, vx, vy, vz = W.ensemble(nsys, 2026)
@@ -649,6 +650,7 @@ def ensemble_run(P, torch, dev):
     with P.Ensemble(counts) as ens:
         theta, scale = ens.autotune(a, codes, target)
         caps = ens.leaf_caps()
+        order = ens.order()
         ens.run(a, codes, *v, 1e-3, 2)  # warm-up: captures the graphs, grows stores
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -669,6 +671,8 @@ def ensemble_run(P, torch, dev):
             setattr(s, key, getattr(a, key)[lo:hi].clone())
         with P.Context(hi - lo, theta=float(theta[k])) as ectx:
             ectx.set_option(P.OPT_LEAF_CAP, int(caps[k]))
+            if order:
+                ectx.set_closure(order)
             s.id.copy_(torch.arange(hi - lo, dtype=torch.int32, device=dev))
             ectx.tick(s, codes[lo:hi])
             e = median_rel_error(ectx, s, hi - lo, 19 + c)
@@ -679,6 +683,8 @@ def ensemble_run(P, torch, dev):
     ctxs = [P.Context(int(counts[k]), theta=float(theta[k])) for k in range(nsys)]
     for k in range(nsys):
         ctxs[k].set_option(P.OPT_LEAF_CAP, int(caps[k]))
+        if order:
+            ctxs[k].set_closure(order)
 
     def one_pass():
         for k in range(nsys):
@@ -707,7 +713,8 @@ def ensemble_run(P, torch, dev):
                           "theta_per_class": {str(float(t)): int(c) for t, c in zip(vals, cnts)},
                           "leaf_cap_per_class": {str(int(t)): int(c)
                                                  for t, c in zip(cvals, ccnts)},
-                          "grid_scale": scale},
+                          "grid_scale": scale,
+                          "expansion_order": order},
             "accuracy_per_size_class": per_class,
             "one_system_at_a_time_ticks_per_s": seq,
             "speedup_over_one_at_a_time": (ticks / dt) / seq}

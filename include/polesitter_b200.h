@@ -206,15 +206,17 @@ ps_result_t ps_b200_ensemble_create(ps_b200_ensemble_t** out, const size_t* coun
                                     size_t n_systems, const float* theta);
 
 /* The autotuner, on copies of the given state (arrs and the codes array are
- * not changed): per leaf capacity of the ladder (default {1, 16, 32, 64})
+ * not changed): per expansion order it may try (ps_b200_ensemble_set_order;
+ * default both), per leaf capacity of the ladder (default {1, 16, 32, 64})
  * and size class (systems with equal floor(log2 N)), the smallest theta of
  * {1, 1.5, 2, 3, 4, 6, 8} whose median relative force error against an FP64
  * direct sum (1024 sampled particles of the class's first system, ticked
  * alone) is at most target_median_error (none: 8); then, class by class from
  * the one holding the most particles, the leaf capacity (with its theta)
  * whose forces replay of the whole ensemble is fastest among those that met
- * the target; then the traversal grids' scale among {1, 1/2, 1/4}, by the
- * same replay time.  theta_out (n_systems) and grid_scale_out receive the
+ * the target, and the order whose result replays fastest; then the
+ * traversal grids' scale among {1, 1/2, 1/4}, by the same replay time.
+ * theta_out (n_systems) and grid_scale_out receive the
  * choice (either may be NULL); ps_b200_ensemble_leaf_caps reads the leaf
  * capacities. */
 ps_result_t ps_b200_ensemble_autotune(ps_b200_ensemble_t* ens, const ps_particle_arrs_t* arrs,
@@ -233,6 +235,12 @@ ps_result_t ps_b200_ensemble_set_leaf_caps(ps_b200_ensemble_t* ens, const uint32
 /* the leaf capacities the autotuner tries (each 1..256) */
 ps_result_t ps_b200_ensemble_set_leaf_ladder(ps_b200_ensemble_t* ens, const uint32_t* caps,
                                              size_t n);
+/* local expansion of all systems: 0 the reference's (default), 1 the order-1
+ * expansion of the closure's mode 1 (PS_B200_OPT_CLOSURE); a negative order
+ * lets ps_b200_ensemble_autotune try both and keep the faster at its target
+ * error, which ps_b200_ensemble_order then reads back */
+ps_result_t ps_b200_ensemble_set_order(ps_b200_ensemble_t* ens, int order);
+ps_result_t ps_b200_ensemble_order(ps_b200_ensemble_t* ens, int* order_out);
 ps_result_t ps_b200_ensemble_destroy(ps_b200_ensemble_t* ens);
 
 /* message of the last CUDA-side failure on this thread */

@@ -42,7 +42,8 @@ EXPORTED = ("ps_init", "ps_prepare_particles", "ps_calc_forces", "ps_destroy",
             "ps_b200_closure_train", "ps_b200_ensemble_create", "ps_b200_ensemble_autotune",
             "ps_b200_ensemble_run", "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy",
             "ps_b200_ensemble_leaf_caps", "ps_b200_ensemble_set_leaf_caps",
-            "ps_b200_ensemble_set_leaf_ladder")
+            "ps_b200_ensemble_set_leaf_ladder", "ps_b200_ensemble_set_order",
+            "ps_b200_ensemble_order")
 
 
 class ParticleArrs(C.Structure):
@@ -130,10 +131,13 @@ def lib() -> C.CDLL:
     L.ps_b200_ensemble_leaf_caps.argtypes = [vp, vp, sz]
     L.ps_b200_ensemble_set_leaf_caps.argtypes = [vp, vp, sz]
     L.ps_b200_ensemble_set_leaf_ladder.argtypes = [vp, vp, sz]
+    L.ps_b200_ensemble_set_order.argtypes = [vp, C.c_int]
+    L.ps_b200_ensemble_order.argtypes = [vp, vp]
     for name in ("ps_b200_ensemble_create", "ps_b200_ensemble_autotune", "ps_b200_ensemble_run",
                  "ps_b200_ensemble_theta", "ps_b200_ensemble_destroy",
                  "ps_b200_ensemble_leaf_caps", "ps_b200_ensemble_set_leaf_caps",
-                 "ps_b200_ensemble_set_leaf_ladder"):
+                 "ps_b200_ensemble_set_leaf_ladder", "ps_b200_ensemble_set_order",
+                 "ps_b200_ensemble_order"):
         getattr(L, name).restype = C.c_int
     L.ps_b200_run_ticks.restype = C.c_int
     L.ps_b200_run_ticks.argtypes = [vp, C.POINTER(ParticleArrs), vp, vp, vp, vp, f32, C.c_uint32]
@@ -420,6 +424,16 @@ class Ensemble:
         c = np.ascontiguousarray(caps, np.uint32)
         _check("ps_b200_ensemble_set_leaf_ladder", lib().ps_b200_ensemble_set_leaf_ladder(
             self.ptr, c.ctypes.data, len(c)))
+
+    def set_order(self, order: int):
+        """Local expansion of all systems: 0 (the reference's), 1 (order-1), or
+        -1 to let ``autotune`` try both."""
+        _check("ps_b200_ensemble_set_order", lib().ps_b200_ensemble_set_order(self.ptr, order))
+
+    def order(self) -> int:
+        o = C.c_int()
+        _check("ps_b200_ensemble_order", lib().ps_b200_ensemble_order(self.ptr, C.byref(o)))
+        return o.value
 
     def destroy(self):
         if self.ptr:

@@ -106,6 +106,9 @@ int psg_ensemble_systems(void* ens, float* theta_out, size_t n);
 int psg_ensemble_leaf_caps(void* ens, uint32_t* cap_out, size_t n);
 /* ladder != 0: the leaf capacities the autotuner tries; else one per system */
 int psg_ensemble_set_leaf_caps(void* ens, const uint32_t* caps, size_t n, int ladder);
+/* local expansion order of all systems (0 or 1; < 0: the autotuner tries both) */
+int psg_ensemble_set_order(void* ens, int order);
+int psg_ensemble_order(void* ens, int* out);
 const char* psg_last_error(void);
 void psg_set_error(const char* msg);
 

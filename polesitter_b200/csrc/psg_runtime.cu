@@ -988,6 +988,8 @@ struct Ensemble {
     double grid_scale = 1.0;
     int variant = PSG_MORTON_AVX2;
     std::vector<uint32_t> leaf_ladder{1u, 16u, 32u, 64u};  // leaf capacities the autotuner tries
+    int order = 0;                     // local expansion: 0 the reference's, 1 order-1
+    std::vector<int> order_ladder{0, 1};  // expansion orders the autotuner tries
 };
 
 static DevArrays slice(const DevArrays& a, size_t off) {
@@ -1004,6 +1006,19 @@ static int ensure_tick_scratch(State* s) {
     PSG_ALLOC(s->tk_bbox, 4 * sizeof(float));
     for (int c = 0; c < 3; ++c) PSG_ALLOC(s->tk_v[c], s->max_particles * 4);
     for (int c = 0; c < 3; ++c) PSG_ALLOC(s->tk_vmir[c], s->max_particles * 4);
+    return PSG_OK;
+}
+
+// the local expansion of a state's traversal: 0 the reference's order 0,
+// 1 the order-1 expansion (closure mode 1: its field gradients per node)
+static int set_order(State* s, int order) {
+    if (order >= 1) {
+        const int r = closure_alloc(s);
+        if (r != PSG_OK) return r;
+    }
+    s->cl.mode = order >= 1 ? 1 : 0;
+    s->order = order >= 1 ? 1 : 0;
+    reset_near_levels(s);
     return PSG_OK;
 }
 
@@ -1382,8 +1397,11 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
         rep = r2;
     }
     const size_t ncls = classes.size(), nlc = e->leaf_ladder.size();
-    std::vector<std::vector<float>> th(nlc, std::vector<float>(ncls, ladder[nl - 1]));
-    std::vector<std::vector<bool>> met(nlc, std::vector<bool>(ncls, false));
+    const size_t nor = e->order_ladder.size();
+    std::vector<std::vector<std::vector<float>>> thx(
+        nor, std::vector<std::vector<float>>(nlc, std::vector<float>(ncls, ladder[nl - 1])));
+    std::vector<std::vector<std::vector<bool>>> metx(
+        nor, std::vector<std::vector<bool>>(nlc, std::vector<bool>(ncls, false)));
     const size_t kSample = 1024;
     uint32_t* d_tg = nullptr;
     double* d_f64 = nullptr;
@@ -1405,7 +1423,11 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
         r = init_state(s, n, 2.0f);
         if (r == PSG_OK) r = ensure_tick_scratch(s);
         const DevArrays ck = slice(c, e->offset[k]);
+        for (size_t oi = 0; oi < nor && r == PSG_OK; ++oi)
         for (size_t li = 0; li < nlc && r == PSG_OK; ++li) {
+            if ((r = set_order(s, e->order_ladder[oi])) != PSG_OK) break;
+            auto& th = thx[oi];
+            auto& met = metx[oi];
             s->leaf_cap = e->leaf_ladder[li];
             for (int ti = 0; ti < nl && r == PSG_OK; ++ti) {
                 s->theta = ladder[ti];
@@ -1474,42 +1496,64 @@ static int ens_autotune(Ensemble* e, const psg_arrays_t* a, float target, float*
         }
         return rr;
     };
+    // per expansion order: the class-by-class descent below, then the order
+    // whose final replay is fastest
+    size_t oi = 0;
     auto set_class = [&](size_t ci, size_t li) {
         for (size_t k = 0; k < e->nsys; ++k) {
             if (cls[k] != classes[ci]) continue;
             e->cap[k] = e->leaf_ladder[li];
-            e->theta[k] = th[li][ci];
+            e->theta[k] = thx[oi][li][ci];
         }
     };
-    // start from each class's first leaf capacity that met the target
-    std::vector<size_t> pick(ncls, 0);
-    for (size_t ci = 0; ci < ncls; ++ci)
-        for (size_t li = 0; li < nlc; ++li)
-            if (met[li][ci]) {
-                pick[ci] = li;
-                break;
-            }
-    for (size_t ci = 0; ci < ncls; ++ci) set_class(ci, pick[ci]);
-    if (r == PSG_OK) r = upload_systems(e);
-    // then class by class the fastest whole replay
-    for (size_t ci = 0; ci < ncls && r == PSG_OK && nlc > 1; ++ci) {
+    std::vector<std::vector<size_t>> picks(nor, std::vector<size_t>(ncls, 0));
+    std::vector<double> order_ms(nor, 1e300);
+    for (oi = 0; oi < nor && r == PSG_OK; ++oi) {
+        const auto& met = metx[oi];
+        auto& pick = picks[oi];
+        e->order = e->order_ladder[oi];
+        if ((r = set_order(e->fs, e->order)) != PSG_OK) break;
+        e->dirty = true;
+        // start from each class's first leaf capacity that met the target
+        for (size_t ci = 0; ci < ncls; ++ci)
+            for (size_t li = 0; li < nlc; ++li)
+                if (met[li][ci]) {
+                    pick[ci] = li;
+                    break;
+                }
+        for (size_t ci = 0; ci < ncls; ++ci) set_class(ci, pick[ci]);
+        if ((r = upload_systems(e)) != PSG_OK) break;
+        // then class by class the fastest whole replay
         double best = 1e300;
-        size_t best_li = pick[ci];
-        for (size_t li = 0; li < nlc && r == PSG_OK; ++li) {
-            if (!met[li][ci] && met[pick[ci]][ci]) continue;
-            set_class(ci, li);
-            if ((r = upload_systems(e)) != PSG_OK) break;
-            e->dirty = true;
-            float ms = 0.f;
-            if ((r = replay(&ms)) != PSG_OK) break;
-            if (ms < best) {
-                best = ms;
-                best_li = li;
+        for (size_t ci = 0; ci < ncls && r == PSG_OK; ++ci) {
+            best = 1e300;
+            size_t best_li = pick[ci];
+            for (size_t li = 0; li < nlc && r == PSG_OK; ++li) {
+                if (nlc > 1 && !met[li][ci] && met[pick[ci]][ci]) continue;
+                if (nlc == 1 && li != pick[ci]) continue;
+                set_class(ci, li);
+                if ((r = upload_systems(e)) != PSG_OK) break;
+                e->dirty = true;
+                float ms = 0.f;
+                if ((r = replay(&ms)) != PSG_OK) break;
+                if (ms < best) {
+                    best = ms;
+                    best_li = li;
+                }
             }
+            pick[ci] = best_li;
+            set_class(ci, best_li);
+            if (r == PSG_OK) r = upload_systems(e);
         }
-        pick[ci] = best_li;
-        set_class(ci, best_li);
+        order_ms[oi] = best;
+    }
+    if (r == PSG_OK) {
+        oi = (size_t)(std::min_element(order_ms.begin(), order_ms.end()) - order_ms.begin());
+        e->order = e->order_ladder[oi];
+        r = set_order(e->fs, e->order);
+        for (size_t ci = 0; ci < ncls; ++ci) set_class(ci, picks[oi][ci]);
         if (r == PSG_OK) r = upload_systems(e);
+        e->dirty = true;
     }
     // launch shape: the traversal grids' scale
     if (r == PSG_OK) {
@@ -1826,6 +1870,28 @@ int psg_ensemble_set_leaf_caps(void* h, const uint32_t* caps, size_t n, int ladd
     for (size_t k = 0; k < n; ++k) e->cap[k] = caps[k];
     e->dirty = true;
     return psg::upload_systems(e);
+}
+
+int psg_ensemble_set_order(void* h, int order) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || order > 1) return PSG_EINVAL;
+    PSG_CHECK(cudaSetDevice(e->device));
+    if (order < 0) {
+        e->order_ladder = {0, 1};
+        return PSG_OK;
+    }
+    e->order_ladder = {order};
+    e->order = order;
+    e->dirty = true;
+    const int r = psg::set_order(e->fs, order);
+    return r == PSG_OK ? psg::upload_systems(e) : r;
+}
+
+int psg_ensemble_order(void* h, int* out) {
+    psg::Ensemble* e = static_cast<psg::Ensemble*>(h);
+    if (!e || e->magic != psg::kEnsMagic || !out) return PSG_EINVAL;
+    *out = e->order;
+    return PSG_OK;
 }
 
 // ---- learned closure ----------------------------------------------------------

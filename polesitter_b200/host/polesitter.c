@@ -353,6 +353,20 @@ ps_result_t ps_b200_ensemble_set_leaf_ladder(ps_b200_ensemble_t* ens, const uint
     return to_ps(psg_ensemble_set_leaf_caps(ens, caps, n, 1));
 }
 
+ps_result_t ps_b200_ensemble_set_order(ps_b200_ensemble_t* ens, int order) {
+    if (!ens) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_set_order(ens, order));
+}
+
+ps_result_t ps_b200_ensemble_order(ps_b200_ensemble_t* ens, int* order_out) {
+    if (!ens || !order_out) {
+        return PS_EINVAL;
+    }
+    return to_ps(psg_ensemble_order(ens, order_out));
+}
+
 ps_result_t ps_b200_ensemble_destroy(ps_b200_ensemble_t* ens) {
     if (!ens) {
         return PS_EINVAL;

@@ -1,9 +1,10 @@
 """The batched ensemble (ps_b200_ensemble_*), through the C ABI.
 
-Many independent systems advanced together in replayed CUDA graphs must give
-exactly what each system gives on its own: the same sorted positions, ids,
-forces and velocities as ps_b200_run_ticks per system with the same theta
-and leaf capacity, bit for bit.  The autotuner must leave the state
+Many independent systems advanced together (every phase one launch over all
+systems, replayed CUDA graphs) must give exactly what each system gives on
+its own: the same sorted positions, ids, forces and velocities as
+ps_b200_run_ticks per system with the same theta, leaf capacity and
+expansion order, bit for bit.  The autotuner must leave the state
 untouched and choose, per size class, a theta and leaf capacity whose error
 meets its target."""
 
@@ -38,9 +39,10 @@ def _part(p, a, b):
     return q
 
 
-@pytest.mark.parametrize("caps", [None, [1, 16, 32, 1, 64, 8, 2, 16, 16]],
-                         ids=["leaf1", "mixed_leaf_caps"])
-def test_ensemble_equals_each_system_alone(caps):
+@pytest.mark.parametrize("caps,order", [(None, 0), ([1, 16, 32, 1, 64, 8, 2, 16, 16], 0),
+                                        ([1, 16, 32, 1, 64, 8, 2, 16, 16], 1)],
+                         ids=["leaf1", "mixed_leaf_caps", "mixed_leaf_caps_order1"])
+def test_ensemble_equals_each_system_alone(caps, order):
     torch = pytest.importorskip("torch")
     counts, p, vx, vy, vz = W.ensemble(7, 3, n_min=64, n_max=40000)
     counts = np.concatenate([counts, [1, 2]])  # tiny systems too
@@ -58,6 +60,8 @@ def test_ensemble_equals_each_system_alone(caps):
         if caps is not None:
             ens.set_leaf_caps(caps)
             assert np.array_equal(ens.leaf_caps(), caps)
+        ens.set_order(order)
+        assert ens.order() == order
         ens.run(d, codes, *v, 1e-3, 3)
     torch.cuda.synchronize()
     for k in range(len(counts)):
@@ -67,6 +71,8 @@ def test_ensemble_equals_each_system_alone(caps):
         with P.Context(int(b - a), theta=float(theta[k])) as ctx:
             if caps is not None:
                 ctx.set_option(P.OPT_LEAF_CAP, caps[k])
+            if order:
+                ctx.set_closure(order)
             ctx.run_ticks(q, np.zeros(b - a, np.uint32), *vk, 1e-3, 3)
         for key in KEYS:
             assert np.array_equal(getattr(d, key)[a:b].cpu().numpy(), getattr(q, key)), (k, key)
@@ -85,6 +91,8 @@ def test_autotune_meets_target_and_leaves_state():
     with P.Ensemble(counts) as ens:
         theta, scale = ens.autotune(d, codes, target)
         caps = ens.leaf_caps()
+        order = ens.order()
+        assert order in (0, 1)
         assert set(caps.tolist()) <= {1, 16, 32, 64}
         assert np.array_equal(ens.theta(), theta)
         for k, v in before.items():
@@ -101,6 +109,8 @@ def test_autotune_meets_target_and_leaves_state():
         q = _part(p, a, b)
         with P.Context(int(b - a), theta=float(theta[k])) as ctx:
             ctx.set_option(P.OPT_LEAF_CAP, int(caps[k]))
+            if order:
+                ctx.set_closure(order)
             ctx.tick(q, np.zeros(b - a, np.uint32))
             tg = np.arange(0, b - a, max(1, (b - a) // 512), dtype=np.uint32)
             f64 = ctx.direct_f64(q, tg)
