@@ -62,6 +62,7 @@ constexpr uint32_t kNsPool = 4096;        // near-list entries a warp reserves a
 constexpr uint32_t kChunkPool = 16;       // P2P spill chunks a warp reserves at once
 constexpr uint32_t kDenseChunk = 32;      // target particles per dense work record
 constexpr uint32_t kDenseSwitch = 32;     // fullest leaf from which the DENSE leaf pass runs
+constexpr uint32_t kDenseCap = 8;         // ... or leaf capacity (leaves of many particles)
 
 enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
@@ -464,7 +465,8 @@ __device__ __forceinline__ void leaf_epilogue(SmemLeaf& sm, const LeafOut o, uin
 }
 
 // DENSE (leaf pass only): the variant for trees whose fullest leaf holds at
-// least kDenseSwitch particles, which hands full leaves to k_dense_p2p.  Both
+// least kDenseSwitch particles or whose leaf capacity is kDenseCap or more,
+// which hands full leaves to k_dense_p2p.  Both
 // variants are launched; each returns at once unless the tree is its kind.
 // XL (leaf pass only): the variant that also serves chain groups and
 // streamed P2P, launched only when the near lists stop short of the deepest
@@ -489,7 +491,8 @@ __global__ void __launch_bounds__(
     if (MODE == MODE_LEAF && (status->err & PSG_ERR_NS_OVERFLOW)) return;
     // the variant for this tree (batched systems: each group takes its
     // system's variant, so a system sums exactly as it does alone)
-    if (MODE == MODE_LEAF && !tv.part_sys && ((status->max_leaf >= kDenseSwitch) != DENSE))
+    if (MODE == MODE_LEAF && !tv.part_sys &&
+        ((status->max_leaf >= kDenseSwitch || A.leaf_cap >= kDenseCap) != DENSE))
         return;
     // a shallower level's near lists did not fit: this level's are void
     if (MODE == MODE_INTERNAL && (status->ns_fail & ((1u << A.level) - 1u))) return;
@@ -569,8 +572,10 @@ __global__ void __launch_bounds__(
             if (tv.part_sys) {
                 gsys = tv.part_sys[tv.info[pid].x];
                 th2 = tv.sys_theta2[gsys];
-                if (MODE == MODE_LEAF && ((int)dp < tv.sys_heavy[gsys] ||
-                                          ((tv.sys_maxleaf[gsys] >= kDenseSwitch) != DENSE)))
+                if (MODE == MODE_LEAF &&
+                    ((int)dp < tv.sys_heavy[gsys] ||
+                     ((tv.sys_maxleaf[gsys] >= kDenseSwitch || tv.sys_cap[gsys] >= kDenseCap) !=
+                      DENSE)))
                     continue;
             }
             uint32_t cl = 0;

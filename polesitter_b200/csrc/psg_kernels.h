@@ -162,5 +162,6 @@ struct TravArgs {
     int ns_levels;      // near lists exist for nodes of depth <= ns_levels; deeper
                         // groups walk their ancestor chain (k_traverse.cu)
     int stream;         // 1: P2P summed in the leaf pass as sources are found, no spill
+    uint32_t leaf_cap;  // the tree's leaf capacity (one system)
 };
 }  // namespace psg

@@ -451,6 +451,7 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     A.heavy_frontier = s->heavy_frontier;
     A.heavy_fcap = s->heavy_fcap;
     A.ns_levels = near_levels(s);
+    A.leaf_cap = s->leaf_cap;
     A.stream = (s->stream_p2p || s->force_stream) ? 1 : 0;
     const double gs = s->grid_scale > 0.0 ? s->grid_scale : 1.0;
     auto scaled = [&](int g) {
