@@ -14,7 +14,7 @@ timed step.
 the learned closure's snapshot family (an equal-mass Plummer sphere plus 32
 sub-clumps holding 30% of the mass, seeded), theta = 6.25, leaf capacity 16,
 closure mode 2: the order-1 local expansion, the shipped MLP correction and
-the per-tick FP64 judge on 4096 sampled particles.  Beside it, the metric
+the per-tick FP64 judge on 1024 sampled particles.  Beside it, the metric
 itself: each method's ticks/s at the closure's error bound (median relative
 force error <= 1e-3 against the FP64 direct sum) on the same snapshot -- the
 plain GPU FMM (the reference's far field, mode 0) on the reference's tree and
@@ -80,7 +80,7 @@ MODE1_LADDERS = ((16, (8.0, 9.0, 10.0, 11.0, 12.0)),
 C2_THETA, C2_SEED = 2.0, 42
 WORKLOADS = {
     "closure": ("learned-closure FMM tick (ps_prepare_particles + ps_calc_forces, closure mode 2: "
-                "order-1 local expansion + BF16 MLP correction + FP64 judge on 4096 particles), "
+                "order-1 local expansion + BF16 MLP correction + FP64 judge on 1024 particles), "
                 "N=1,048,576 clumpy Plummer (a=1, r<=10a, plus 32 sub-clumps with 30% of the mass, "
                 "equal mass 1/N), theta=6.25, leaf capacity 16, float32 SoA"),
     "plain": ("plain FMM tick (ps_prepare_particles + ps_calc_forces), Plummer sphere "
@@ -377,7 +377,7 @@ def run_b200(args):
     if closure:
         med = [j["median_mlp"] if j["used"] else j["median_base"] for j in judge]
         accuracy["judge"] = {
-            "per_tick": "the tick's own FP64 judge (4096 particles, a new sample every tick)",
+            "per_tick": "the tick's own FP64 judge (1024 particles, a new sample every tick)",
             "median_of_tick_medians": float(statistics.median(med)),
             "max_of_tick_medians": float(max(med)),
             "median_without_correction": float(statistics.median(j["median_base"] for j in judge)),

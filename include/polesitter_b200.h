@@ -50,6 +50,10 @@ size_t ps_b200_context_size(void);
 #define PS_B200_OPT_JUDGE_BLOCKS 15  /* blocks per SM (1..8, default 4) of the closure judge's
                                         FP64 direct sum, which runs beside the tree build and
                                         traversal: more take a larger share of the SMs */
+#define PS_B200_OPT_JUDGE_SAMPLES 16 /* particles in the closure judge's sample (64..4096,
+                                        default 1024).  Its FP64 direct sum costs samples x N
+                                        pair terms a tick; the median it decides on has a
+                                        relative standard error of ~1/sqrt(samples) */
 ps_result_t ps_b200_set_option(ps_context_t* ctx, int key, double value);
 
 /* Morton quantisation of ps_prepare_particles, process-wide (it takes no
@@ -147,9 +151,10 @@ ps_result_t ps_b200_run_ticks(ps_context_t* ctx, const ps_particle_arrs_t* arrs,
  *      GELU, BF16 weights, FP32 accumulation, on the tensor cores) maps each
  *      particle's leaf field, field gradient, offset in the leaf and leaf
  *      depth to a force correction.  Each tick an FP64 direct sum on a
- *      sample of 4096 particles judges it: the correction is applied only
- *      when it lowers the sample's median relative error, else the mode-1
- *      forces stand.  Needs weights (ps_b200_closure_set_weights).
+ *      sample of particles (a new one every tick; 1024 particles unless
+ *      PS_B200_OPT_JUDGE_SAMPLES says otherwise) judges it: the correction
+ *      is applied only when it lowers the sample's median relative error,
+ *      else the mode-1 forces stand.  Needs weights (ps_b200_closure_set_weights).
  * The parameter vector is PS_B200_CLOSURE_PARAMS floats:
  *   W1[16][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64][8] b4[8]
  * (W[in][out]; inputs 13..15 and outputs 3..7 are padding). */

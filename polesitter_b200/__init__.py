@@ -28,7 +28,7 @@ OPT_DEBUG, OPT_THETA, OPT_TIMING, OPT_KAHAN, OPT_CLOSURE, OPT_JUDGE = 1, 2, 4, 6
 OPT_HEAVY_DEPTH = 9
 OPT_LEAF_CAP = 10
 OPT_NEAR_LEVELS, OPT_STREAM, OPT_SHRINK_STORES, OPT_SORT_SPIN = 11, 12, 13, 14
-OPT_JUDGE_BLOCKS = 15
+OPT_JUDGE_BLOCKS, OPT_JUDGE_SAMPLES = 15, 16
 CLOSURE_PARAMS = 9928
 MORTON_AVX2, MORTON_NEON, MORTON_SCALAR = 0, 1, 2
 

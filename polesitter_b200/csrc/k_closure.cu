@@ -289,7 +289,10 @@ __global__ void __launch_bounds__(1024) k_judge_decide(const uint32_t* tg, int s
                                                        const float4* dF, int allow,
                                                        JudgeOut* out) {
     __shared__ float e0[kJudgeSamples], e1[kJudgeSamples];
-    for (int k = threadIdx.x; k < kJudgeSamples; k += blockDim.x) {
+    // the sort runs over the smallest power of two >= s, padded with FLT_MAX
+    int s2 = 2;
+    while (s2 < s && s2 < kJudgeSamples) s2 <<= 1;
+    for (int k = threadIdx.x; k < s2; k += blockDim.x) {
         float a = FLT_MAX, b = FLT_MAX;
         if (k < s) {
             const uint32_t i = tg[k];
@@ -307,9 +310,9 @@ __global__ void __launch_bounds__(1024) k_judge_decide(const uint32_t* tg, int s
     }
     __syncthreads();
     // bitonic sort, ascending, both arrays
-    for (int size = 2; size <= kJudgeSamples; size <<= 1) {
+    for (int size = 2; size <= s2; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < kJudgeSamples; i += blockDim.x) {
+            for (int i = threadIdx.x; i < s2; i += blockDim.x) {
                 const int j = i ^ stride;
                 if (j > i) {
                     const bool up = (i & size) == 0;

@@ -1034,109 +1034,88 @@ __global__ void __launch_bounds__(
 // Sums are taken in chain order, so the result does not depend on
 // scheduling.
 
+// A tile of 32 source particles, pair-packed: pair m holds particles 2m and
+// 2m + 1 as a = {x, x', y, y'} and b = {z, z', w, w'}, so one 128-bit
+// shared load gives two sources' coordinates as the float2 operands of
+// sm_100's paired FP32 instructions (__fadd2_rn, __ffma2_rn, __fmul2_rn):
+// one issued instruction does a step of two pairs.
 struct DenseTile {
-    float4 p[32];
-    uint32_t m[32];
+    float4 a[16];
+    float4 b[16];
 };
 
-// one target against the tile's sources j = j0, j0 + S, ... < nt; MASKED:
-// a source counts only if its child mask holds the target's leaf q.  Plain
-// sums alternate between two accumulator sets (independent FMA chains),
-// added at the end of the tile.
-template <bool MASKED, bool KAHAN>
-__device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t j0, uint32_t S,
-                                           uint32_t nt, uint32_t q, float4 t, float& ax,
-                                           float& ay, float& az, float& cx, float& cy, float& cz,
-                                           uint32_t& used) {
-    if constexpr (KAHAN) {
-        for (uint32_t j = j0; j < nt; j += S) {
-            const float4 p = tile.p[j];
-            float w = p.w;
-            if (MASKED) {
-                const bool on = (tile.m[j] >> q) & 1u;
-                w = on ? w : 0.f;
-                used += on ? 1u : 0u;
-            } else {
-                ++used;
-            }
-            float fx, fy, fz;
-            const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
-            const float inv = rsqrtf(r2);
-            const float f = w * (inv * inv * inv);
-            fx = __fmul_rn(dx, f);
-            fy = __fmul_rn(dy, f);
-            fz = __fmul_rn(dz, f);
-            const float yx = __fsub_rn(fx, cx);
-            const float yy = __fsub_rn(fy, cy);
-            const float yz = __fsub_rn(fz, cz);
-            const float tx = __fadd_rn(ax, yx);
-            const float ty = __fadd_rn(ay, yy);
-            const float tz = __fadd_rn(az, yz);
-            cx = __fsub_rn(__fsub_rn(tx, ax), yx);
-            cy = __fsub_rn(__fsub_rn(ty, ay), yy);
-            cz = __fsub_rn(__fsub_rn(tz, az), yz);
-            ax = tx;
-            ay = ty;
-            az = tz;
-        }
-    } else {
-        float ex = 0.f, ey = 0.f, ez = 0.f;
-        uint32_t j = j0;
-#pragma unroll 2
-        for (; j + S < nt; j += 2 * S) {
-            const float4 p0 = tile.p[j], p1 = tile.p[j + S];
-            float w0 = p0.w, w1 = p1.w;
-            if (MASKED) {
-                const bool on0 = (tile.m[j] >> q) & 1u, on1 = (tile.m[j + S] >> q) & 1u;
-                w0 = on0 ? w0 : 0.f;
-                w1 = on1 ? w1 : 0.f;
-                used += (on0 ? 1u : 0u) + (on1 ? 1u : 0u);
-            } else {
-                used += 2;
-            }
-            const float dx0 = p0.x - t.x, dy0 = p0.y - t.y, dz0 = p0.z - t.z;
-            const float dx1 = p1.x - t.x, dy1 = p1.y - t.y, dz1 = p1.z - t.z;
-            const float i0 = rsqrtf(fmaf(dx0, dx0, fmaf(dy0, dy0, fmaf(dz0, dz0, 0.1f))));
-            const float i1 = rsqrtf(fmaf(dx1, dx1, fmaf(dy1, dy1, fmaf(dz1, dz1, 0.1f))));
-            const float f0 = w0 * (i0 * i0 * i0), f1 = w1 * (i1 * i1 * i1);
-            ax = fmaf(dx0, f0, ax);
-            ay = fmaf(dy0, f0, ay);
-            az = fmaf(dz0, f0, az);
-            ex = fmaf(dx1, f1, ex);
-            ey = fmaf(dy1, f1, ey);
-            ez = fmaf(dz1, f1, ez);
-        }
-        if (j < nt) {
-            const float4 p = tile.p[j];
-            float w = p.w;
-            if (MASKED) {
-                const bool on = (tile.m[j] >> q) & 1u;
-                w = on ? w : 0.f;
-                used += on ? 1u : 0u;
-            } else {
-                ++used;
-            }
-            const float dx = p.x - t.x, dy = p.y - t.y, dz = p.z - t.z;
-            const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 0.1f))));
-            const float f = w * (inv * inv * inv);
-            ax = fmaf(dx, f, ax);
-            ay = fmaf(dy, f, ay);
-            az = fmaf(dz, f, az);
-        }
-        ax += ex;
-        ay += ey;
-        az += ez;
-    }
+__device__ __forceinline__ void tile_put(DenseTile& tile, uint32_t lane, float4 p) {
+    float* a = reinterpret_cast<float*>(&tile.a[lane >> 1]);
+    float* b = reinterpret_cast<float*>(&tile.b[lane >> 1]);
+    const uint32_t h = lane & 1u;
+    a[h] = p.x;
+    a[2 + h] = p.y;
+    b[h] = p.z;
+    b[2 + h] = p.w;
 }
 
+// one target against the tile's source pairs m = m0, m0 + S, ... (sources
+// 2m and 2m + 1, fewer than nt real ones; the slot past an odd nt holds a
+// zero mass, which adds exactly zero).  Plain sums keep the two sources of
+// a pair in the two halves of float2 accumulators (two FMA chains in one
+// instruction); Kahan sums go source by source.
+template <bool KAHAN>
+__device__ __forceinline__ void dense_tile(const DenseTile& tile, uint32_t m0, uint32_t S,
+                                           uint32_t nt, float4 t, float2& sx, float2& sy,
+                                           float2& sz, float& ax, float& ay, float& az,
+                                           float& cx, float& cy, float& cz) {
+    if constexpr (KAHAN) {
+        for (uint32_t m = m0; 2 * m < nt; m += S) {
+            const float4 a = tile.a[m], b = tile.b[m];
+            for (uint32_t h = 0; h < 2 && 2 * m + h < nt; ++h) {
+                const float px = h ? a.y : a.x, py = h ? a.w : a.z, pz = h ? b.y : b.x,
+                            pw = h ? b.w : b.z;
+                const float dx = px - t.x, dy = py - t.y, dz = pz - t.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
+                const float inv = rsqrtf(r2);
+                const float f = pw * (inv * inv * inv);
+                const float yx = __fsub_rn(__fmul_rn(dx, f), cx);
+                const float yy = __fsub_rn(__fmul_rn(dy, f), cy);
+                const float yz = __fsub_rn(__fmul_rn(dz, f), cz);
+                const float tx = __fadd_rn(ax, yx);
+                const float ty = __fadd_rn(ay, yy);
+                const float tz = __fadd_rn(az, yz);
+                cx = __fsub_rn(__fsub_rn(tx, ax), yx);
+                cy = __fsub_rn(__fsub_rn(ty, ay), yy);
+                cz = __fsub_rn(__fsub_rn(tz, az), yz);
+                ax = tx;
+                ay = ty;
+                az = tz;
+            }
+        }
+    } else {
+        const float2 ntx = make_float2(-t.x, -t.x), nty = make_float2(-t.y, -t.y),
+                     ntz = make_float2(-t.z, -t.z), eps = make_float2(0.1f, 0.1f);
+        const uint32_t np = (nt + 1u) >> 1;
+#pragma unroll 2
+        for (uint32_t m = m0; m < np; m += S) {
+            const float4 a = tile.a[m], b = tile.b[m];
+            const float2 dx = __fadd2_rn(make_float2(a.x, a.y), ntx);
+            const float2 dy = __fadd2_rn(make_float2(a.z, a.w), nty);
+            const float2 dz = __fadd2_rn(make_float2(b.x, b.y), ntz);
+            float2 r = __ffma2_rn(dz, dz, eps);
+            r = __ffma2_rn(dy, dy, r);
+            r = __ffma2_rn(dx, dx, r);
+            const float2 i = make_float2(rsqrtf(r.x), rsqrtf(r.y));
+            const float2 f = __fmul2_rn(make_float2(b.z, b.w), __fmul2_rn(__fmul2_rn(i, i), i));
+            sx = __ffma2_rn(dx, f, sx);
+            sy = __ffma2_rn(dy, f, sy);
+            sz = __ffma2_rn(dz, f, sz);
+        }
+    }
+}
 
 // The particles of the chunk entries the lanes hold (entry start es, count
 // en; en = 0 for an entry not taken) against target t: laid end to end by a
 // warp prefix sum, they pass through the warp's shared tile 32 at a time --
 // lane j finds the entry of flat particle b + j by a binary search over the
 // prefix sums and stages it (coalesced within a leaf) -- and every lane runs
-// its target against the tile's particles j = slice, slice + S, ...
+// its target against the tile's source pairs m = slice, slice + S, ...
 // Returns the particles summed (the same on every lane).
 template <bool KAHAN>
 __device__ __forceinline__ uint32_t sum_tiles(DenseTile& tile, const float4* __restrict__ xyzm,
@@ -1160,18 +1139,23 @@ __device__ __forceinline__ uint32_t sum_tiles(DenseTile& tile, const float4* __r
         const uint32_t e_excl = __shfl_sync(0xFFFFFFFFu, excl, e);
         return f < ptot ? xyzm[e_start + (f - e_excl)] : make_float4(0.f, 0.f, 0.f, 0.f);
     };
-    uint32_t used = 0;
+    float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
     float4 pcur = ptot ? fetch(0u) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (uint32_t b = 0; b < ptot; b += 32) {
         __syncwarp();
-        tile.p[lane] = pcur;
+        tile_put(tile, lane, pcur);
         __syncwarp();
         // the next tile's particle is in flight while this tile is summed
         if (b + 32 < ptot) pcur = fetch(b + 32);
         const uint32_t nt = min(32u, ptot - b);
-        dense_tile<false, KAHAN>(tile, slice, S, nt, 0u, t, ax, ay, az, cx, cy, cz, used);
+        dense_tile<KAHAN>(tile, slice, S, nt, t, sx, sy, sz, ax, ay, az, cx, cy, cz);
     }
     __syncwarp();
+    if constexpr (!KAHAN) {
+        ax += sx.x + sx.y;
+        ay += sy.x + sy.y;
+        az += sz.x + sz.y;
+    }
     return ptot;
 }
 
@@ -1431,6 +1415,7 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
 // order and sums them per particle afterwards.
 constexpr int kHeavyThreads = 512;
 constexpr int kHeavyWarps = kHeavyThreads / 32;
+constexpr int kHeavyTargets = 8;  // particles of a multi-particle leaf summed together
 
 // exclusive block scan of v; returns the block total
 __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t& excl, uint32_t* s_w) {
@@ -1450,13 +1435,14 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t& excl, uint3
 }
 
 template <bool DEBUG, bool GRAD>
-__global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
+__global__ void __launch_bounds__(kHeavyThreads, 2) k_heavy_leaf(TravArgs A) {
     __shared__ uint32_t s_w[kHeavyWarps];
     __shared__ uint32_t s_rec;
     __shared__ float s_red[kHeavyWarps][12];
     __shared__ float4 s_g[2];  // multi-particle leaf: field gradient (xx yy zz xy), local field
     __shared__ float2 s_g1;
     __shared__ unsigned long long s_cnt[kHeavyWarps][3];
+    __shared__ float s_redt[kHeavyWarps][3 * kHeavyTargets];
     Status* status = A.status;
     // (a run whose near lists ran out is void: see k_trav)
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_HEAVY_OVERFLOW |
@@ -1542,69 +1528,74 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
         float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
         unsigned long long n_m2l = 0, n_p2p = 0, n_inter = 0;
+        // one candidate: MAC, then M2L, a P2P source or its children
+        auto visit = [&](uint32_t sn, float4 sg, uint32_t& c, uint32_t& link, uint32_t& pf) {
+            float dx, dy, dz, d2;
+            if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w, th2, dx, dy, dz,
+                              d2)) {
+                const float4 mp = tv.mp[sn];
+                float fx, fy, fz;
+                if constexpr (GRAD) {
+                    float g3, gi;
+                    m2l_field_grad(dx, dy, dz, d2, mp, fx, fy, fz, g3, gi);
+                    g[0] += fmaf(g3 * dx, dx, -gi);
+                    g[1] += fmaf(g3 * dy, dy, -gi);
+                    g[2] += fmaf(g3 * dz, dz, -gi);
+                    g[3] += g3 * dx * dy;
+                    g[4] += g3 * dx * dz;
+                    g[5] += g3 * dy * dz;
+                } else {
+                    m2l_field(dx, dy, dz, d2, mp, fx, fy, fz);
+                }
+                ax += fx;
+                ay += fy;
+                az += fz;
+                ++n_m2l;
+            } else {
+                link = tv.link[sn];
+                c = link >> 28;
+                if (c == 0) {  // leaf x leaf: P2P
+                    const uint4 si = tv.info[sn];
+                    if (multi) {
+                        pf = 1;
+                    } else {
+                        p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz, cx, cy,
+                                  cz);
+                    }
+                    ++n_p2p;
+                    n_inter += (unsigned long long)si.y * ui.y;
+                }
+            }
+        };
         while (F > 0) {
             uint32_t Fn = 0;
-            for (uint32_t i0 = 0; i0 < F; i0 += kHeavyThreads) {
-                const uint32_t i = i0 + tid;
-                uint32_t c = 0, link = 0, pf = 0, sn = 0;
-                if (i < F) {
-                    sn = fa[i];
-                    const float4 sg = tv.geo[sn];
-                    float dx, dy, dz, d2;
-                    if (mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z, sg.w, th2, dx,
-                                      dy, dz, d2)) {
-                        const float4 mp = tv.mp[sn];
-                        float fx, fy, fz;
-                        if constexpr (GRAD) {
-                            float g3, gi;
-                            m2l_field_grad(dx, dy, dz, d2, mp, fx, fy, fz, g3, gi);
-                            g[0] += fmaf(g3 * dx, dx, -gi);
-                            g[1] += fmaf(g3 * dy, dy, -gi);
-                            g[2] += fmaf(g3 * dz, dz, -gi);
-                            g[3] += g3 * dx * dy;
-                            g[4] += g3 * dx * dz;
-                            g[5] += g3 * dy * dz;
-                        } else {
-                            m2l_field(dx, dy, dz, d2, mp, fx, fy, fz);
-                        }
-                        ax += fx;
-                        ay += fy;
-                        az += fz;
-                        ++n_m2l;
-                    } else {
-                        link = tv.link[sn];
-                        c = link >> 28;
-                        if (c == 0) {  // leaf x leaf: P2P
-                            const uint4 si = tv.info[sn];
-                            if (multi) {
-                                pf = 1;
-                            } else {
-                                p2p_range(A.xyzm, make_uint2(si.x, si.y), t, A.kahan, bx, by, bz,
-                                          cx, cy, cz);
-                            }
-                            ++n_p2p;
-                            n_inter += (unsigned long long)si.y * ui.y;
-                        }
-                    }
-                }
-                if (multi) {
-                    uint32_t pex;
-                    const uint32_t ptot = block_scan(pf, pex, s_w);
-                    if (np2p + ptot > A.heavy_fcap) {
-                        if (tid == 0) set_err(status, PSG_ERR_HEAVY_OVERFLOW);
-                        return;
-                    }
-                    if (pf) fp[np2p + pex] = sn;
-                    np2p += ptot;
-                }
+            // two candidates per thread and step (candidates i and i + 512 of
+            // the step's 1024), their loads in flight together; one block
+            // scan places both threads' children and P2P sources
+            for (uint32_t i0 = 0; i0 < F; i0 += 2 * kHeavyThreads) {
+                const uint32_t ia = i0 + tid, ib = ia + kHeavyThreads;
+                const uint32_t sa = ia < F ? fa[ia] : kNone, sb = ib < F ? fa[ib] : kNone;
+                const float4 ga = sa != kNone ? tv.geo[sa] : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 gb = sb != kNone ? tv.geo[sb] : make_float4(0.f, 0.f, 0.f, 0.f);
+                uint32_t ca = 0, la = 0, pa = 0, cb = 0, lb = 0, pb = 0;
+                if (sa != kNone) visit(sa, ga, ca, la, pa);
+                if (sb != kNone) visit(sb, gb, cb, lb, pb);
+                // children counts in bits 0..15 (at most 8 x 1024 a step), P2P
+                // sources above
                 uint32_t ex;
-                const uint32_t tot = block_scan(c, ex, s_w);
-                if (Fn + tot > A.heavy_fcap) {
+                const uint32_t tot = block_scan((ca + cb) | ((pa + pb) << 16), ex, s_w);
+                const uint32_t ctot = tot & 0xFFFFu, ptot = tot >> 16;
+                const uint32_t cex = ex & 0xFFFFu, pex = ex >> 16;
+                if (Fn + ctot > A.heavy_fcap || np2p + ptot > A.heavy_fcap) {
                     if (tid == 0) set_err(status, PSG_ERR_HEAVY_OVERFLOW);
                     return;
                 }
-                for (uint32_t k = 0; k < c; ++k) fb[Fn + ex + k] = (link & kLinkMask) + k;
-                Fn += tot;
+                if (pa) fp[np2p + pex] = sa;
+                if (pb) fp[np2p + pex + pa] = sb;
+                np2p += ptot;
+                for (uint32_t k = 0; k < ca; ++k) fb[Fn + cex + k] = (la & kLinkMask) + k;
+                for (uint32_t k = 0; k < cb; ++k) fb[Fn + cex + ca + k] = (lb & kLinkMask) + k;
+                Fn += ctot;
             }
             __syncthreads();
             uint32_t* tmp = fa;
@@ -1692,44 +1683,90 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy_leaf(TravArgs A) {
         }
         __syncthreads();
         if (multi) {
-            // P2P + L2P per particle over the listed sources, fixed-order sums
+            // P2P + L2P of the leaf's particles over the listed sources,
+            // kHeavyTargets particles a pass: each source particle is loaded
+            // once a pass and summed into every target's accumulators (a
+            // target's partial sum per thread runs over the same sources in
+            // the same order as one target a pass would); fixed-order sums
+            // over warps, then over the block
             const float4 L = s_g[1];
-            for (uint32_t k = 0; k < ui.y; ++k) {
-                const float4 tk = A.xyzm[ui.x + k];
-                float px = 0.f, py = 0.f, pz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
-                for (uint32_t e = tid; e < np2p; e += kHeavyThreads) {
-                    const uint4 si = tv.info[fp[e]];
-                    p2p_range(A.xyzm, make_uint2(si.x, si.y), tk, A.kahan, px, py, pz, qx, qy,
-                              qz);
+            for (uint32_t k0 = 0; k0 < ui.y; k0 += kHeavyTargets) {
+                const uint32_t nk = min((uint32_t)kHeavyTargets, ui.y - k0);
+                float4 tk[kHeavyTargets];
+                float acc[kHeavyTargets][3];
+#pragma unroll
+                for (int k = 0; k < kHeavyTargets; ++k) {
+                    tk[k] = A.xyzm[ui.x + k0 + min((uint32_t)k, nk - 1)];
+                    acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
                 }
-                const float r0 = warp_sum(px - qx), r1 = warp_sum(py - qy),
-                            r2 = warp_sum(pz - qz);
-                if (lane == 0) {
-                    s_red[w][0] = r0;
-                    s_red[w][1] = r1;
-                    s_red[w][2] = r2;
+                if (A.kahan) {
+                    // compensated sums: one target at a time (a rare mode)
+                    for (uint32_t k = 0; k < nk; ++k) {
+                        float px = 0.f, py = 0.f, pz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
+                        const float4 t1 = A.xyzm[ui.x + k0 + k];
+                        for (uint32_t e = tid; e < np2p; e += kHeavyThreads) {
+                            const uint4 si = tv.info[fp[e]];
+                            p2p_range(A.xyzm, make_uint2(si.x, si.y), t1, true, px, py, pz, qx,
+                                      qy, qz);
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < kHeavyTargets; ++kk)
+                            if ((uint32_t)kk == k) {
+                                acc[kk][0] = px - qx;
+                                acc[kk][1] = py - qy;
+                                acc[kk][2] = pz - qz;
+                            }
+                    }
+                } else {
+                    for (uint32_t e = tid; e < np2p; e += kHeavyThreads) {
+                        const uint4 si = tv.info[fp[e]];
+                        for (uint32_t j = 0; j < si.y; ++j) {
+                            const float4 p = A.xyzm[si.x + j];
+#pragma unroll
+                            for (int k = 0; k < kHeavyTargets; ++k) {
+                                const float dx = p.x - tk[k].x, dy = p.y - tk[k].y,
+                                            dz = p.z - tk[k].z;
+                                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
+                                const float inv = rsqrtf(r2);
+                                const float f = p.w * (inv * inv * inv);
+                                acc[k][0] = fmaf(dx, f, acc[k][0]);
+                                acc[k][1] = fmaf(dy, f, acc[k][1]);
+                                acc[k][2] = fmaf(dz, f, acc[k][2]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kHeavyTargets; ++k) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float x = warp_sum(acc[k][c]);
+                        if (lane == 0) s_redt[w][3 * k + c] = x;
+                    }
                 }
                 __syncthreads();
-                if (tid == 0) {
+                if (tid < nk) {
                     float sx = 0.f, sy = 0.f, sz = 0.f;
                     for (int q = 0; q < kHeavyWarps; ++q) {
-                        sx += s_red[q][0];
-                        sy += s_red[q][1];
-                        sz += s_red[q][2];
+                        sx += s_redt[q][3 * tid];
+                        sy += s_redt[q][3 * tid + 1];
+                        sz += s_redt[q][3 * tid + 2];
                     }
+                    const uint32_t i = ui.x + k0 + tid;
+                    const float4 t1 = A.xyzm[i];
                     float lx = L.y, ly = L.z, lz = L.w;
                     if constexpr (GRAD) {
                         const float3 at =
-                            grad_apply(s_g[0], s_g1, tk.x - ug.x, tk.y - ug.y, tk.z - ug.z);
+                            grad_apply(s_g[0], s_g1, t1.x - ug.x, t1.y - ug.y, t1.z - ug.z);
                         lx += at.x;
                         ly += at.y;
                         lz += at.z;
-                        if (A.leaf_of) A.leaf_of[ui.x + k] = u;
+                        if (A.leaf_of) A.leaf_of[i] = u;
                     }
-                    const double mm = (double)tk.w;
-                    A.fx[ui.x + k] = (float)(mm * ((double)lx + (double)sx));
-                    A.fy[ui.x + k] = (float)(mm * ((double)ly + (double)sy));
-                    A.fz[ui.x + k] = (float)(mm * ((double)lz + (double)sz));
+                    const double mm = (double)t1.w;
+                    A.fx[i] = (float)(mm * ((double)lx + (double)sx));
+                    A.fy[i] = (float)(mm * ((double)ly + (double)sy));
+                    A.fz[i] = (float)(mm * ((double)lz + (double)sz));
                 }
                 __syncthreads();
             }

@@ -23,7 +23,8 @@ constexpr int kMlpHid = 64;
 constexpr int kMlpOut = 8;
 constexpr int kMlpOutUsed = 3;
 constexpr float kMlpOutScale = 0.01f;  // dF = m * s * kMlpOutScale * y
-constexpr int kJudgeSamples = 4096;
+constexpr int kJudgeSamples = 4096;  // the judge's largest sample
+constexpr int kJudgeDefault = 1024;  // its sample unless set
 
 // FP32 parameter vector, the layout every entry point uses:
 //   W1[16][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64][8] b4[8]

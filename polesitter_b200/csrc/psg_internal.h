@@ -131,6 +131,7 @@ int psg_prepare_noalloc(const float* x, const float* y, const float* z, size_t n
 #define PSG_OPT_SHRINK_STORES 13 /* 1: shrink the growable traversal stores now */
 #define PSG_OPT_SORT_SPIN 14     /* > 0: sort look-back polls, first tile publishing late */
 #define PSG_OPT_JUDGE_BLOCKS 15  /* blocks per SM of the closure judge's FP64 sum (1..8) */
+#define PSG_OPT_JUDGE_SAMPLES 16 /* particles the closure judge samples (64..4096) */
 #define PSG_MAX_LEAF_CAP 256
 
 /* the learned far-field closure (k_closure.cu) */

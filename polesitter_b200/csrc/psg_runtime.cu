@@ -62,6 +62,7 @@ struct ClosureState {
     int mode;            // 0 off (the reference), 1 order-1 local, 2 order-1 + MLP
     int judge;           // run the sampled FP64 judge in mode 1 too
     int judge_bps;       // blocks per SM of the judge's FP64 direct sum (1..8)
+    int judge_samples;   // particles of the judge's sample (64..kJudgeSamples)
     float4* lg0;         // per node: field gradient xx yy zz xy
     float2* lg1;         //           xz yz
     uint32_t* leaf_of;   // per sorted particle: its leaf
@@ -371,6 +372,7 @@ static int closure_alloc(State* s) {
     PSG_ALLOC(c.judge_f64, kJudgeSamples * 3 * sizeof(double));
     c.judge_part_n = direct_f64_part_doubles(n, kJudgeSamples, s->sms * 8);
     if (c.judge_bps == 0) c.judge_bps = 4;
+    if (c.judge_samples == 0) c.judge_samples = kJudgeDefault;
     PSG_ALLOC(c.judge_part, c.judge_part_n * sizeof(double));
     PSG_ALLOC(c.d_judge, sizeof(JudgeOut));
     PSG_CHECK(cudaMallocHost((void**)&c.h_judge, sizeof(JudgeOut)));
@@ -680,7 +682,7 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     // quarter of the GPU's block slots
     ClosureState& cj = s->cl;
     const bool judge = s->order >= 1 && n > 1 && ((cj.mode == 2 && cj.have_weights) || cj.judge);
-    const int smp = n < (size_t)kJudgeSamples ? (int)n : kJudgeSamples;
+    const int smp = n < (size_t)cj.judge_samples ? (int)n : cj.judge_samples;
     if (judge) {
         PSG_CHECK(cudaEventRecord(cj.ev_sorted, st));
         PSG_CHECK(cudaStreamWaitEvent(cj.side, cj.ev_sorted, 0));
@@ -1657,6 +1659,11 @@ int psg_set_option(void* mem, int key, double value) {
         case PSG_OPT_JUDGE_BLOCKS:
             if (value < 1 || value > 8 || (double)(int)value != value) return PSG_EINVAL;
             s->cl.judge_bps = (int)value;
+            return PSG_OK;
+        case PSG_OPT_JUDGE_SAMPLES:
+            if (value < 64 || value > psg::kJudgeSamples || (double)(int)value != value)
+                return PSG_EINVAL;
+            s->cl.judge_samples = (int)value;
             return PSG_OK;
         case PSG_OPT_HEAVY_DEPTH:
             if (value > 5) return PSG_EINVAL;

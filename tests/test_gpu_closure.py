@@ -179,10 +179,18 @@ def test_judge_falls_back_when_the_network_hurts():
         b = p0.copy()
         ctx.tick(b, np.zeros(n, np.uint32))
         j = ctx.closure_last()
-    assert j["samples"] == 4096
-    assert not j["used"]
+        # the largest sample judges the same way
+        ctx.set_option(P.OPT_JUDGE_SAMPLES, 4096)
+        c = p0.copy()
+        ctx.tick(c, np.zeros(n, np.uint32))
+        j4 = ctx.closure_last()
+        with pytest.raises(P.PolesitterError):
+            ctx.set_option(P.OPT_JUDGE_SAMPLES, 8192)
+    assert j["samples"] == 1024 and j4["samples"] == 4096
+    assert not j["used"] and not j4["used"]
     assert j["median_mlp"] > j["median_base"]
     assert np.array_equal(forces(a), forces(b))
+    assert np.array_equal(forces(a), forces(c))
 
 
 WEIGHTS = CL.default_weights_path()
