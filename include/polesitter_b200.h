@@ -110,9 +110,8 @@ ps_result_t ps_b200_direct_f64(ps_context_t* ctx, const ps_particle_arrs_t* arrs
  *     ps_prepare_particles.
  *   - arrs->cnt must be 1 .. 4,194,304; larger counts return PS_EINVAL.
  *   - The first call on a device resolves the scratch's device address and
- *     keeps it for that device; make it before any stream capture.  After a
- *     cudaDeviceReset that kept address is stale: do not mix this call with
- *     device resets in one process.
+ *     keeps it for that device.  After a cudaDeviceReset that kept address
+ *     is stale: do not mix this call with device resets in one process.
  *   - Runs on the legacy default stream and returns when the results are
  *     final.  All calls share the one scratch array: calls that overlap on
  *     the GPU race, so serialise them. */

@@ -18,11 +18,10 @@
 //   * cnt must be 1 .. kNoAllocMaxParticles (4,194,304); larger counts are
 //     rejected with PS_EINVAL and a message in ps_b200_last_error().
 //   * The first call on each device resolves the scratch array's device
-//     address (cudaGetSymbolAddress) and caches it for that device; make
-//     that first call before any stream capture.  The cached address belongs
-//     to the device's context at that time: after cudaDeviceReset the next
-//     call would pass a stale address, so do not mix this entry point with
-//     device resets in one process.
+//     address (cudaGetSymbolAddress) and caches it for that device.  The
+//     cached address belongs to the device's context at that time: after
+//     cudaDeviceReset the next call would pass a stale address, so do not
+//     mix this entry point with device resets in one process.
 //   * Work runs on the legacy default stream and the call returns after the
 //     codes and the box are final.  All calls share the one scratch array, so
 //     calls that overlap on the GPU (e.g. from several host threads) race;

@@ -54,6 +54,7 @@ namespace psg {
 
 constexpr int kTravWarps = 4;
 constexpr int kTravThreads = kTravWarps * 32;
+static_assert(kTravWarps == kDenseWarpsPerBlock, "k_dense_p2p runs kTravThreads a block");
 constexpr int kCandBuf = 256;             // children of 32 opened entries
 constexpr int kStackCap = 384;            // DFS stack (node, child mask)
 constexpr int kStackSlack = 72;           // 9 levels x 7: growth of a single-entry descent
@@ -1236,11 +1237,17 @@ __device__ __forceinline__ ChunkHead load_chunk(const P2PStore& st, uint32_t c, 
 }
 
 template <bool DEBUG, bool GRAD, bool KAHAN>
-__global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
+__global__ void __launch_bounds__(kTravThreads, kDenseBlocksPerSm) k_dense_p2p(TravArgs A) {
     __shared__ float4 s_part[kTravWarps][32];  // per-leaf sums of the record's targets
     __shared__ DenseTile tiles[kTravWarps];
+    __shared__ uint2 s_ent[kTravWarps][32];  // pass 2: a leaf's entries, 32 at a time
     float4* part = s_part[threadIdx.x >> 5];
     DenseTile& tile = tiles[threadIdx.x >> 5];
+    uint2* ent = s_ent[threadIdx.x >> 5];
+    // this warp's list of partial entries (source start, count | mask << 16)
+    const uint32_t wslot = blockIdx.x * kTravWarps + (threadIdx.x >> 5);
+    if (wslot >= A.dense_part_warps) return;  // (no list: the other warps take the records)
+    uint2* const plist = A.dense_part + (size_t)wslot * kDensePartCap;
     Status* status = A.status;
     if (status->err & (PSG_ERR_NODES | PSG_ERR_SORT_SPIN | PSG_ERR_DENSE_OVERFLOW)) return;
     const TreeView& tv = A.tv;
@@ -1273,92 +1280,129 @@ __global__ void __launch_bounds__(kTravThreads) k_dense_p2p(TravArgs A) {
         part[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
         float bx = 0.f, by = 0.f, bz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-        uint32_t used = 0, partial_q = 0;
-        // pass 1: the entries that serve every leaf of the record; the next
-        // chunk's header and entries are loaded while a chunk is summed
+        uint32_t used = 0;
+        // The chain is walked once, in segments.  Pass 1 sums the entries
+        // that serve every leaf of the record and keeps the others (partial
+        // entries) in the warp's list, in chain order; when the list could
+        // not take another chunk, or at the chain's end, pass 2 sums the
+        // listed entries leaf by leaf and the list starts over.  While a
+        // chunk is summed, the next chunk's source ranges and the header
+        // after it are in flight.
+        auto src_range = [&](const ChunkHead& hh) -> uint2 {
+            if (lane < hh.cnt && (hh.mask & run) != 0u) {
+                const uint4 si = tv.info[hh.src];
+                return make_uint2(si.x, si.y);
+            }
+            return make_uint2(0u, 0u);
+        };
         ChunkHead h = load_chunk(A.p2p, rec.y, lane);
-        for (uint32_t c = rec.y; c != kNone;) {
-            const uint32_t cnt = h.cnt;
-            uint32_t em = 0, es = 0, en = 0;
-            if (lane < cnt) {
-                em = h.mask & run;
-                if (em == run) {
-                    const uint4 si = tv.info[h.src];
-                    es = si.x;
-                    en = si.y;
-                }
-            }
-            c = h.next;
-            h = load_chunk(A.p2p, c, lane);
-            partial_q |= __reduce_or_sync(0xFFFFFFFFu, em != run ? em : 0u);
-            if (S >= 8u) {
-                for (uint32_t full = __ballot_sync(0xFFFFFFFFu, em == run); full;
-                     full &= full - 1) {
-                    const uint32_t e = __ffs(full) - 1;
-                    const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
-                    const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
-                    walk_leaf<KAHAN>(xyzm, s0, n0, slice, S, t, bx, by, bz, cx, cy, cz);
-                    if (DEBUG) used += n0;
-                }
-            } else {
-                const uint32_t got =
-                    sum_tiles<KAHAN>(tile, xyzm, es, en, slice, S, t, bx, by, bz, cx, cy, cz);
-                if (DEBUG) used += got;
-            }
-        }
-        // pass 2: per leaf of the record, the entries that serve it but not
-        // every leaf of the record
-        for (uint32_t m = partial_q; m; m &= m - 1) {
-            const uint32_t qq = __ffs(m) - 1;
-            const uint4 ci = tv.info[fc + qq];
-            const uint32_t lo = max(ci.x, first), hi = min(ci.x + ci.y, first + cnt_t);
-            if (hi <= lo) continue;
-            const uint32_t nq = hi - lo;
-            uint32_t Tq = 1;
-            while (Tq < nq) Tq <<= 1;
-            const uint32_t Sq = 32u / Tq, tq = lane & (Tq - 1u), sq = lane / Tq;
-            const bool actq = tq < nq;
-            const uint32_t iq = lo + (actq ? tq : 0u);
-            const float4 tp = xyzm[iq];
-            float px = 0.f, py = 0.f, pz = 0.f, kx = 0.f, ky = 0.f, kz = 0.f;
-            uint32_t usedq = 0;
-            ChunkHead hq = load_chunk(A.p2p, rec.y, lane);
-            for (uint32_t c = rec.y; c != kNone;) {
-                const uint32_t cnt = hq.cnt;
-                uint32_t em = 0, es = 0, en = 0;
-                if (lane < cnt) em = hq.mask & run;
-                const bool mine = em != run && ((em >> qq) & 1u);
-                if (mine) {
-                    const uint4 si = tv.info[hq.src];
-                    es = si.x;
-                    en = si.y;
-                }
-                c = hq.next;
-                hq = load_chunk(A.p2p, c, lane);
-                if (Sq >= 8u) {
-                    for (uint32_t pm = __ballot_sync(0xFFFFFFFFu, mine); pm; pm &= pm - 1) {
-                        const uint32_t e = __ffs(pm) - 1;
+        uint2 hr = src_range(h);
+        ChunkHead hn = load_chunk(A.p2p, h.next, lane);
+        uint32_t c = rec.y;
+        for (;;) {
+            uint32_t npart = 0, partial_q = 0;
+            while (c != kNone && npart + 32u <= kDensePartCap) {
+                const uint32_t em = lane < h.cnt ? (h.mask & run) : 0u;
+                const uint32_t es = hr.x, en = hr.y;
+                c = h.next;
+                h = hn;
+                hr = src_range(h);
+                hn = load_chunk(A.p2p, h.next, lane);
+                const bool partial = em != 0u && em != run;
+                partial_q |= __reduce_or_sync(0xFFFFFFFFu, partial ? em : 0u);
+                const uint32_t pb = __ballot_sync(0xFFFFFFFFu, partial);
+                if (partial)
+                    plist[npart + __popc(pb & ((1u << lane) - 1u))] =
+                        make_uint2(es, en | (em << 16));
+                npart += __popc(pb);
+                if (S >= 8u) {
+                    for (uint32_t full = __ballot_sync(0xFFFFFFFFu, em == run); full;
+                         full &= full - 1) {
+                        const uint32_t e = __ffs(full) - 1;
                         const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, e);
                         const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, en, e);
-                        walk_leaf<KAHAN>(xyzm, s0, n0, sq, Sq, tp, px, py, pz, kx, ky, kz);
-                        if (DEBUG) usedq += n0;
+                        walk_leaf<KAHAN>(xyzm, s0, n0, slice, S, t, bx, by, bz, cx, cy, cz);
+                        if (DEBUG) used += n0;
                     }
-                } else if (__any_sync(0xFFFFFFFFu, mine)) {
-                    const uint32_t got = sum_tiles<KAHAN>(tile, xyzm, es, en, sq, Sq, tp, px, py,
-                                                          pz, kx, ky, kz);
-                    if (DEBUG) usedq += got;
+                } else {
+                    const uint32_t got = sum_tiles<KAHAN>(tile, xyzm, es, em == run ? en : 0u,
+                                                          slice, S, t, bx, by, bz, cx, cy, cz);
+                    if (DEBUG) used += got;
                 }
             }
-            px -= kx;
-            py -= ky;
-            pz -= kz;
-            for (uint32_t o = Tq; o < 32u; o <<= 1) {
-                px += __shfl_xor_sync(0xFFFFFFFFu, px, o);
-                py += __shfl_xor_sync(0xFFFFFFFFu, py, o);
-                pz += __shfl_xor_sync(0xFFFFFFFFu, pz, o);
+            // pass 2: per leaf q of the record, its listed entries, gathered
+            // 32 at a time in shared memory so that the tiles run full; the
+            // lanes are dealt over q's targets alone (T_q lanes, 32 / T_q
+            // slices)
+            __syncwarp();
+            for (uint32_t m = partial_q; m; m &= m - 1) {
+                const uint32_t qq = __ffs(m) - 1;
+                const uint4 ci = tv.info[fc + qq];
+                const uint32_t lo = max(ci.x, first), hi = min(ci.x + ci.y, first + cnt_t);
+                if (hi <= lo) continue;
+                const uint32_t nq = hi - lo;
+                uint32_t Tq = 1;
+                while (Tq < nq) Tq <<= 1;
+                const uint32_t Sq = 32u / Tq, tq = lane & (Tq - 1u), sq = lane / Tq;
+                const bool actq = tq < nq;
+                const uint32_t iq = lo + (actq ? tq : 0u);
+                const float4 tp = xyzm[iq];
+                float px = 0.f, py = 0.f, pz = 0.f, kx = 0.f, ky = 0.f, kz = 0.f;
+                uint32_t usedq = 0, kept = 0;
+                for (uint32_t b = 0;; b += 32) {
+                    // take the next 32 listed entries' share for q; sum the
+                    // gathered ones when 32 are in (or at the list's end)
+                    const bool more = b < npart;
+                    uint2 v = make_uint2(0u, 0u);
+                    if (more && b + lane < npart) v = plist[b + lane];
+                    const bool mine = (v.y >> (16 + qq)) & 1u;
+                    const uint32_t mb = __ballot_sync(0xFFFFFFFFu, mine);
+                    const uint32_t pos = kept + __popc(mb & ((1u << lane) - 1u));
+                    const uint2 e2 = make_uint2(v.x, v.y & 0xFFFFu);
+                    if (mine && pos < 32u) ent[pos] = e2;
+                    kept += __popc(mb);
+                    if (kept >= 32u || (!more && kept > 0u)) {
+                        const uint32_t k = min(kept, 32u);
+                        __syncwarp();
+                        const uint2 g = lane < k ? ent[lane] : make_uint2(0u, 0u);
+                        __syncwarp();
+                        if (mine && pos >= 32u) ent[pos - 32u] = e2;
+                        kept -= k;
+                        if (Sq >= 8u) {
+                            for (uint32_t pm = __ballot_sync(0xFFFFFFFFu, lane < k); pm;
+                                 pm &= pm - 1) {
+                                const uint32_t e = __ffs(pm) - 1;
+                                const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, g.x, e);
+                                const uint32_t n0 = __shfl_sync(0xFFFFFFFFu, g.y, e);
+                                walk_leaf<KAHAN>(xyzm, s0, n0, sq, Sq, tp, px, py, pz, kx, ky, kz);
+                                if (DEBUG) usedq += n0;
+                            }
+                        } else {
+                            const uint32_t got = sum_tiles<KAHAN>(tile, xyzm, g.x, g.y, sq, Sq, tp,
+                                                                  px, py, pz, kx, ky, kz);
+                            if (DEBUG) usedq += got;
+                        }
+                    }
+                    if (!more) break;
+                }
+                px -= kx;
+                py -= ky;
+                pz -= kz;
+                for (uint32_t o = Tq; o < 32u; o <<= 1) {
+                    px += __shfl_xor_sync(0xFFFFFFFFu, px, o);
+                    py += __shfl_xor_sync(0xFFFFFFFFu, py, o);
+                    pz += __shfl_xor_sync(0xFFFFFFFFu, pz, o);
+                }
+                if (actq && sq == 0) {
+                    float4& pp = part[iq - first];
+                    pp.x += px;
+                    pp.y += py;
+                    pp.z += pz;
+                }
+                if (DEBUG) inter += (actq && sq == 0) ? usedq : 0u;
+                __syncwarp();
             }
-            if (actq && sq == 0) part[iq - first] = make_float4(px, py, pz, 0.f);
-            if (DEBUG) inter += (actq && sq == 0) ? usedq : 0u;
+            if (c == kNone) break;
         }
         __syncwarp();
         if (DEBUG) inter += (active && slice == 0) ? used : 0u;

@@ -138,6 +138,15 @@ void launch_direct_f64(const float4* xyzm, size_t n, const uint32_t* targets, si
 #include "psg_common.cuh"
 
 namespace psg {
+// k_dense_p2p: blocks per SM, warps per block, and the partial entries
+// (source leaves that serve only some leaves of a record) a warp keeps for
+// its record's second pass
+constexpr int kDenseBlocksPerSm = 8;
+constexpr int kDenseWarpsPerBlock = 4;
+constexpr uint32_t kDensePartCap = 2048;
+}  // namespace psg
+
+namespace psg {
 struct TravArgs {
     TreeView tv;
     P2PStore p2p;       // spill chunks of P2P source lists longer than a chunk
@@ -156,6 +165,8 @@ struct TravArgs {
     uint32_t* leaf_of;  // closure: leaf node of each sorted particle (order 1)
     uint4* dense_rec;   // full-leaf P2P work records: leaf | q << 28, chain, first, count
     uint32_t dense_cap;
+    uint2* dense_part;  // per warp of k_dense_p2p: kDensePartCap partial entries
+    uint32_t dense_part_warps;
     int heavy_depth;    // leaf children of nodes above this depth go to k_heavy_leaf
     uint32_t* heavy_frontier;  // per block: 2 x heavy_fcap candidate slots
     uint32_t heavy_fcap;

@@ -106,6 +106,8 @@ struct State {
     P2PStore p2p;
     uint4* dense_rec;      // full-leaf P2P work records
     uint32_t dense_cap;
+    uint2* dense_part;     // per warp of k_dense_p2p: its record's partial entries
+    uint32_t dense_part_warps;
     uint32_t* heavy_frontier;
     uint32_t heavy_fcap;
     int heavy_slots;       // blocks of k_heavy_leaf
@@ -190,6 +192,13 @@ static int alloc_dense(State* s, uint32_t cap) {
     return PSG_OK;
 }
 
+// blocks of k_dense_p2p for n particles: the blocks that fit on the SMs,
+// fewer for a small system (whose records, if any, are few), so an ensemble
+// of small systems does not launch thousands of idle blocks each
+static size_t dense_grid(const State* s, size_t n) {
+    return std::min<size_t>((size_t)s->sms * kDenseBlocksPerSm, std::max<size_t>(4, n / 64));
+}
+
 // frontier buffers of k_heavy_leaf: 2 x cap candidates per block
 static int alloc_heavy(State* s, uint32_t cap) {
     if (s->heavy_frontier) cudaFree(s->heavy_frontier);
@@ -242,7 +251,7 @@ static void free_state(State* s) {
                   s->tv.mp, s->tv.lt, s->tv.info, s->tv.parent, s->tv.arrive, s->tv.cbase,
                   s->tv.ns_off, s->tv.ns_cnt, s->tv.dbg_m2l, s->tv.dbg_p2p, s->tv.link,
                   s->tv.p2p_head, s->ns, s->p2p.src, s->p2p.mask, s->p2p.next, s->p2p.cnt,
-                  s->d_status, s->dense_rec, s->heavy_frontier, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
+                  s->d_status, s->dense_rec, s->dense_part, s->heavy_frontier, s->tk_partial, s->tk_bbox, s->tk_v[0], s->tk_v[1], s->tk_v[2],
                   s->tk_vmir[0], s->tk_vmir[1], s->tk_vmir[2], s->cl.lg0, s->cl.lg1,
                   s->cl.leaf_of, s->cl.dF, s->cl.params, s->cl.packed, s->cl.judge_tg,
                   s->cl.judge_f64, s->cl.judge_part, s->cl.d_judge};
@@ -328,6 +337,8 @@ static int init_state(State* s, size_t maxp, float theta, const uint32_t* lvl_ca
     if (r != PSG_OK) return r;
     r = alloc_dense(s, (uint32_t)(n / 4 + 1024));
     if (r != PSG_OK) return r;
+    s->dense_part_warps = (uint32_t)dense_grid(s, n) * kDenseWarpsPerBlock;
+    PSG_ALLOC(s->dense_part, (size_t)s->dense_part_warps * kDensePartCap * sizeof(uint2));
     // shallow leaves: a frontier holds at most one level's nodes plus the
     // parent's near list
     s->heavy_slots = 64;
@@ -449,6 +460,8 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     A.tv.lg1 = o ? s->cl.lg1 : nullptr;
     A.dense_rec = s->dense_rec;
     A.dense_cap = s->dense_cap;
+    A.dense_part = s->dense_part;
+    A.dense_part_warps = s->dense_part_warps;
     A.heavy_depth = heavy_depth_for(s);
     A.heavy_frontier = s->heavy_frontier;
     A.heavy_fcap = s->heavy_fcap;
@@ -476,12 +489,7 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
     const int lg[2] = {scaled(s->trav_grid[o][0][xl]), scaled(s->trav_grid[o][1][xl])};
     launch_traverse_leaves(A, lg, s->stream);
     record(s, PH_DENSE);
-    // full-leaf records: 12 blocks per SM, fewer for a small system (whose
-    // records, if any, are few), so an ensemble of small systems does not
-    // launch thousands of idle blocks each
-    const size_t dense_blocks =
-        std::min<size_t>((size_t)s->sms * 12, std::max<size_t>(4, s->trav_n / 64));
-    launch_dense_p2p(A, scaled((int)dense_blocks), s->stream);
+    launch_dense_p2p(A, scaled((int)dense_grid(s, s->trav_n)), s->stream);
     PSG_CHECK(cudaStreamWaitEvent(s->stream, s->ev_heavy, 0));
     record(s, PH_END);
     return PSG_OK;
