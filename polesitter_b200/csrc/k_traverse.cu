@@ -69,6 +69,7 @@ enum { MODE_INTERNAL = 0, MODE_LEAF = 1 };
 
 struct SmemInternal {
     float4 cgeo[8];  // the group's children: centre + half width
+    float4 cgp[4][2];  // ... pair-packed for the MAC (cgp_put)
     uint32_t cand_node[kCandBuf];
     uint32_t ns_cnt[8];
     uint32_t dbg_m2l[8];
@@ -78,6 +79,7 @@ struct SmemInternal {
 
 struct SmemLeaf {
     float4 cgeo[8];
+    float4 cgp[4][2];
     float4 chain_geo[8];    // chain groups: the ancestors a_{K+1} .. p under test
     float4 sL[8];           // the children's local fields
     float4 sG0[8];          // closure order 1: the children's field gradients
@@ -142,6 +144,24 @@ __device__ __forceinline__ float3 grad_apply(float4 g0, float2 g1, float vx, flo
     return make_float3(fmaf(g0.x, vx, fmaf(g0.w, vy, g1.x * vz)),
                        fmaf(g0.w, vx, fmaf(g0.y, vy, g1.y * vz)),
                        fmaf(g1.x, vx, fmaf(g1.y, vy, g0.z * vz)));
+}
+
+// Children 2k and 2k + 1 of the group, pair-packed for the paired FP32
+// instructions: cgp[k][0] = (x, x', y, y'), cgp[k][1] = (z, z', w, w');
+// zeros past the nc children, so that every lane computes with finite
+// values (a masked term is x * 0, which a NaN would survive).
+// Warp-collective.
+__device__ __forceinline__ void cgp_put(float4 (*cgp)[2], const float4* cgeo, uint32_t nc) {
+    const uint32_t lane = lane_id();
+    __syncwarp();
+    if (lane < 4) {
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 a = 2 * lane < nc ? cgeo[2 * lane] : z;
+        const float4 b = 2 * lane + 1 < nc ? cgeo[2 * lane + 1] : z;
+        cgp[lane][0] = make_float4(a.x, b.x, a.y, b.y);
+        cgp[lane][1] = make_float4(a.z, b.z, a.w, b.w);
+    }
+    __syncwarp();
 }
 
 // Spill the group's staged P2P sources [0, fill) to HBM chunks of
@@ -584,6 +604,7 @@ __global__ void __launch_bounds__(
                 sm.cgeo[lane] = tv.geo[fc + lane];
                 cl = tv.link[fc + lane];
             }
+            cgp_put(sm.cgp, sm.cgeo, nc);
             const uint32_t leaf_mask =
                 __ballot_sync(0xFFFFFFFFu, lane < nc && (cl >> 28) == 0) & 0xFFu;
             const uint32_t tgt_mask =
@@ -679,15 +700,18 @@ __global__ void __launch_bounds__(
             }
             __syncwarp();
 
-            float acc[SL][3];
+            // per pair of children (2k, 2k + 1): field and, for order 1, its
+            // gradient, one child in each half of a float2
+            float2 acc[SL / 2][3];
 #pragma unroll
-            for (int q = 0; q < (int)SL; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.f;
-            float gacc[GRAD ? SL : 1][6];
+            for (int k = 0; k < (int)SL / 2; ++k)
+                acc[k][0] = acc[k][1] = acc[k][2] = make_float2(0.f, 0.f);
+            float2 gacc[GRAD ? SL / 2 : 1][6];
             if constexpr (GRAD) {
 #pragma unroll
-                for (int q = 0; q < (int)SL; ++q)
+                for (int k = 0; k < (int)SL / 2; ++k)
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) gacc[q][k] = 0.f;
+                    for (int c = 0; c < 6; ++c) gacc[k][c] = make_float2(0.f, 0.f);
             }
             uint32_t ssize = 0, e0 = 0;
             uint32_t pfill = 0, phead = kNone;  // MODE_LEAF: staged / spilled P2P sources
@@ -795,38 +819,70 @@ __global__ void __launch_bounds__(
                     }
                     const uint32_t chunk_mask = __reduce_or_sync(0xFFFFFFFFu, smask);
                     uint32_t near_bits = 0;
+                    // children two at a time: the MAC per child (mac_separated,
+                    // scalar, so its decisions are the reference's), then the
+                    // M2L of m2l_field(_grad) for both children in paired FP32
+                    // instructions, each half rounding as the scalar form does
 #pragma unroll
-                    for (uint32_t k = 0; k < SL; ++k) {
-                        const uint32_t q = base + k;
-                        if (!((chunk_mask >> q) & 1u)) continue;
-                        const float4 ug = sm.cgeo[q];
-                        float dx, dy, dz, d2;
-                        const bool act = (smask >> q) & 1u;
-                        const bool sep = mac_separated(ug.x, ug.y, ug.z, ug.w, sg.x, sg.y, sg.z,
-                                                       sg.w, th2, dx, dy, dz, d2) && act;
-                        // branch-free: every lane evaluates, only separated pairs add
-                        float fx, fy, fz;
+                    for (uint32_t k = 0; k < SL / 2; ++k) {
+                        const uint32_t q = base + 2 * k;  // children q and q + 1
+                        if (!((chunk_mask >> q) & 3u)) continue;
+                        const float4 ga = sm.cgp[q >> 1][0], gb = sm.cgp[q >> 1][1];
+                        float dx0, dy0, dz0, e0, dx1, dy1, dz1, e1;
+                        const bool m0 = mac_separated(ga.x, ga.z, gb.x, gb.z, sg.x, sg.y, sg.z,
+                                                      sg.w, th2, dx0, dy0, dz0, e0);
+                        const bool m1 = mac_separated(ga.y, ga.w, gb.y, gb.w, sg.x, sg.y, sg.z,
+                                                      sg.w, th2, dx1, dy1, dz1, e1);
+                        const float2 dx = make_float2(dx0, dx1), dy = make_float2(dy0, dy1),
+                                     dz = make_float2(dz0, dz1), d2 = make_float2(e0, e1);
+                        const bool a0 = (smask >> q) & 1u, a1 = (smask >> (q + 1)) & 1u;
+                        const bool s0 = m0 && a0, s1 = m1 && a1;
+                        // branch-free: every lane evaluates, only separated
+                        // pairs add (x * 1 + acc = x + acc, x * 0 + acc = acc)
+                        const float2 on = make_float2(s0 ? 1.f : 0.f, s1 ? 1.f : 0.f);
+                        const float2 soft = __fadd2_rn(d2, make_float2(0.1f, 0.1f));
+                        const float2 inv = make_float2(rsqrtf(soft.x), rsqrtf(soft.y));
+                        const float2 inv2 = __fmul2_rn(inv, inv);
+                        const float2 ir3 = __fmul2_rn(inv2, inv);
+                        const float2 ir5 = __fmul2_rn(ir3, inv2);
+                        const float2 mx = make_float2(smp.x, smp.x),
+                                     my = make_float2(smp.y, smp.y),
+                                     mz = make_float2(smp.z, smp.z),
+                                     mw = make_float2(smp.w, smp.w);
+                        const float2 mdr =
+                            __ffma2_rn(my, dx, __ffma2_rn(mz, dy, __fmul2_rn(mw, dz)));
+                        const float2 a = __ffma2_rn(
+                            mx, ir3, __fmul2_rn(__fmul2_rn(make_float2(-3.f, -3.f), mdr), ir5));
+                        const float2 fx = __ffma2_rn(dx, a, __fmul2_rn(my, ir3));
+                        const float2 fy = __ffma2_rn(dy, a, __fmul2_rn(mz, ir3));
+                        const float2 fz = __ffma2_rn(dz, a, __fmul2_rn(mw, ir3));
+                        acc[k][0] = __ffma2_rn(fx, on, acc[k][0]);
+                        acc[k][1] = __ffma2_rn(fy, on, acc[k][1]);
+                        acc[k][2] = __ffma2_rn(fz, on, acc[k][2]);
                         if constexpr (GRAD) {
-                            float g3, gi;
-                            m2l_field_grad(dx, dy, dz, d2, smp, fx, fy, fz, g3, gi);
-                            g3 = sep ? g3 : 0.f;
-                            gi = sep ? gi : 0.f;
-                            gacc[k][0] += fmaf(g3 * dx, dx, -gi);
-                            gacc[k][1] += fmaf(g3 * dy, dy, -gi);
-                            gacc[k][2] += fmaf(g3 * dz, dz, -gi);
-                            gacc[k][3] += g3 * dx * dy;
-                            gacc[k][4] += g3 * dx * dz;
-                            gacc[k][5] += g3 * dy * dz;
-                        } else {
-                            m2l_field(dx, dy, dz, d2, smp, fx, fy, fz);
+                            // g3 d d^T - gi I, g3 = 3 m0 / r^5, gi = m0 / r^3
+                            const float2 g3 = __fmul2_rn(
+                                __fmul2_rn(__fmul2_rn(make_float2(3.f, 3.f), mx), ir5), on);
+                            const float2 gi = __fmul2_rn(__fmul2_rn(mx, ir3), on);
+                            const float2 ngi = make_float2(-gi.x, -gi.y);
+                            const float2 gx = __fmul2_rn(g3, dx), gy = __fmul2_rn(g3, dy);
+                            gacc[k][0] = __fadd2_rn(gacc[k][0], __ffma2_rn(gx, dx, ngi));
+                            gacc[k][1] = __fadd2_rn(gacc[k][1], __ffma2_rn(gy, dy, ngi));
+                            gacc[k][2] = __fadd2_rn(gacc[k][2],
+                                                    __ffma2_rn(__fmul2_rn(g3, dz), dz, ngi));
+                            gacc[k][3] = __ffma2_rn(gx, dy, gacc[k][3]);
+                            gacc[k][4] = __ffma2_rn(gx, dz, gacc[k][4]);
+                            gacc[k][5] = __ffma2_rn(gy, dz, gacc[k][5]);
                         }
-                        acc[k][0] += sep ? fx : 0.f;
-                        acc[k][1] += sep ? fy : 0.f;
-                        acc[k][2] += sep ? fz : 0.f;
-                        if (act && !sep) near_bits |= 1u << q;
+                        if (a0 && !s0) near_bits |= 1u << q;
+                        if (a1 && !s1) near_bits |= 2u << q;
                         if (DEBUG) {
-                            const uint32_t bm = __ballot_sync(0xFFFFFFFFu, sep);
-                            if (lane == 0) sm.dbg_m2l[q] += __popc(bm);
+                            const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, s0);
+                            const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, s1);
+                            if (lane == 0) {
+                                sm.dbg_m2l[q] += __popc(b0);
+                                sm.dbg_m2l[q + 1] += __popc(b1);
+                            }
                         }
                     }
                     if constexpr (MODE == MODE_INTERNAL) {
@@ -953,9 +1009,10 @@ __global__ void __launch_bounds__(
             for (uint32_t k = 0; k < SL; ++k) {
                 const uint32_t q = base + k;
                 if (!((tgt_mask >> q) & 1u)) continue;
-                const float ax = warp_sum(acc[k][0]);
-                const float ay = warp_sum(acc[k][1]);
-                const float az = warp_sum(acc[k][2]);
+                const float2* ak = acc[k >> 1];
+                const float ax = warp_sum((k & 1) ? ak[0].y : ak[0].x);
+                const float ay = warp_sum((k & 1) ? ak[1].y : ak[1].x);
+                const float az = warp_sum((k & 1) ? ak[2].y : ak[2].x);
                 float4 L = make_float4(0.f, __fadd_rn(ax, Lb.y), __fadd_rn(ay, Lb.z),
                                        __fadd_rn(az, Lb.w));
                 float4 G0 = Gp0;
@@ -966,12 +1023,13 @@ __global__ void __launch_bounds__(
                     L.y += sh.x;
                     L.z += sh.y;
                     L.w += sh.z;
-                    G0.x += warp_sum(gacc[k][0]);
-                    G0.y += warp_sum(gacc[k][1]);
-                    G0.z += warp_sum(gacc[k][2]);
-                    G0.w += warp_sum(gacc[k][3]);
-                    G1.x += warp_sum(gacc[k][4]);
-                    G1.y += warp_sum(gacc[k][5]);
+                    const float2* gk = gacc[k >> 1];
+                    G0.x += warp_sum((k & 1) ? gk[0].y : gk[0].x);
+                    G0.y += warp_sum((k & 1) ? gk[1].y : gk[1].x);
+                    G0.z += warp_sum((k & 1) ? gk[2].y : gk[2].x);
+                    G0.w += warp_sum((k & 1) ? gk[3].y : gk[3].x);
+                    G1.x += warp_sum((k & 1) ? gk[4].y : gk[4].x);
+                    G1.y += warp_sum((k & 1) ? gk[5].y : gk[5].x);
                 }
                 if (lane == 0) {
                     const uint32_t u = fc + q;
@@ -1448,9 +1506,9 @@ __global__ void __launch_bounds__(kTravThreads, kDenseBlocksPerSm) k_dense_p2p(T
 }
 
 // L2L + L2P + P2P of the shallow leaves (depth <= heavy_depth; the leaf
-// pass starts below them), one block each.  A shallow leaf is a large cell, so its walk -- the reference's
-// (t leaf, s) recursion over the whole candidate set -- reaches a large part
-// of the tree; the block runs it level-synchronously: the frontier of
+// pass starts below them), one block each.  A shallow leaf is a large cell,
+// so its walk -- the reference's (t leaf, s) recursion over the whole
+// candidate set -- reaches a large part of the tree; the block runs it level-synchronously: the frontier of
 // candidates at one level is tested by all threads (separated: M2L, leaf:
 // P2P, else: its children go to the next frontier, placed by a block scan).
 // Frontier order and the final reduction are fixed, so the result does not
