@@ -95,11 +95,11 @@ KERNELS_PER_TICK = {"plain": 39, "closure": 45}
 # DRAM bytes (read + write) of one launch of the dominant kernel, from the
 # ncu captures summarised under profiles/ (None: not captured for this
 # configuration)
-DOMINANT_DRAM_BYTES = {"plain": 255.3e6, "closure": 0.53e9}
+DOMINANT_DRAM_BYTES = {"plain": 255.3e6, "closure": 0.56e9}
 TRAFFIC_NOTE = {
     "plain": "dram read+write bytes per launch, ncu capture of this workload",
     "closure": "dram read+write bytes per launch of k_dense_p2p, ncu capture of the same kernel "
-               "at N=131072 (54.4 MB) scaled by the full-leaf pair count (x 9.74) to N=1M"}
+               "at N=131072 (57.5 MB) scaled by the full-leaf pair count (x 9.74) to N=1M"}
 FLOP_M2L = 35         # per M2L pair: polesitter.h:1065-1092
 FLOP_M2L_ORDER1 = 59  # ... plus the monopole field gradient (closure order 1)
 FLOP_P2P = 20         # per particle pair: polesitter.h:1424-1444

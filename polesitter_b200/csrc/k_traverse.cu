@@ -1508,9 +1508,10 @@ __global__ void __launch_bounds__(kTravThreads, kDenseBlocksPerSm) k_dense_p2p(T
 // L2L + L2P + P2P of the shallow leaves (depth <= heavy_depth; the leaf
 // pass starts below them), one block each.  A shallow leaf is a large cell,
 // so its walk -- the reference's (t leaf, s) recursion over the whole
-// candidate set -- reaches a large part of the tree; the block runs it level-synchronously: the frontier of
-// candidates at one level is tested by all threads (separated: M2L, leaf:
-// P2P, else: its children go to the next frontier, placed by a block scan).
+// candidate set -- reaches a large part of the tree; the block runs it
+// level-synchronously: the frontier of candidates at one level is tested by
+// all threads (separated: M2L, leaf: P2P, else: its children go to the next
+// frontier, placed by a block scan).
 // Frontier order and the final reduction are fixed, so the result does not
 // depend on scheduling.  A one-particle leaf sums its P2P during the walk; a
 // leaf holding more (leaf capacity > 1) lists its P2P sources in frontier
@@ -1787,10 +1788,8 @@ __global__ void __launch_bounds__(kHeavyThreads, 2) k_heavy_leaf(TravArgs A) {
         if (multi) {
             // P2P + L2P of the leaf's particles over the listed sources,
             // kHeavyTargets particles a pass: each source particle is loaded
-            // once a pass and summed into every target's accumulators (a
-            // target's partial sum per thread runs over the same sources in
-            // the same order as one target a pass would); fixed-order sums
-            // over warps, then over the block
+            // once a pass and summed into every target's accumulators;
+            // fixed-order sums over warps, then over the block
             const float4 L = s_g[1];
             for (uint32_t k0 = 0; k0 < ui.y; k0 += kHeavyTargets) {
                 const uint32_t nk = min((uint32_t)kHeavyTargets, ui.y - k0);
@@ -1820,22 +1819,71 @@ __global__ void __launch_bounds__(kHeavyThreads, 2) k_heavy_leaf(TravArgs A) {
                             }
                     }
                 } else {
-                    for (uint32_t e = tid; e < np2p; e += kHeavyThreads) {
-                        const uint4 si = tv.info[fp[e]];
-                        for (uint32_t j = 0; j < si.y; ++j) {
-                            const float4 p = A.xyzm[si.x + j];
+                    // the listed source leaves, 32 a warp at a time, their
+                    // particles laid end to end (a warp prefix sum) and dealt
+                    // one per lane, so that no lane idles on a short leaf;
+                    // the targets two at a time in paired FP32 instructions
+                    constexpr int KP = kHeavyTargets / 2;
+                    float2 ntx[KP], nty[KP], ntz[KP], sx[KP], sy[KP], sz[KP];
 #pragma unroll
-                            for (int k = 0; k < kHeavyTargets; ++k) {
-                                const float dx = p.x - tk[k].x, dy = p.y - tk[k].y,
-                                            dz = p.z - tk[k].z;
-                                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) + 0.1f;
-                                const float inv = rsqrtf(r2);
-                                const float f = p.w * (inv * inv * inv);
-                                acc[k][0] = fmaf(dx, f, acc[k][0]);
-                                acc[k][1] = fmaf(dy, f, acc[k][1]);
-                                acc[k][2] = fmaf(dz, f, acc[k][2]);
+                    for (int k = 0; k < KP; ++k) {
+                        ntx[k] = make_float2(-tk[2 * k].x, -tk[2 * k + 1].x);
+                        nty[k] = make_float2(-tk[2 * k].y, -tk[2 * k + 1].y);
+                        ntz[k] = make_float2(-tk[2 * k].z, -tk[2 * k + 1].z);
+                        sx[k] = sy[k] = sz[k] = make_float2(0.f, 0.f);
+                    }
+                    const float2 eps = make_float2(0.1f, 0.1f);
+                    for (uint32_t e0 = w * 32u; e0 < np2p; e0 += kHeavyThreads) {
+                        uint32_t es = 0, en = 0;
+                        if (e0 + lane < np2p) {
+                            const uint4 si = tv.info[fp[e0 + lane]];
+                            es = si.x;
+                            en = si.y;
+                        }
+                        const uint32_t incl = warp_incl_scan(en);
+                        const uint32_t ptot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+                        const uint32_t excl = incl - en;
+                        for (uint32_t b = 0; b < ptot; b += 32) {
+                            // lane's particle: the entry whose prefix holds b + lane
+                            const uint32_t f = b + lane;
+                            uint32_t ee = 0;
+#pragma unroll
+                            for (uint32_t step = 16; step > 0; step >>= 1) {
+                                const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, ee + step - 1);
+                                if (v <= f) ee += step;
+                            }
+                            const uint32_t s0 = __shfl_sync(0xFFFFFFFFu, es, ee);
+                            const uint32_t x0 = __shfl_sync(0xFFFFFFFFu, excl, ee);
+                            if (f < ptot) {
+                                const float4 p = A.xyzm[s0 + (f - x0)];
+                                const float2 px = make_float2(p.x, p.x), py = make_float2(p.y, p.y),
+                                             pz = make_float2(p.z, p.z), pw = make_float2(p.w, p.w);
+#pragma unroll
+                                for (int k = 0; k < KP; ++k) {
+                                    const float2 dx = __fadd2_rn(px, ntx[k]);
+                                    const float2 dy = __fadd2_rn(py, nty[k]);
+                                    const float2 dz = __fadd2_rn(pz, ntz[k]);
+                                    float2 r = __ffma2_rn(dz, dz, eps);
+                                    r = __ffma2_rn(dy, dy, r);
+                                    r = __ffma2_rn(dx, dx, r);
+                                    const float2 i = make_float2(rsqrtf(r.x), rsqrtf(r.y));
+                                    const float2 fw =
+                                        __fmul2_rn(pw, __fmul2_rn(__fmul2_rn(i, i), i));
+                                    sx[k] = __ffma2_rn(dx, fw, sx[k]);
+                                    sy[k] = __ffma2_rn(dy, fw, sy[k]);
+                                    sz[k] = __ffma2_rn(dz, fw, sz[k]);
+                                }
                             }
                         }
+                    }
+#pragma unroll
+                    for (int k = 0; k < KP; ++k) {
+                        acc[2 * k][0] = sx[k].x;
+                        acc[2 * k + 1][0] = sx[k].y;
+                        acc[2 * k][1] = sy[k].x;
+                        acc[2 * k + 1][1] = sy[k].y;
+                        acc[2 * k][2] = sz[k].x;
+                        acc[2 * k + 1][2] = sz[k].y;
                     }
                 }
 #pragma unroll
