@@ -1,8 +1,9 @@
 // The learned far-field closure (no counterpart in the reference): per-particle
-// features from the order-1 local expansion, the MLP correction on the tensor
-// cores (BF16 mma.sync m16n8k16, FP32 accumulation), the sampled FP64 judge
-// with fallback to the uncorrected forces, and the training kernels
-// (forward on the tensor cores, backward and Adam in FP32).
+// features from the order-1 local expansion, the MLP correction on the
+// 5th-generation tensor cores (tcgen05.mma, BF16 operands in shared memory,
+// FP32 accumulators in tensor memory), the sampled FP64 judge with fallback
+// to the uncorrected forces, and the training kernels (forward on the tensor
+// cores with mma.sync m16n8k16, backward and Adam in FP32).
 //
 // Features of particle i in leaf u (half width h, depth d), with the leaf's
 // field L and field gradient G after the order-1 downward pass:
@@ -12,6 +13,7 @@
 //
 // Bounds: the MLP is ~2 x 9.9K flop per particle on the BF16 tensor pipe and
 // reads ~80 B per particle; the judge is 4096 x N FP64 pair terms.
+#include <algorithm>
 #include <cfloat>
 #include <cuda_bf16.h>
 
@@ -187,68 +189,266 @@ __device__ __forceinline__ void load_packed(MlpPacked& dst, const MlpPacked* src
     for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) d[i] = s[i];
 }
 
-// ---- inference: dF for every particle of the last tick -------------------
-__global__ void __launch_bounds__(128) k_closure_mlp(TreeView tv, const uint32_t* leaf_of,
-                                                     const float4* __restrict__ xyzm, size_t n,
-                                                     const MlpPacked* __restrict__ wts,
-                                                     float4* __restrict__ dF) {
-    __shared__ __align__(16) MlpPacked sw;
-    __shared__ float feat[4][16][17];
-    __shared__ float ysm[4][16][9];
-    __shared__ float scl[4][16];
-    load_packed(sw, wts);
-    __syncthreads();
-    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    const size_t tiles = (n + 15) / 16;
-    for (size_t tile = (size_t)blockIdx.x * 4 + w; tile < tiles; tile += (size_t)gridDim.x * 4) {
-        const size_t i = tile * 16 + lane;
-        if (lane < 16) {
-            float x[16];
-            float sc = 0.f;
-            if (i < n) {
-                sc = closure_features(tv, leaf_of, xyzm, i, x);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 16; ++k) x[k] = 0.f;
-            }
-#pragma unroll
-            for (int k = 0; k < 16; ++k) feat[w][lane][k] = x[k];
-            scl[w][lane] = sc;
-        }
-        __syncwarp();
-        warp_mlp<false>(sw, feat[w], ysm[w], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
-        __syncwarp();
-        if (lane < 16 && i < n) {
-            const float sc = scl[w][lane];
-            dF[i] = make_float4(sc * ysm[w][lane][0], sc * ysm[w][lane][1], sc * ysm[w][lane][2],
-                                0.f);
-        }
-        __syncwarp();
+// ---- inference on the 5th-generation tensor cores (tcgen05, TMEM) ----------
+// CTAs of 128 threads (4 per SM) take tiles of 128 particles; thread t owns
+// row t.  Each layer is D[128 x N] = A[128 x K] . Wt^T (K x N) by
+// tcgen05.mma (kind::f16: BF16 operands from shared memory, FP32
+// accumulator in tensor memory), issued by one thread, its completion
+// signalled on an mbarrier; every thread then reads its row of D from
+// tensor memory (tcgen05.ld), adds the bias, applies GELU and writes the
+// BF16 row as the next layer's A.  Shared-memory operands are in the
+// no-swizzle K-major layout: 8-row x 16-byte core matrices, 128 B apart
+// along the rows (the descriptor's stride offset) and R/8 x 128 B apart
+// along K (its leading offset) for a matrix of R rows.
+constexpr int kTcRows = 128;       // the MMA's M, one particle per row
+constexpr uint32_t kTcCols = 64;   // tensor-memory columns: one 128 x 64 FP32 accumulator
+constexpr long long kTcWaitCycles = 1ll << 31;  // ~1 s: the bound on an MMA's completion
+// CTAs per SM: while one waits on its MMA, the others compute features and
+// activations (41 KB of shared memory and 64 tensor-memory columns each)
+constexpr int kTcBlocksPerSm = 4;
+
+struct __align__(128) TcSmem {
+    uint8_t a0[kTcRows * kMlpIn * 2];   // features, 128 x 16
+    uint8_t h[kTcRows * kMlpHid * 2];   // hidden activations, 128 x 64
+    uint8_t w1[kMlpHid * kMlpIn * 2];   // Wt1: N = 64 rows x K = 16
+    uint8_t w2[kMlpHid * kMlpHid * 2];  // Wt2: 64 x 64
+    uint8_t w3[kMlpHid * kMlpHid * 2];  // Wt3: 64 x 64
+    uint8_t w4[16 * kMlpHid * 2];       // Wt4: N = 16 rows (8 .. 15 zero) x K = 64
+    float b1[kMlpHid], b2[kMlpHid], b3[kMlpHid], b4[16];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+// byte offset of element (row, k) of a K-major BF16 operand of `rows` rows
+__device__ __forceinline__ uint32_t kmaj_off(uint32_t row, uint32_t k, uint32_t rows) {
+    return ((k >> 3) * (rows >> 3) + (row >> 3)) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// shared-memory matrix descriptor of a K-major operand at shared address
+// saddr (no swizzle; leading offset = rows/8 x 128 B between the two 8-wide
+// K chunks of one MMA, stride offset = 128 B between 8-row groups; version 1)
+__device__ __forceinline__ uint64_t kmaj_desc(uint32_t saddr, uint32_t rows) {
+    const uint64_t lbo = (uint64_t)(rows >> 3) * 128u, sbo = 128u;
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((lbo >> 4) << 16) | ((sbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+// instruction descriptor: BF16 A and B (K-major), FP32 D, M = 128, N = n
+__host__ __device__ constexpr uint32_t tc_idesc(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) |
+           ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// one thread: D (+)= A . B over `ksteps` K-steps of 16, then the commit that
+// arrives on the mbarrier when they are done
+__device__ __forceinline__ void tc_layer(uint32_t tmem, uint32_t a_addr, uint32_t a_rows,
+                                         uint32_t b_addr, uint32_t b_rows, uint32_t idesc,
+                                         int ksteps, uint32_t mbar) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    for (int s = 0; s < ksteps; ++s) {
+        const uint64_t ad = kmaj_desc(a_addr + (uint32_t)s * 2u * (a_rows >> 3) * 128u, a_rows);
+        const uint64_t bd = kmaj_desc(b_addr + (uint32_t)s * 2u * (b_rows >> 3) * 128u, b_rows);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(s));
+    }
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+        : "memory");
+}
+
+// wait for the mbarrier's phase `ph` to complete, at most kTcWaitCycles
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t ph) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(ph)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > kTcWaitCycles) return false;
     }
 }
 
-// the network on given inputs x[n][16] -> y[n][8] (checks of the tensor-core path)
-__global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x, size_t n,
-                                                     const MlpPacked* __restrict__ wts,
-                                                     float* __restrict__ y) {
-    __shared__ __align__(16) MlpPacked sw;
-    __shared__ float feat[4][16][17];
-    __shared__ float ysm[4][16][9];
-    load_packed(sw, wts);
-    __syncthreads();
-    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    const size_t tiles = (n + 15) / 16;
-    for (size_t tile = (size_t)blockIdx.x * 4 + w; tile < tiles; tile += (size_t)gridDim.x * 4) {
-        const size_t i = tile * 16 + lane;
-        if (lane < 16)
-            for (int k = 0; k < 16; ++k) feat[w][lane][k] = i < n ? x[i * 16 + k] : 0.f;
-        __syncwarp();
-        warp_mlp<false>(sw, feat[w], ysm[w], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
-        __syncwarp();
-        if (lane < 16 && i < n)
-            for (int o = 0; o < kMlpOut; ++o) y[i * kMlpOut + o] = ysm[w][lane][o];
-        __syncwarp();
+// this thread's row of the accumulator, columns [c0, c0 + 16)
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// GELU with the hardware's approximate tanh (PTX tanh.approx.f32, relative
+// error below 2^-10.9): far below the BF16 rounding every activation gets
+// next, and a quarter of the closure network's time against tanhf
+__device__ __forceinline__ float gelu_hw(float x) {
+    const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+    float th;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(th) : "f"(u));
+    return 0.5f * x * (1.0f + th);
+}
+
+// z = D[t] + b; GELU(z) rounded to BF16 into row t of the activations
+__device__ __forceinline__ void tc_act(TcSmem& sm, uint32_t trow, const float* bias, uint32_t t) {
+#pragma unroll
+    for (int c0 = 0; c0 < kMlpHid; c0 += 16) {
+        float v[16];
+        tc_ld16(trow + (uint32_t)c0, v);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            uint4 q;
+            uint32_t* qq = reinterpret_cast<uint32_t*>(&q);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int k = c0 + half * 8 + 2 * j;
+                qq[j] = pack_bf16x2(gelu_hw(v[half * 8 + 2 * j] + bias[k]),
+                                    gelu_hw(v[half * 8 + 2 * j + 1] + bias[k + 1]));
+            }
+            *reinterpret_cast<uint4*>(sm.h + kmaj_off(t, (uint32_t)(c0 + half * 8), kTcRows)) = q;
+        }
     }
+}
+
+__device__ __forceinline__ void tc_sync() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+}
+
+// FEAT: features from the tree (the closure's correction dF = s y); else
+// given inputs x[n][16] -> y[n][8] (the checks of the tensor-core path)
+template <bool FEAT>
+__global__ void __launch_bounds__(kTcRows, kTcBlocksPerSm)
+    k_mlp_tc(TreeView tv, const uint32_t* leaf_of, const float4* __restrict__ xyzm,
+             const float* __restrict__ xin, size_t n, const MlpPacked* __restrict__ wts,
+             float4* __restrict__ dF, float* __restrict__ yout, uint32_t* err) {
+    __shared__ TcSmem sm;
+    const uint32_t t = threadIdx.x, w = t >> 5;
+    const uint32_t mbar = smem_u32(&sm.mbar);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&sm.tmem)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // weights (transposed, BF16) and biases into the operand layout
+    for (uint32_t e = t; e < (uint32_t)(kMlpHid * kMlpIn); e += kTcRows) {
+        const uint32_t r = e / kMlpIn, k = e % kMlpIn;
+        *reinterpret_cast<uint16_t*>(sm.w1 + kmaj_off(r, k, kMlpHid)) = wts->wt1[r * kLd1 + k];
+    }
+    for (uint32_t e = t; e < (uint32_t)(kMlpHid * kMlpHid); e += kTcRows) {
+        const uint32_t r = e / kMlpHid, k = e % kMlpHid;
+        *reinterpret_cast<uint16_t*>(sm.w2 + kmaj_off(r, k, kMlpHid)) = wts->wt2[r * kLdH + k];
+        *reinterpret_cast<uint16_t*>(sm.w3 + kmaj_off(r, k, kMlpHid)) = wts->wt3[r * kLdH + k];
+    }
+    for (uint32_t e = t; e < 16u * kMlpHid; e += kTcRows) {
+        const uint32_t r = e / kMlpHid, k = e % kMlpHid;
+        *reinterpret_cast<uint16_t*>(sm.w4 + kmaj_off(r, k, 16)) =
+            r < (uint32_t)kMlpOut ? wts->wt4[r * kLdH + k] : (uint16_t)0;
+    }
+    if (t < (uint32_t)kMlpHid) {
+        sm.b1[t] = wts->b1[t];
+        sm.b2[t] = wts->b2[t];
+        sm.b3[t] = wts->b3[t];
+    }
+    if (t < 16) sm.b4[t] = t < (uint32_t)kMlpOut ? wts->b4[t] : 0.f;
+    tc_sync();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem;
+    const uint32_t trow = tmem + ((w * 32u) << 16);  // this warp's 32 lanes
+    const uint32_t a0 = smem_u32(sm.a0), hh = smem_u32(sm.h);
+    const uint32_t w1 = smem_u32(sm.w1), w2 = smem_u32(sm.w2), w3 = smem_u32(sm.w3),
+                   w4 = smem_u32(sm.w4);
+    uint32_t ph = 0;
+    bool ok = true;
+    const size_t tiles = (n + kTcRows - 1) / kTcRows;
+    for (size_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const size_t i = tile * kTcRows + t;
+        float x[16];
+        float sc = 0.f;
+        if (i < n) {
+            if constexpr (FEAT) {
+                sc = closure_features(tv, leaf_of, xyzm, i, x);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; ++k) x[k] = xin[i * 16 + k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = 0.f;
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            uint4 q;
+            q.x = pack_bf16x2(x[8 * c + 0], x[8 * c + 1]);
+            q.y = pack_bf16x2(x[8 * c + 2], x[8 * c + 3]);
+            q.z = pack_bf16x2(x[8 * c + 4], x[8 * c + 5]);
+            q.w = pack_bf16x2(x[8 * c + 6], x[8 * c + 7]);
+            *reinterpret_cast<uint4*>(sm.a0 + kmaj_off(t, (uint32_t)(8 * c), kTcRows)) = q;
+        }
+        // layers 1 .. 3 (64 wide), then the output layer (16 wide, 8 used)
+        const uint32_t a_addr[4] = {a0, hh, hh, hh};
+        const uint32_t b_addr[4] = {w1, w2, w3, w4};
+        const float* bias[3] = {sm.b1, sm.b2, sm.b3};
+        for (int l = 0; l < 4 && ok; ++l) {
+            tc_sync();
+            if (t == 0)
+                tc_layer(tmem, a_addr[l], kTcRows, b_addr[l], l < 3 ? kMlpHid : 16,
+                         tc_idesc(l < 3 ? kMlpHid : 16), l == 0 ? 1 : 4, mbar);
+            const bool done = tc_wait(mbar, ph);
+            ph ^= 1u;
+            ok = !__syncthreads_or(!done);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (l < 3) {
+                tc_act(sm, trow, bias[l], t);
+            } else {
+                float y[16];
+                tc_ld16(trow, y);
+                if (i < n) {
+                    if constexpr (FEAT) {
+                        dF[i] = make_float4(sc * (y[0] + sm.b4[0]), sc * (y[1] + sm.b4[1]),
+                                            sc * (y[2] + sm.b4[2]), 0.f);
+                    } else {
+#pragma unroll
+                        for (int o = 0; o < kMlpOut; ++o) yout[i * kMlpOut + o] = y[o] + sm.b4[o];
+                    }
+                }
+            }
+        }
+    }
+    if (!ok) {
+        // an MMA that did not complete in time: report it, give the last
+        // commit one more bounded wait, then release the tensor memory
+        if (t == 0) atomicOr(err, PSG_ERR_TC_TIMEOUT);
+        tc_wait(mbar, ph ^ 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (w == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTcCols)
+                     : "memory");
 }
 
 // features (and scale) of selected particles, for building training data
@@ -517,20 +717,21 @@ __global__ void k_mlp_adam(float* __restrict__ p, float* __restrict__ m, float* 
 
 // ---- launchers ------------------------------------------------------------------
 void launch_closure_mlp(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm, size_t n,
-                        const MlpPacked* w, float4* dF, int sms, cudaStream_t st) {
-    const size_t tiles = (n + 15) / 16;
-    size_t grid = (tiles + 3) / 4;
-    const size_t cap = (size_t)sms * 8;
-    if (grid > cap) grid = cap;
-    if (grid < 1) grid = 1;
-    k_closure_mlp<<<(unsigned)grid, 128, 0, st>>>(tv, leaf_of, xyzm, n, w, dF);
+                        const MlpPacked* w, float4* dF, int sms, uint32_t* err, cudaStream_t st) {
+    const size_t tiles = (n + kTcRows - 1) / kTcRows;
+    const size_t grid =
+        std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * kTcBlocksPerSm));
+    k_mlp_tc<true><<<(unsigned)grid, kTcRows, 0, st>>>(tv, leaf_of, xyzm, nullptr, n, w, dF,
+                                                       nullptr, err);
 }
 
-void launch_mlp_forward(const float* x, size_t n, const MlpPacked* w, float* y, cudaStream_t st) {
-    size_t grid = ((n + 15) / 16 + 3) / 4;
-    if (grid > 4096) grid = 4096;
-    if (grid < 1) grid = 1;
-    k_mlp_forward<<<(unsigned)grid, 128, 0, st>>>(x, n, w, y);
+void launch_mlp_forward(const float* x, size_t n, const MlpPacked* w, float* y, int sms,
+                        uint32_t* err, cudaStream_t st) {
+    const size_t tiles = (n + kTcRows - 1) / kTcRows;
+    const size_t grid =
+        std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * kTcBlocksPerSm));
+    k_mlp_tc<false><<<(unsigned)grid, kTcRows, 0, st>>>(TreeView{}, nullptr, nullptr, x, n, w,
+                                                        nullptr, y, err);
 }
 
 void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm,

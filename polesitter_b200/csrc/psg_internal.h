@@ -30,6 +30,7 @@ extern "C" {
 #define PSG_ERR_DENSE_OVERFLOW 0x20u /* full-leaf record list too small: regrow, rerun */
 #define PSG_ERR_HEAVY_OVERFLOW 0x40u /* shallow-leaf records or frontier too small */
 #define PSG_ERR_CHAIN_ORDER 0x80u   /* an order-1 group without near lists (host bug) */
+#define PSG_ERR_TC_TIMEOUT 0x100u   /* a tensor-core MMA did not complete in time */
 
 /* debug statistics slots (Status.stat) */
 #define PSG_STAT_MAC 0

@@ -99,8 +99,10 @@ void launch_forest_single_forces(const uint32_t* sys_off, uint32_t nsys, float* 
 // k_closure.cu -- the learned far-field closure (no counterpart in the reference)
 struct MlpPacked;
 struct JudgeOut;
+// the network's inference on the tensor cores (tcgen05); err receives
+// PSG_ERR_TC_TIMEOUT if an MMA does not complete
 void launch_closure_mlp(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm, size_t n,
-                        const MlpPacked* w, float4* dF, int sms, cudaStream_t st);
+                        const MlpPacked* w, float4* dF, int sms, uint32_t* err, cudaStream_t st);
 void launch_closure_features(const TreeView& tv, const uint32_t* leaf_of, const float4* xyzm,
                              size_t n, const uint32_t* idx, size_t k, float* x_out,
                              float* scale_out, cudaStream_t st);
@@ -115,7 +117,8 @@ void launch_judge_decide(const uint32_t* tg, int s, const double* f64, const flo
 void launch_closure_apply(float* fx, float* fy, float* fz, const float4* dF, size_t n,
                           const JudgeOut* j, int sms, cudaStream_t st);
 void launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t st);
-void launch_mlp_forward(const float* x, size_t n, const MlpPacked* w, float* y, cudaStream_t st);
+void launch_mlp_forward(const float* x, size_t n, const MlpPacked* w, float* y, int sms,
+                        uint32_t* err, cudaStream_t st);
 cudaError_t prepare_mlp_grad_kernel();
 size_t mlp_train_smem_bytes();
 void launch_mlp_grad(const float* X, const float* T, const uint32_t* perm, size_t b0,

@@ -753,7 +753,8 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
             tv.lg0 = c.lg0;
             tv.lg1 = c.lg1;
             if (mlp) {
-                launch_closure_mlp(tv, c.leaf_of, s->xyzm, n, c.packed, c.dF, s->sms, st);
+                launch_closure_mlp(tv, c.leaf_of, s->xyzm, n, c.packed, c.dF, s->sms,
+                                   &s->d_status->err, st);
             } else {
                 PSG_CHECK(cudaMemsetAsync(c.dF, 0, n * sizeof(float4), st));
             }
@@ -764,7 +765,15 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
             PSG_CHECK(cudaGetLastError());
             PSG_CHECK(cudaMemcpyAsync(c.h_judge, c.d_judge, sizeof(JudgeOut),
                                       cudaMemcpyDeviceToHost, st));
+            if (mlp)
+                PSG_CHECK(cudaMemcpyAsync(&s->h_status->err, &s->d_status->err, 4,
+                                          cudaMemcpyDeviceToHost, st));
             PSG_CHECK(cudaStreamSynchronize(st));
+            if (mlp && (s->h_status->err & PSG_ERR_TC_TIMEOUT)) {
+                std::snprintf(g_err, sizeof(g_err),
+                              "closure network: a tensor-core MMA did not complete");
+                return PSG_EDEVICE;
+            }
             c.last = *c.h_judge;
             ++c.tick;
         }
@@ -2111,12 +2120,20 @@ int psg_closure_forward(void* mem, const float* x, size_t n, const float* params
     PSG_CHECK(cudaMemcpyAsync(d_x, x, n * 16 * 4, cudaMemcpyHostToDevice, st));
     PSG_CHECK(cudaMemcpyAsync(d_p, params, psg::kMlpParams * 4, cudaMemcpyHostToDevice, st));
     psg::launch_mlp_pack(d_p, d_w, st);
-    psg::launch_mlp_forward(d_x, n, d_w, d_y, st);
+    PSG_CHECK(cudaMemsetAsync(&s->d_status->err, 0, 4, st));
+    psg::launch_mlp_forward(d_x, n, d_w, d_y, s->sms, &s->d_status->err, st);
     PSG_CHECK(cudaGetLastError());
     PSG_CHECK(cudaMemcpyAsync(y_out, d_y, n * 8 * 4, cudaMemcpyDeviceToHost, st));
+    PSG_CHECK(cudaMemcpyAsync(&s->h_status->err, &s->d_status->err, 4, cudaMemcpyDeviceToHost,
+                              st));
     PSG_CHECK(cudaStreamSynchronize(st));
     void* bufs[] = {d_x, d_p, d_y, d_w};
     for (void* b : bufs) cudaFree(b);
+    if (s->h_status->err & PSG_ERR_TC_TIMEOUT) {
+        std::snprintf(psg::g_err, sizeof(psg::g_err),
+                      "closure network: a tensor-core MMA did not complete");
+        return PSG_EDEVICE;
+    }
     return PSG_OK;
 }
 
