@@ -473,15 +473,37 @@ static int enqueue_traversal(State* s, const float4* xyzm, float* fx, float* fy,
         const int v = (int)(g * gs);
         return v < 1 ? 1 : v;
     };
-    for (int k = 2; k <= A.ns_levels; ++k)
+    // Shallow leaves on the aux stream.  Their walk reads the near lists and
+    // fields of the groups above depth heavy_depth, final once the internal
+    // level of depth heavy_depth - 1 is done, so it starts there and runs
+    // beside the deeper levels and the leaf pass (which starts at the groups
+    // of depth heavy_depth).
+    bool heavy_started = false;
+    auto start_heavy = [&]() -> int {
+        PSG_CHECK(cudaEventRecord(s->ev_levels, s->stream));
+        PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
+        launch_heavy_leaf(A, scaled(s->heavy_slots), s->aux);
+        PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
+        heavy_started = true;
+        return PSG_OK;
+    };
+    const int heavy_ready = A.heavy_depth - 1;
+    if (heavy_ready < 2) {
+        const int r = start_heavy();
+        if (r != PSG_OK) return r;
+    }
+    for (int k = 2; k <= A.ns_levels; ++k) {
         launch_traverse_internal(A, k, scaled(s->trav_int_grid[o]), s->stream);
+        if (k == heavy_ready) {
+            const int r = start_heavy();
+            if (r != PSG_OK) return r;
+        }
+    }
     record(s, PH_TRAV);
-    // shallow leaves on the aux stream, beside the leaf pass; the leaf
-    // pass starts at the groups of depth heavy_depth
-    PSG_CHECK(cudaEventRecord(s->ev_levels, s->stream));
-    PSG_CHECK(cudaStreamWaitEvent(s->aux, s->ev_levels, 0));
-    launch_heavy_leaf(A, scaled(s->heavy_slots), s->aux);
-    PSG_CHECK(cudaEventRecord(s->ev_heavy, s->aux));
+    if (!heavy_started) {
+        const int r = start_heavy();
+        if (r != PSG_OK) return r;
+    }
     // one system: the leaf pass starts past the shallow groups; many: each
     // group checks its own system's depth
     launch_leaf_start(s->d_status, s->tv.part_sys ? 0 : A.heavy_depth, o, s->stream);
