@@ -162,7 +162,9 @@ def test_applied_correction_is_the_oracle_network(oracle):
     xo, so = CO.features_from_raw(raw)
     yo, _ = CO.forward(prm, xo)
     want = so[:, None] * yo[:, :3]
-    assert rel_l2(dF, want) < 1e-2
+    # measured ~1.2e-4 (BF16 network, tcgen05 accumulation order, the
+    # hardware tanh); a feature scaled wrong by a percent would exceed 1e-3
+    assert rel_l2(dF, want) < 1e-3
 
 
 def test_judge_falls_back_when_the_network_hurts():
