@@ -113,6 +113,17 @@ struct State {
     int heavy_slots;       // blocks of k_heavy_leaf
     cudaStream_t aux;      // k_heavy_leaf, beside the leaf pass
     cudaEvent_t ev_levels, ev_heavy;
+    // host-array calls: the sorted arrays (final after the gather) go back to
+    // pinned host buffers on their own stream while the traversal runs
+    struct EarlyCopy {
+        void* h;
+        const void* dv;
+    } early[6];
+    int n_early = 0;
+    size_t early_bytes = 0;
+    bool early_issued = false;
+    cudaStream_t copy_out = nullptr;
+    cudaEvent_t ev_written = nullptr, ev_copied = nullptr;
     int heavy_depth;       // option; < 0: derived from theta
     int forest_heavy;      // many systems: the deepest of their shallow-leaf depths
     int ns_levels;         // near lists are stored for node depths <= this (kMaxDepth: all);
@@ -236,6 +247,15 @@ static void free_mirror(Mirror& mi) {
 }
 
 // true when the GPU can dereference p (device or managed memory)
+static bool pinned_host(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 static bool on_device(const void* p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -272,6 +292,12 @@ static void free_state(State* s) {
     }
     if (s->ev_levels) cudaEventDestroy(s->ev_levels);
     if (s->ev_heavy) cudaEventDestroy(s->ev_heavy);
+    if (s->copy_out) {
+        cudaStreamSynchronize(s->copy_out);
+        cudaStreamDestroy(s->copy_out);
+    }
+    if (s->ev_written) cudaEventDestroy(s->ev_written);
+    if (s->ev_copied) cudaEventDestroy(s->ev_copied);
     if (s->stream) cudaStreamDestroy(s->stream);
     s->magic = 0;
 }
@@ -706,6 +732,15 @@ static int tick_core(State* s, const DevArrays& d, size_t n, float cx, float cy,
     record(s, PH_SORT);
     launch_gather(s->sort.perm, d.x, d.y, d.z, d.m, d.id, n, s->xyzm, s->ids, g, st);
     launch_writeback(s->xyzm, s->ids, n, d.x, d.y, d.z, d.m, d.id, g, st);
+    if (s->n_early && !s->early_issued) {
+        PSG_CHECK(cudaEventRecord(s->ev_written, st));
+        PSG_CHECK(cudaStreamWaitEvent(s->copy_out, s->ev_written, 0));
+        for (int k = 0; k < s->n_early; ++k)
+            PSG_CHECK(cudaMemcpyAsync(s->early[k].h, s->early[k].dv, s->early_bytes,
+                                      cudaMemcpyDeviceToHost, s->copy_out));
+        PSG_CHECK(cudaEventRecord(s->ev_copied, s->copy_out));
+        s->early_issued = true;
+    }
     record(s, PH_GATHER);
     // closure judge: its FP64 direct sum needs only the sorted particles, so
     // it runs on a side stream under the tree build and traversal, on a
@@ -838,9 +873,40 @@ static int calc(State* s, const psg_arrays_t* a, float cx, float cy, float cz, f
     DevArrays d;
     int r = map_arrays(s, a, d, true);
     if (r != PSG_OK) return r;
+    // sorted positions, masses, ids and codes into pinned host arrays go back
+    // while the traversal runs (a pageable copy would block this thread, so
+    // those wait for the end); the forces go back at the end
+    s->n_early = 0;
+    s->early_issued = false;
+    s->early_bytes = n * 4;
+    if (d.any_host) {
+        void* const hs[6] = {a->x, a->y, a->z, a->mass, a->id, a->codes};
+        const void* const ds[6] = {d.x, d.y, d.z, d.m, d.id, d.codes};
+        const int which[6] = {0, 1, 2, 3, 7, 8};
+        for (int k = 0; k < 6; ++k) {
+            if (d.dev[which[k]] || !pinned_host(hs[k])) continue;
+            s->early[s->n_early++] = State::EarlyCopy{hs[k], ds[k]};
+            d.dev[which[k]] = true;  // (unmap_arrays skips it)
+        }
+        if (s->n_early && !s->copy_out) {
+            PSG_CHECK(cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking));
+            PSG_CHECK(cudaEventCreateWithFlags(&s->ev_written, cudaEventDisableTiming));
+            PSG_CHECK(cudaEventCreateWithFlags(&s->ev_copied, cudaEventDisableTiming));
+        }
+    }
     r = tick_core(s, d, n, cx, cy, cz, hw, nullptr);
-    if (r != PSG_OK) return r;
-    r = unmap_arrays(s, a, d);
+    if (r == PSG_OK) r = unmap_arrays(s, a, d);
+    if (s->early_issued) {
+        // the forces' copies and the tick's end wait for the early copies too
+        const cudaError_t e = cudaStreamWaitEvent(s->stream, s->ev_copied, 0);
+        if (e != cudaSuccess && r == PSG_OK) {
+            note("cudaStreamWaitEvent", e);
+            r = PSG_EDEVICE;
+        }
+        cudaStreamSynchronize(s->copy_out);
+    }
+    s->n_early = 0;
+    s->early_issued = false;
     if (r != PSG_OK) return r;
     PSG_CHECK(cudaStreamSynchronize(s->stream));
     return PSG_OK;
